@@ -1,0 +1,214 @@
+"""ctypes binding of ``libfmcs.so`` (include/fmcs_capi.h).
+
+This is the Python face of the drop-in boundary: every method is one C-ABI
+call.  Arrays may be numpy arrays (host memory; the library stages them) or
+CUDA tensors / objects exposing ``data_ptr()`` (device memory, used in place).
+
+There is no CPU fallback: if the shared library is missing or no GPU is
+visible, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfmcs.so")
+
+FMCS_OK = 0
+FMCS_E_INVAL = -1
+FMCS_E_OOM = -2
+FMCS_E_TIMEOUT = -3
+FMCS_E_CUDA = -4
+
+# Every symbol include/fmcs_capi.h declares.
+EXPORTS = (
+    "fmcs_create", "fmcs_destroy", "fmcs_last_error", "fmcs_synchronize", "fmcs_stream",
+    "fmcs_workspace_bytes", "fmcs_stitch", "fmcs_gather", "fmcs_sort_round", "fmcs_hash_round",
+    "fmcs_run_plan", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
+)
+
+
+class FmcsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fmcs error {code}: {msg}")
+        self.code = code
+
+
+class Slice(C.Structure):
+    _fields_ = [("src", C.c_void_p), ("src_bytes", C.c_uint32), ("src_bits", C.c_uint32),
+                ("start", C.c_uint32), ("end", C.c_uint32)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libfmcs.so and declare its signatures (raises if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run __graft_entry__.build() (nvcc, sm_100a)")
+    L = C.CDLL(path)
+    vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+    u32p = C.POINTER(C.c_uint32)
+    L.fmcs_create.argtypes = [C.POINTER(vp), i32, C.c_size_t]
+    L.fmcs_destroy.argtypes = [vp]
+    L.fmcs_destroy.restype = None
+    L.fmcs_last_error.argtypes = [vp]
+    L.fmcs_last_error.restype = C.c_char_p
+    L.fmcs_synchronize.argtypes = [vp]
+    L.fmcs_stream.argtypes = [vp]
+    L.fmcs_stream.restype = vp
+    L.fmcs_workspace_bytes.argtypes = [vp]
+    L.fmcs_workspace_bytes.restype = C.c_size_t
+    L.fmcs_stitch.argtypes = [vp, C.POINTER(Slice), u32, vp, u32, u64]
+    L.fmcs_gather.argtypes = [vp, vp, u32, vp, vp, u64]
+    L.fmcs_sort_round.argtypes = [vp, vp, u32, u32, vp, vp, vp, vp, u64, u32p]
+    L.fmcs_hash_round.argtypes = [vp, vp, u32, vp, vp, vp, u64, i32, u32p]
+    L.fmcs_run_plan.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32p, u32, u64, i32,
+                                vp, vp, u32p]
+    L.fmcs_profile.argtypes = [vp, i32]
+    L.fmcs_profile_report.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.fmcs_launch_count.argtypes = [vp]
+    L.fmcs_launch_count.restype = C.c_ulonglong
+    _lib = L
+    return L
+
+
+def _addr(a) -> Optional[int]:
+    """Address of a numpy array (host) or a device tensor (data_ptr)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return int(a.data_ptr())
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return int(a.ctypes.data)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _itemsize(a) -> int:
+    if hasattr(a, "element_size"):
+        return int(a.element_size())
+    return int(a.dtype.itemsize)
+
+
+def _len(a) -> int:
+    return int(a.shape[0])
+
+
+def _u32arr(xs: Sequence[int]):
+    return (C.c_uint32 * len(xs))(*[int(x) for x in xs])
+
+
+class Context:
+    """An fmcs_ctx: one CUDA stream and a reusable device workspace."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._L = load()
+        h = C.c_void_p()
+        rc = self._L.fmcs_create(C.byref(h), device, hbm_budget_bytes)
+        if rc != FMCS_OK:
+            raise FmcsError(rc, f"fmcs_create failed on device {device}")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fmcs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc: int):
+        if rc != FMCS_OK:
+            msg = self._L.fmcs_last_error(self._h)
+            raise FmcsError(rc, msg.decode() if msg else "")
+
+    def synchronize(self):
+        self._check(self._L.fmcs_synchronize(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.fmcs_stream(self._h) or 0)
+
+    def profile(self, enable: bool = True):
+        self._check(self._L.fmcs_profile(self._h, 1 if enable else 0))
+
+    def profile_report(self) -> dict:
+        """Per-kernel {launches, ms} since the last report (synchronizes)."""
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        self._check(self._L.fmcs_profile_report(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def launch_count(self) -> int:
+        return int(self._L.fmcs_launch_count(self._h))
+
+    def workspace_bytes(self) -> int:
+        return int(self._L.fmcs_workspace_bytes(self._h))
+
+    # -- (a) --------------------------------------------------------------
+    def stitch(self, slices, bank, n: Optional[int] = None):
+        """slices: [(array, src_bits, start, end)]; bank: output array."""
+        n = _len(bank) if n is None else n
+        arr = (Slice * len(slices))()
+        for i, (a, bits, s, e) in enumerate(slices):
+            arr[i] = Slice(_addr(a), _itemsize(a), bits, s, e)
+        self._check(self._L.fmcs_stitch(self._h, arr, len(slices), _addr(bank), _itemsize(bank), n))
+        return bank
+
+    # -- (c) --------------------------------------------------------------
+    def gather(self, bank, order, out):
+        self._check(self._L.fmcs_gather(self._h, _addr(bank), _itemsize(bank), _addr(order),
+                                        _addr(out), _len(order)))
+        return out
+
+    # -- (b)+(d) ----------------------------------------------------------
+    def sort_round(self, bank, key_bits: int, order, in_group=None, out_group=None,
+                   sorted_bank=None) -> int:
+        ng = C.c_uint32(0)
+        self._check(self._L.fmcs_sort_round(self._h, _addr(bank), _itemsize(bank), key_bits,
+                                            _addr(order), _addr(in_group), _addr(out_group),
+                                            _addr(sorted_bank), _len(bank), C.byref(ng)))
+        return ng.value
+
+    # -- (e) --------------------------------------------------------------
+    def hash_round(self, bank, order, in_group=None, out_group=None, last_round=False) -> int:
+        ng = C.c_uint32(0)
+        self._check(self._L.fmcs_hash_round(self._h, _addr(bank), _itemsize(bank), _addr(order),
+                                            _addr(in_group), _addr(out_group), _len(bank),
+                                            1 if last_round else 0, C.byref(ng)))
+        return ng.value
+
+    # -- whole plan ---------------------------------------------------------
+    def run_plan(self, cols, bw, split, order_out, group_out=None, col_order=None,
+                 hash: bool = False) -> int:
+        n = _len(cols[0])
+        ptrs = (C.c_void_p * len(cols))(*[_addr(c) for c in cols])
+        ng = C.c_uint32(0)
+        co = None if col_order is None else _u32arr(col_order)
+        self._check(self._L.fmcs_run_plan(self._h, ptrs, _u32arr([_itemsize(c) for c in cols]),
+                                          _u32arr(bw), len(cols), co, _u32arr(split), len(split), n,
+                                          1 if hash else 0, _addr(order_out), _addr(group_out),
+                                          C.byref(ng)))
+        return ng.value

@@ -1,0 +1,381 @@
+// capi.cu -- the extern "C" entry points of include/fmcs_capi.h.
+//
+// Host-side orchestration of one round / one plan: argument checks (the
+// reference asserts or exits instead, e.g. src/mergesort.h:2926-2931,
+// src/stitch_composer.cpp:684-687), host<->device staging for host pointers,
+// the round loop of Composer::multiRoundSorting (src/composer.cpp:48-135) and
+// of StitchComposer::run_single_plan (src/stitch_composer.cpp:555-806), and the
+// final status check of the bounded device waits.
+#include "fmcs_internal.h"
+#include "plan.h"
+
+#include <cstring>
+#include <vector>
+
+namespace fmcs {
+
+namespace {
+
+constexpr int kCtrNgroups = 40;   // counters slot word for group counts
+
+// Device view of an input: the pointer itself, or a staged copy of host data.
+int stage_in(fmcs_ctx *ctx, const void *p, size_t bytes, int slot, const void **out)
+{
+    if (!p) {
+        *out = nullptr;
+        return FMCS_OK;
+    }
+    if (is_device_ptr(p)) {
+        *out = p;
+        return FMCS_OK;
+    }
+    void *d;
+    int rc = ws_get(ctx, slot, bytes, &d);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "stage in");
+    *out = d;
+    return FMCS_OK;
+}
+
+// Device view of an output: the pointer itself, or a staging buffer that is
+// copied back by copy_out.
+int stage_out(fmcs_ctx *ctx, void *p, size_t bytes, int slot, void **out, bool *host)
+{
+    *host = false;
+    if (!p) {
+        *out = nullptr;
+        return FMCS_OK;
+    }
+    if (is_device_ptr(p)) {
+        *out = p;
+        return FMCS_OK;
+    }
+    *host = true;
+    return ws_get(ctx, slot, bytes, out);
+}
+
+int copy_out(fmcs_ctx *ctx, void *host, const void *dev, size_t bytes)
+{
+    cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "copy out");
+}
+
+bool valid_bank(uint32_t b) { return b == 1 || b == 2 || b == 4 || b == 8; }
+
+int finish(fmcs_ctx *ctx, const char *what, uint32_t *ngroups, const uint32_t *d_ng)
+{
+    if (ngroups && d_ng) {
+        cudaError_t e = cudaMemcpyAsync(ctx->h_small + 1, d_ng, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                        ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    }
+    int rc = check_status(ctx, what);   // synchronizes
+    if (rc) return rc;
+    if (ngroups) *ngroups = d_ng ? ctx->h_small[1] : 0;
+    return FMCS_OK;
+}
+
+int counters(fmcs_ctx *ctx, uint32_t **w)
+{
+    void *p;
+    int rc = ws_get(ctx, kSlotCounters, 4096, &p);
+    *w = (uint32_t *)p;
+    return rc;
+}
+
+// One sort round on device data.  order (device) is in/out; seg_start/d_nseg
+// describe the runs of in_group when the caller already has them.
+int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits, uint32_t *order,
+                   const uint32_t *in_group, const uint32_t *seg_start, const uint32_t *d_nseg,
+                   uint32_t *out_group, void *keys_out, uint32_t *next_seg_start, uint32_t *d_next_nseg,
+                   uint64_t n, uint32_t *d_ngroups)
+{
+    int rc;
+    void *p;
+    if (!keys_out) {
+        if ((rc = ws_get(ctx, kSlotKeys0, n * bank_bytes, &p))) return rc;
+        keys_out = p;
+    }
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    if (in_group && !seg_start) {
+        if ((rc = ws_get(ctx, kSlotSegStart, (n + 2) * sizeof(uint32_t), &p))) return rc;
+        uint32_t *ss = (uint32_t *)p;
+        if ((rc = launch_segments(ctx, in_group, ss, w + kCtrNgroups + 1, n))) return rc;
+        seg_start = ss;
+        d_nseg = w + kCtrNgroups + 1;
+    }
+    SortArgs a;
+    a.bank = bank;
+    a.bank_bytes = bank_bytes;
+    a.key_bits = key_bits;
+    a.order_in = in_group ? order : nullptr;
+    a.seg_start = in_group ? seg_start : nullptr;
+    a.nseg_host = 0;
+    a.d_nseg = in_group ? d_nseg : nullptr;
+    a.order_out = order;
+    a.keys_out = keys_out;
+    a.n = n;
+    if ((rc = sort_segments(ctx, a))) return rc;
+    if (out_group || next_seg_start)
+        return launch_group_ids_segments(ctx, keys_out, bank_bytes, in_group, out_group, next_seg_start, n,
+                                         next_seg_start ? d_next_nseg : d_ngroups);
+    return FMCS_OK;
+}
+
+}  // namespace
+}  // namespace fmcs
+
+using namespace fmcs;
+
+extern "C" int fmcs_stitch(fmcs_ctx *ctx, const fmcs_slice *slices, uint32_t nslices, void *bank,
+                           uint32_t bank_bytes, uint64_t n)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (!slices || nslices == 0 || nslices > (uint32_t)kMaxSlices || !valid_bank(bank_bytes) || (!bank && n))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_stitch: invalid arguments");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_stitch: n must be < 2^32");
+    std::vector<StitchSlice> sl(nslices);
+    size_t stage_bytes = 0;
+    for (uint32_t i = 0; i < nslices; ++i) {
+        const fmcs_slice &s = slices[i];
+        if (!valid_bank(s.src_bytes) || s.src_bits == 0 || s.src_bits > 8 * s.src_bytes || s.start < 1 ||
+            s.end < s.start || s.end > s.src_bits || (!s.src && n))
+            return set_error(ctx, FMCS_E_INVAL, "fmcs_stitch: invalid slice");
+        if (!is_device_ptr(s.src)) stage_bytes += ((n * s.src_bytes + 255) & ~uint64_t(255));
+    }
+    int rc;
+    char *stage = nullptr;
+    if (stage_bytes) {
+        void *p;
+        if ((rc = ws_get(ctx, kSlotColStage, stage_bytes, &p))) return rc;
+        stage = (char *)p;
+    }
+    for (uint32_t i = 0; i < nslices; ++i) {
+        const fmcs_slice &s = slices[i];
+        const void *src = s.src;
+        if (!is_device_ptr(src)) {
+            cudaError_t e = cudaMemcpyAsync(stage, src, n * s.src_bytes, cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_stitch stage");
+            src = stage;
+            stage += ((n * s.src_bytes + 255) & ~uint64_t(255));
+        }
+        sl[i] = StitchSlice{src, s.src_bytes, s.src_bits - s.end, s.end - s.start + 1};
+    }
+    void *dbank;
+    bool host_out;
+    if ((rc = stage_out(ctx, bank, n * bank_bytes, kSlotStageOut0, &dbank, &host_out))) return rc;
+    if ((rc = launch_stitch(ctx, sl.data(), (int)nslices, dbank, bank_bytes, n))) return rc;
+    if (host_out && (rc = copy_out(ctx, bank, dbank, n * bank_bytes))) return rc;
+    return finish(ctx, "fmcs_stitch", nullptr, nullptr);
+}
+
+extern "C" int fmcs_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order, void *out,
+                           uint64_t n)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (!valid_bank(bank_bytes) || (n && (!bank || !order || !out)))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_gather: invalid arguments");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_gather: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    int rc;
+    const void *dbank = nullptr, *dorder = nullptr;
+    if ((rc = stage_in(ctx, bank, n * bank_bytes, kSlotStageIn0, &dbank))) return rc;
+    if ((rc = stage_in(ctx, order, n * 4, kSlotStageIn1, &dorder))) return rc;
+    void *dout;
+    bool host_out;
+    if ((rc = stage_out(ctx, out, n * bank_bytes, kSlotStageOut0, &dout, &host_out))) return rc;
+    if ((rc = launch_gather(ctx, dbank, bank_bytes, (const uint32_t *)dorder, dout, n))) return rc;
+    if (host_out && (rc = copy_out(ctx, out, dout, n * bank_bytes))) return rc;
+    return finish(ctx, "fmcs_gather", nullptr, nullptr);
+}
+
+extern "C" int fmcs_sort_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits,
+                               uint32_t *order, const uint32_t *in_group, uint32_t *out_group, void *sorted_bank,
+                               uint64_t n, uint32_t *ngroups)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (ngroups) *ngroups = 0;
+    if (!(bank_bytes == 2 || bank_bytes == 4 || bank_bytes == 8))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round: bank_bytes must be 2, 4 or 8");
+    if (key_bits == 0 || key_bits > 8 * bank_bytes)
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round: key_bits must be in 1..8*bank_bytes");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    if (!bank || !order) return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round: bank and order are required");
+    int rc;
+    const void *dbank = nullptr, *dig = nullptr;
+    if ((rc = stage_in(ctx, bank, n * bank_bytes, kSlotStageIn0, &dbank))) return rc;
+    if ((rc = stage_in(ctx, in_group, n * 4, kSlotStageIn1, &dig))) return rc;
+    void *dorder, *dgroup, *dkeys;
+    bool h_order, h_group, h_keys;
+    if ((rc = stage_out(ctx, order, n * 4, kSlotStageOut0, &dorder, &h_order))) return rc;
+    if (h_order && in_group) {
+        cudaError_t e = cudaMemcpyAsync(dorder, order, n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_sort_round stage order");
+    }
+    if ((rc = stage_out(ctx, out_group, n * 4, kSlotStageOut1, &dgroup, &h_group))) return rc;
+    if ((rc = stage_out(ctx, sorted_bank, n * bank_bytes, kSlotStageOut2, &dkeys, &h_keys))) return rc;
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    if ((rc = sort_round_dev(ctx, dbank, bank_bytes, key_bits, (uint32_t *)dorder, (const uint32_t *)dig, nullptr,
+                             nullptr, (uint32_t *)dgroup, dkeys, nullptr, nullptr, n, d_ng)))
+        return rc;
+    if (h_order && (rc = copy_out(ctx, order, dorder, n * 4))) return rc;
+    if (h_group && (rc = copy_out(ctx, out_group, dgroup, n * 4))) return rc;
+    if (h_keys && (rc = copy_out(ctx, sorted_bank, dkeys, n * bank_bytes))) return rc;
+    return finish(ctx, "fmcs_sort_round", ngroups, out_group ? d_ng : nullptr);
+}
+
+extern "C" int fmcs_hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t *order,
+                               const uint32_t *in_group, uint32_t *out_group, uint64_t n, int last_round,
+                               uint32_t *ngroups)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (ngroups) *ngroups = 0;
+    if (!valid_bank(bank_bytes))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: bank_bytes must be 1, 2, 4 or 8");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    if (!bank || !order || (!last_round && !out_group))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: bank, order and (unless last) out_group required");
+    int rc;
+    const void *dbank = nullptr, *dig = nullptr;
+    if ((rc = stage_in(ctx, bank, n * bank_bytes, kSlotStageIn0, &dbank))) return rc;
+    if ((rc = stage_in(ctx, in_group, n * 4, kSlotStageIn1, &dig))) return rc;
+    void *dorder, *dgroup;
+    bool h_order, h_group;
+    if ((rc = stage_out(ctx, order, n * 4, kSlotStageOut0, &dorder, &h_order))) return rc;
+    if (h_order && in_group) {
+        cudaError_t e = cudaMemcpyAsync(dorder, order, n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_hash_round stage order");
+    }
+    if ((rc = stage_out(ctx, out_group, n * 4, kSlotStageOut1, &dgroup, &h_group))) return rc;
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    uint32_t *oin = in_group ? (uint32_t *)dorder : nullptr;
+    if (!in_group && last_round) {
+        // round 0 and last: the order stays iota
+        if ((rc = launch_iota(ctx, (uint32_t *)dorder, n))) return rc;
+        oin = (uint32_t *)dorder;
+    }
+    if ((rc = hash_round(ctx, dbank, bank_bytes, oin, (uint32_t *)dorder, (const uint32_t *)dig,
+                         (uint32_t *)dgroup, n, last_round != 0, d_ng)))
+        return rc;
+    if (h_order && (rc = copy_out(ctx, order, dorder, n * 4))) return rc;
+    if (h_group && (rc = copy_out(ctx, out_group, dgroup, n * 4))) return rc;
+    return finish(ctx, "fmcs_hash_round", ngroups, d_ng);
+}
+
+extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
+                             uint32_t ncols, const uint32_t *col_order, const uint32_t *split, uint32_t nbanks,
+                             uint64_t n, int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (ngroups) *ngroups = 0;
+    if (!cols || !col_bytes || !bw || !split || ncols == 0 || nbanks == 0 || ncols > kMaxPlanCols ||
+        nbanks > kMaxPlanBanks)
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: invalid arguments");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: n must be < 2^32");
+    if (n && !order_out) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: order_out is required");
+    for (uint32_t c = 0; c < ncols; ++c) {
+        if (!valid_bank(col_bytes[c]) || bw[c] == 0 || bw[c] > 8 * col_bytes[c] || (n && !cols[c]))
+            return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: invalid column");
+        if (!hash && col_bytes[c] == 1)   // src/stitch_composer.cpp:681-687
+            return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: 8-bit columns are not sortable (hash only)");
+    }
+    std::vector<uint32_t> corder(ncols);
+    for (uint32_t c = 0; c < ncols; ++c) corder[c] = col_order ? col_order[c] : c;
+    Plan plan;
+    std::string perr;
+    if (!build_plan(bw, ncols, corder.data(), split, nbanks, hash != 0, plan, perr))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: " + perr);
+    if (n == 0) return FMCS_OK;
+    int rc;
+    void *p;
+    // stage host columns once
+    std::vector<const void *> dcols(ncols);
+    size_t stage_bytes = 0;
+    for (uint32_t c = 0; c < ncols; ++c)
+        if (!is_device_ptr(cols[c])) stage_bytes += ((n * col_bytes[c] + 255) & ~uint64_t(255));
+    char *stage = nullptr;
+    if (stage_bytes) {
+        if ((rc = ws_get(ctx, kSlotColStage, stage_bytes, &p))) return rc;
+        stage = (char *)p;
+    }
+    for (uint32_t c = 0; c < ncols; ++c) {
+        if (is_device_ptr(cols[c])) {
+            dcols[c] = cols[c];
+        } else {
+            cudaError_t e = cudaMemcpyAsync(stage, cols[c], n * col_bytes[c], cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_plan stage");
+            dcols[c] = stage;
+            stage += ((n * col_bytes[c] + 255) & ~uint64_t(255));
+        }
+    }
+    void *dorder, *dgroup_out;
+    bool h_order, h_group;
+    if ((rc = stage_out(ctx, order_out, n * 4, kSlotStageOut0, &dorder, &h_order))) return rc;
+    if ((rc = stage_out(ctx, group_out, n * 4, kSlotStageOut1, &dgroup_out, &h_group))) return rc;
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    // group ping-pong and segment starts
+    uint32_t *g[2];
+    if ((rc = ws_get(ctx, kSlotGroupA, n * 4, &p))) return rc;
+    g[0] = (uint32_t *)p;
+    if ((rc = ws_get(ctx, kSlotGroupB, n * 4, &p))) return rc;
+    g[1] = (uint32_t *)p;
+    uint32_t *segs[2];
+    if ((rc = ws_get(ctx, kSlotSegStart, 2 * (n + 2) * sizeof(uint32_t), &p))) return rc;
+    segs[0] = (uint32_t *)p;
+    segs[1] = segs[0] + (n + 2);
+    uint32_t *d_nseg[2] = {w + kCtrNgroups + 2, w + kCtrNgroups + 3};
+    const uint32_t *in_group = nullptr;
+    const uint32_t *seg_in = nullptr;
+    const uint32_t *d_nseg_in = nullptr;
+    for (uint32_t b = 0; b < nbanks; ++b) {
+        const BankPlan &bp = plan.banks[b];
+        const bool last = (b + 1 == nbanks);
+        // (a) stitch the bank
+        void *bank;
+        if ((rc = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, &bank))) return rc;
+        std::vector<StitchSlice> sl(bp.slices.size());
+        for (size_t k = 0; k < bp.slices.size(); ++k) {
+            const SliceRec &r = bp.slices[k];
+            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
+        }
+        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n))) return rc;
+        uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
+        if (!hash) {
+            // (b)+(d): sort, then group ids (+ the next round's segments)
+            uint32_t *ns = last ? nullptr : segs[b & 1];
+            if ((rc = sort_round_dev(ctx, bank, bp.bytes, bp.bits, (uint32_t *)dorder, in_group, seg_in, d_nseg_in,
+                                     og, nullptr, ns, d_nseg[b & 1], n, d_ng)))
+                return rc;
+            seg_in = ns;
+            d_nseg_in = d_nseg[b & 1];
+        } else {
+            // (e): hash grouping rounds; the last round leaves the order alone
+            uint32_t *oin = in_group ? (uint32_t *)dorder : nullptr;
+            if (!in_group && last) {
+                if ((rc = launch_iota(ctx, (uint32_t *)dorder, n))) return rc;
+                oin = (uint32_t *)dorder;
+            }
+            if ((rc = hash_round(ctx, bank, bp.bytes, oin, (uint32_t *)dorder, in_group, og, n, last, d_ng)))
+                return rc;
+        }
+        in_group = og;
+    }
+    if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
+    if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
+    return finish(ctx, "fmcs_run_plan", ngroups, d_ng);
+}

@@ -1,0 +1,254 @@
+// context.cu -- fmcs_ctx lifetime, the device workspace (named slots that grow
+// on demand and are reused across calls; the reference instead mallocs and
+// frees every buffer per call, src/common.h:18-31), the device status word that
+// bounded waits report through, and error strings.
+#include "fmcs_internal.h"
+
+#include <cstdio>
+#include <cstring>
+
+namespace fmcs {
+
+int set_error(fmcs_ctx *ctx, int code, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(fmcs_ctx *ctx, cudaError_t e, const char *what)
+{
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? FMCS_E_OOM : FMCS_E_CUDA, buf);
+}
+
+int ws_get(fmcs_ctx *ctx, int slot, size_t bytes, void **out, bool zero_new)
+{
+    Workspace &w = ctx->ws;
+    if (bytes == 0) bytes = 256;
+    if (w.cap[slot] >= bytes) {
+        *out = w.ptr[slot];
+        return FMCS_OK;
+    }
+    size_t want = bytes + bytes / 8;
+    want = (want + 4095) & ~size_t(4095);
+    if (ctx->budget && ctx->held - w.cap[slot] + want > ctx->budget) {
+        want = bytes;
+        if (ctx->held - w.cap[slot] + want > ctx->budget) {
+            char buf[200];
+            snprintf(buf, sizeof(buf), "workspace budget exceeded: need %zu more bytes over %zu",
+                     want, ctx->budget);
+            return set_error(ctx, FMCS_E_OOM, buf);
+        }
+    }
+    if (w.ptr[slot]) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "workspace sync");
+        cudaFree(w.ptr[slot]);
+        ctx->held -= w.cap[slot];
+        w.ptr[slot] = nullptr;
+        w.cap[slot] = 0;
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(ctx, e, "workspace cudaMalloc");
+    }
+    if (zero_new) {
+        // look-back words must not carry a stale (epoch, flag) from whatever
+        // the allocation held before
+        e = cudaMemsetAsync(p, 0, want, ctx->stream);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return cuda_fail(ctx, e, "workspace memset");
+        }
+    }
+    w.ptr[slot] = p;
+    w.cap[slot] = want;
+    ctx->held += want;
+    *out = p;
+    return FMCS_OK;
+}
+
+int check_status(fmcs_ctx *ctx, const char *what)
+{
+    cudaError_t e = cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                                    ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    int s = *ctx->h_status;
+    if (s != 0) {
+        *ctx->h_status = 0;
+        cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+        char buf[200];
+        if (s == FMCS_E_TIMEOUT)
+            snprintf(buf, sizeof(buf), "%s: a device-side wait timed out", what);
+        else
+            snprintf(buf, sizeof(buf), "%s: device reported status %d", what, s);
+        return set_error(ctx, s == FMCS_E_TIMEOUT ? FMCS_E_TIMEOUT : FMCS_E_INVAL, buf);
+    }
+    return FMCS_OK;
+}
+
+static cudaEvent_t take_event(fmcs_ctx *ctx)
+{
+    if (!ctx->ev_pool.empty()) {
+        cudaEvent_t e = ctx->ev_pool.back();
+        ctx->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+LaunchScope::LaunchScope(fmcs_ctx *ctx, const char *name) : ctx_(ctx)
+{
+    ctx->launches++;
+    if (!ctx->prof_on) return;
+    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx)};
+    if (!r.a || !r.b) return;
+    cudaEventRecord(r.a, ctx->stream);
+    rec_ = (int)ctx->prof.size();
+    ctx->prof.push_back(r);
+}
+
+LaunchScope::~LaunchScope()
+{
+    if (rec_ >= 0) cudaEventRecord(ctx_->prof[rec_].b, ctx_->stream);
+}
+
+bool is_device_ptr(const void *p)
+{
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace fmcs
+
+using namespace fmcs;
+
+extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
+{
+    if (!out) return FMCS_E_INVAL;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FMCS_E_CUDA;
+    }
+    if (device < 0 || device >= ndev) return FMCS_E_INVAL;
+    fmcs_ctx *ctx = new fmcs_ctx();
+    ctx->device = device;
+    ctx->budget = hbm_budget_bytes;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, 256);
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, 256);
+    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_small, 64 * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fmcs_destroy(ctx);
+        return FMCS_E_CUDA;
+    }
+    *ctx->h_status = 0;
+    *out = ctx;
+    return FMCS_OK;
+}
+
+extern "C" void fmcs_destroy(fmcs_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int s = 0; s < kSlotCount; ++s)
+        if (ctx->ws.ptr[s]) cudaFree(ctx->ws.ptr[s]);
+    for (auto &r : ctx->prof) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->h_small) cudaFreeHost(ctx->h_small);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char *fmcs_last_error(const fmcs_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" int fmcs_synchronize(fmcs_ctx *ctx)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_synchronize");
+    return FMCS_OK;
+}
+
+extern "C" void *fmcs_stream(fmcs_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" size_t fmcs_workspace_bytes(const fmcs_ctx *ctx) { return ctx ? ctx->held : 0; }
+
+extern "C" int fmcs_profile(fmcs_ctx *ctx, int enable)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    ctx->prof_on = enable != 0;
+    return FMCS_OK;
+}
+
+extern "C" unsigned long long fmcs_launch_count(const fmcs_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
+{
+    if (!ctx || !buf || len == 0) return FMCS_E_INVAL;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_profile_report");
+    struct Agg {
+        std::string name;
+        unsigned long long n = 0;
+        double ms = 0;
+    };
+    std::vector<Agg> agg;
+    for (auto &r : ctx->prof) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) {
+            cudaGetLastError();
+            ms = 0;
+        }
+        size_t k = 0;
+        while (k < agg.size() && agg[k].name != r.name) ++k;
+        if (k == agg.size()) agg.push_back(Agg{r.name});
+        agg[k].n++;
+        agg[k].ms += ms;
+        ctx->ev_pool.push_back(r.a);
+        ctx->ev_pool.push_back(r.b);
+    }
+    ctx->prof.clear();
+    std::string out = "{";
+    for (size_t k = 0; k < agg.size(); ++k) {
+        char tmp[256];
+        snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f}", k ? ", " : "",
+                 agg[k].name.c_str(), agg[k].n, agg[k].ms);
+        out += tmp;
+    }
+    out += "}";
+    if (out.size() + 1 > len) return set_error(ctx, FMCS_E_INVAL, "fmcs_profile_report: buffer too small");
+    memcpy(buf, out.c_str(), out.size() + 1);
+    return FMCS_OK;
+}

@@ -1,0 +1,163 @@
+// fmcs_internal.h -- host-side internals of libfmcs: the context (stream,
+// device workspace, status word), the workspace slots, and the launchers of
+// the sm_100a kernels.  Not part of the public ABI (include/fmcs_capi.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fmcs_capi.h"
+
+namespace fmcs {
+
+// Named workspace slots; each grows on demand and is reused across calls.
+enum Slot : int {
+    kSlotKeys0 = 0,   // sort engine buffer 0 keys (final when the caller wants no keys)
+    kSlotKeys1,       // sort engine buffer 1 keys
+    kSlotVals1,       // sort engine buffer 1 vals
+    kSlotVals0,       // sort engine buffer 0 vals when the caller's order is host memory
+    kSlotSegStart,    // initial segment starts (n + 2)
+    kSlotLarge0,      // large-segment descriptors, ping
+    kSlotLarge1,      // large-segment descriptors, pong
+    kSlotSegHist,     // per large segment digit histograms / offsets
+    kSlotTilePrefix,  // tile prefix per large segment
+    kSlotLookback,    // look-back words
+    kSlotLocalA,      // local lists, warp tier
+    kSlotLocalB,      // block tier (medium)
+    kSlotLocalC,      // block tier (large)
+    kSlotCounters,    // small device counters
+    kSlotScanTiles,   // look-back words of the flag scans
+    kSlotHashTable,   // hash grouping table
+    kSlotHashIdx,     // hash grouping per-row ids
+    kSlotStageIn0,    // host-staging buffers
+    kSlotStageIn1,
+    kSlotStageIn2,
+    kSlotStageOut0,
+    kSlotStageOut1,
+    kSlotStageOut2,
+    kSlotBank0,       // run_plan banks
+    kSlotBank1,
+    kSlotBank2,
+    kSlotBank3,
+    kSlotGroupA,      // run_plan group ping
+    kSlotGroupB,      // run_plan group pong
+    kSlotColStage,    // run_plan host column staging (several columns)
+    kSlotMisc,
+    kSlotCount
+};
+
+struct Workspace {
+    void *ptr[kSlotCount] = {};
+    size_t cap[kSlotCount] = {};
+};
+
+}  // namespace fmcs
+
+struct fmcs_prof_rec {
+    const char *name;
+    cudaEvent_t a, b;
+};
+
+struct fmcs_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0;   // 0 = unlimited
+    size_t held = 0;     // bytes held by the workspace
+    fmcs::Workspace ws;
+    int *d_status = nullptr;       // device status word
+    uint32_t epoch = 1;            // look-back epoch, advanced per launch
+    std::string err;
+    int *h_status = nullptr;       // pinned mirror of the status word
+    uint32_t *h_small = nullptr;   // pinned small read-back area (64 words)
+    // kernel profiler: CUDA events around every launch while enabled
+    bool prof_on = false;
+    std::vector<fmcs_prof_rec> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    unsigned long long launches = 0;   // kernels launched by this context
+};
+
+namespace fmcs {
+
+int set_error(fmcs_ctx *ctx, int code, const std::string &msg);
+int cuda_fail(fmcs_ctx *ctx, cudaError_t e, const char *what);
+// Returns a device pointer of at least `bytes` in `slot` (grown as needed).
+int ws_get(fmcs_ctx *ctx, int slot, size_t bytes, void **out, bool zero_new = false);
+// Checks and clears the device status word (synchronizes the stream).
+int check_status(fmcs_ctx *ctx, const char *what);
+
+// Brackets one kernel launch: counts it and, while profiling is on, records
+// a pair of CUDA events on the context's stream around it.
+class LaunchScope {
+  public:
+    LaunchScope(fmcs_ctx *ctx, const char *name);
+    ~LaunchScope();
+
+  private:
+    fmcs_ctx *ctx_;
+    int rec_ = -1;
+};
+
+// True when the device can dereference p directly (device or managed memory).
+bool is_device_ptr(const void *p);
+
+// ---------------------------------------------------------------- stitch
+struct StitchSlice {
+    const void *src;
+    uint32_t src_bytes;
+    uint32_t rshift;   // src_bits - end
+    uint32_t width;    // end - start + 1
+};
+constexpr int kMaxSlices = 32;
+int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
+                  uint64_t n);
+
+// ---------------------------------------------------------------- gather
+int launch_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order,
+                  void *out, uint64_t n);
+
+// ---------------------------------------------------------------- sort engine
+struct SortArgs {
+    const void *bank;          // device, bank_bytes per row (row order)
+    uint32_t bank_bytes;       // 2, 4 or 8
+    uint32_t key_bits;         // significant bits
+    const uint32_t *order_in;  // device, NULL for round 0 (iota)
+    const uint32_t *seg_start; // device, nseg+1 entries (seg_start[nseg] == n), or NULL = one segment
+    uint32_t nseg_host;        // nseg when known on the host (seg_start != NULL requires d_nseg)
+    const uint32_t *d_nseg;    // device count of segments (with seg_start)
+    uint32_t *order_out;       // device, n (may alias order_in)
+    void *keys_out;            // device, n keys, or NULL
+    uint64_t n;
+};
+int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
+
+// ---------------------------------------------------------------- group ids / segments
+// out_group[i] = number of boundaries in (0, i], boundary at i when
+// keys[i] != keys[i-1] or (in_group && in_group[i] != in_group[i-1]).
+// Optionally writes the group count to *d_ngroups (device) .
+int launch_group_ids(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
+                     uint32_t *out_group, uint64_t n, uint32_t *d_ngroups);
+// seg_start[k] = position of the k-th run start of in_group; seg_start[S] = n;
+// *d_nseg = S (device).
+int launch_segments(fmcs_ctx *ctx, const uint32_t *in_group, uint32_t *seg_start, uint32_t *d_nseg,
+                    uint64_t n);
+
+// Group ids and, when seg_start != NULL, the start of every group (the next
+// round's segments); *d_count = number of groups.
+int launch_group_ids_segments(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
+                              uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *d_count);
+// v[i] = i
+int launch_iota(fmcs_ctx *ctx, uint32_t *v, uint64_t n);
+// rank[i] = (number of set flags in [0, i]) - 1; *d_count = number of set flags.
+int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64_t n, uint32_t *d_count);
+
+// ---------------------------------------------------------------- hash grouping
+int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
+               uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n,
+               bool last_round, uint32_t *d_ngroups);
+
+}  // namespace fmcs

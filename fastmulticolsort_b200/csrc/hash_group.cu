@@ -1,0 +1,210 @@
+// hash_group.cu -- (e) GROUP BY through hashing, one round.
+//
+// Reference: Composer::hashByGroup_reordered<T> (src/composer.cpp:814-976).
+// Per parent group (run of equal in_group) it assigns group ids with a chained
+// hash table in order of FIRST APPEARANCE (Hashing::subgroup_range,
+// src/hashing.h:289-385; hash mix_int/mix_lng, :21-24), the ids of consecutive
+// parent groups continuing from each other (startGrpIdx).  Unless it is the
+// last round it then clusters the oids by id with a stable counting scatter
+// (Partition::histogram_based_reordering, src/partition.h:44-161).
+//
+// B200 design.  First-appearance numbering is order-dependent, so it is made
+// deterministic without a serial walk:
+//   1. one open-addressing table keyed by (parent run, key) over the whole
+//      round; each row claims or finds its slot with a CAS on the slot's
+//      representative row and records the slot, and every row atomicMin's its
+//      position into the slot: the slot's minimum is the key's first
+//      appearance f(i) inside its run;
+//   2. first[i] = (f(i) == i); a one-pass flag scan ranks the first
+//      appearances; id(i) = rank(f(i)).  Runs are in position order, so the
+//      ranks continue across runs exactly like startGrpIdx;
+//   3. the stable clustering is the stable segmented radix sort of
+//      (id, oid) inside each run (segsort.cu).
+// The hash function only spreads keys over slots; ids never depend on it.
+// The reference's remainder-block defect (src/hashing.h:345, every block of a
+// range sized `rem_sz`) is not reproduced: every row of every run is grouped.
+#include "device_common.cuh"
+#include "fmcs_internal.h"
+
+namespace fmcs {
+
+namespace {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+template <typename K>
+__device__ __forceinline__ K key_at(const K *bank, const uint32_t *order, uint64_t i)
+{
+    return order ? bank[order[i]] : bank[i];
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ bank, const uint32_t *__restrict__ order,
+                                                          const uint32_t *__restrict__ run, uint64_t n,
+                                                          uint32_t *rep, uint32_t *minpos, uint64_t mask,
+                                                          uint32_t *slot_of, int *status)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const K k = key_at(bank, order, i);
+        const uint32_t r = run ? run[i] : 0u;
+        uint64_t h = mix64((uint64_t)k ^ ((uint64_t)r * 0x9E3779B97F4A7C15ull)) & mask;
+        uint64_t probes = 0;
+        for (;;) {
+            uint32_t cur = rep[h];
+            if (cur == kEmpty) {
+                const uint32_t prev = atomicCAS(&rep[h], kEmpty, (uint32_t)i);
+                cur = (prev == kEmpty) ? (uint32_t)i : prev;
+            }
+            if (cur == (uint32_t)i ||
+                (key_at(bank, order, cur) == k && (run ? run[cur] : 0u) == r)) {
+                atomicMin(&minpos[h], (uint32_t)i);
+                slot_of[i] = (uint32_t)h;
+                break;
+            }
+            h = (h + 1) & mask;
+            if (++probes > mask) {   // table full: cannot happen with >= 2n slots
+                atomicCAS(status, kDevOk, kDevBadInput);
+                slot_of[i] = 0;
+                break;
+            }
+        }
+    }
+}
+
+__global__ void first_flag_kernel(const uint32_t *__restrict__ slot_of, const uint32_t *__restrict__ minpos,
+                                  uint8_t *__restrict__ first, uint32_t *__restrict__ fpos, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t f = minpos[slot_of[i]];
+        fpos[i] = f;
+        first[i] = (f == (uint32_t)i) ? 1 : 0;
+    }
+}
+
+// id(i) = rank(f(i)); with `row_ids` also scatter the id to the row it
+// belongs to (row-indexed, the layout the segmented sort gathers from).
+__global__ void assign_ids_kernel(const uint32_t *__restrict__ fpos, const uint32_t *__restrict__ rank,
+                                  const uint32_t *__restrict__ order, uint32_t *__restrict__ ids,
+                                  uint32_t *__restrict__ row_ids, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = rank[fpos[i]];
+        if (ids) ids[i] = g;
+        if (row_ids) row_ids[order ? order[i] : (uint32_t)i] = g;
+    }
+}
+
+template <typename K>
+int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const uint32_t *run, uint64_t n,
+                uint32_t *rep, uint32_t *minpos, uint64_t mask, uint32_t *slot_of)
+{
+    const unsigned grid = (unsigned)ctx->num_sms * 8;
+    { LaunchScope ls_(ctx, "hash_insert");
+        hash_insert_kernel<K><<<grid, 256, 0, ctx->stream>>>((const K *)bank, order, run, n, rep, minpos, mask, slot_of,
+                                                            ctx->d_status);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "hash insert launch");
+}
+
+}  // namespace
+
+int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
+               uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n, bool last_round,
+               uint32_t *d_ngroups)
+{
+    if (n == 0) return FMCS_OK;
+    cudaStream_t st = ctx->stream;
+    int rc;
+    void *p;
+    uint64_t cap = 1024;
+    while (cap < 2 * n) cap <<= 1;
+    // table: rep[cap], minpos[cap]
+    if ((rc = ws_get(ctx, kSlotHashTable, cap * 2 * sizeof(uint32_t), &p))) return rc;
+    uint32_t *rep = (uint32_t *)p, *minpos = rep + cap;
+    cudaMemsetAsync(rep, 0xFF, cap * 2 * sizeof(uint32_t), st);
+    // per-row scratch: slot_of / rank (n), fpos (n), run ids (n), first flags (n bytes)
+    if ((rc = ws_get(ctx, kSlotHashIdx, n * 3 * sizeof(uint32_t) + n + 64, &p))) return rc;
+    uint32_t *slot_of = (uint32_t *)p;
+    uint32_t *fpos = slot_of + n;
+    uint32_t *run = fpos + n;
+    uint8_t *first = (uint8_t *)(run + n);
+    if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
+    uint32_t *d_cnt = (uint32_t *)p + 32;   // words 32..39 belong to the hash round
+    uint32_t *seg_start = nullptr;
+    if (in_group) {
+        if ((rc = launch_group_ids(ctx, nullptr, 0, in_group, run, n, nullptr))) return rc;
+    }
+    switch (bank_bytes) {
+    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
+    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
+    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
+    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
+    default: return set_error(ctx, FMCS_E_INVAL, "hash round: bank_bytes must be 1, 2, 4 or 8");
+    }
+    if (rc) return rc;
+    const unsigned grid = (unsigned)ctx->num_sms * 8;
+    { LaunchScope ls_(ctx, "first_flag");
+        first_flag_kernel<<<grid, 256, 0, st>>>(slot_of, minpos, first, fpos, n);
+    }
+    uint32_t *rank = slot_of;   // slot_of is dead after the flags
+    if ((rc = launch_flag_rank(ctx, first, rank, n, d_ngroups))) return rc;
+    if (last_round) {
+        { LaunchScope ls_(ctx, "assign_ids");
+            assign_ids_kernel<<<grid, 256, 0, st>>>(fpos, rank, nullptr, out_group, nullptr, n);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "hash ids launch");
+        if (order_out != order_in) {
+            if (order_in)
+                cudaMemcpyAsync(order_out, order_in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+            else
+                return set_error(ctx, FMCS_E_INVAL, "hash round: internal order");
+        }
+        return FMCS_OK;
+    }
+    // clustering: stable sort of (id, oid) inside each parent run; ids are
+    // scattered to row order so that the sort's gather through order_in reads them.
+    uint32_t *row_ids = run;   // run ids are dead after the insert
+    { LaunchScope ls_(ctx, "assign_ids");
+        assign_ids_kernel<<<grid, 256, 0, st>>>(fpos, rank, order_in, nullptr, row_ids, n);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "hash ids launch");
+    // key width: read the group count back
+    cudaMemcpyAsync(ctx->h_small, d_ngroups, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "hash round sync");
+    const uint32_t G = ctx->h_small[0];
+    uint32_t bits = 1;
+    while (bits < 32 && (1ull << bits) < (uint64_t)G) bits++;
+    if (in_group) {
+        if ((rc = ws_get(ctx, kSlotSegStart, (n + 2) * sizeof(uint32_t), &p))) return rc;
+        seg_start = (uint32_t *)p;
+        if ((rc = launch_segments(ctx, in_group, seg_start, d_cnt, n))) return rc;
+    }
+    SortArgs a;
+    a.bank = row_ids;
+    a.bank_bytes = 4;
+    a.key_bits = bits;
+    a.order_in = order_in;
+    a.seg_start = seg_start;
+    a.nseg_host = 0;
+    a.d_nseg = seg_start ? d_cnt : nullptr;
+    a.order_out = order_out;
+    a.keys_out = out_group;
+    a.n = n;
+    return sort_segments(ctx, a);
+}
+
+}  // namespace fmcs

@@ -1,0 +1,214 @@
+// scan.cu -- (d) group-boundary scan and segment extraction, one pass each.
+//
+// Reference: Composer::extractGroupInfo<T> (src/composer.cpp:630-678) computes
+//   g[0] = 0;  g[i] = g[i-1] + (v[i] != v[i-1] || in[i] != in[i-1])
+// with a scalar loop.  Here one kernel reads each key (and in_group word) once:
+// adjacent difference -> warp ballot -> popc prefix -> block scan -> decoupled
+// look-back across tiles (bounded waits) -> dense ids.  The same kernel, given
+// only in_group, emits the start position of every run of equal in_group (the
+// segments that the next round sorts; the reference finds them with a scalar
+// walk, src/composer.cpp:1280-1335).
+#include "device_common.cuh"
+#include "fmcs_internal.h"
+
+namespace fmcs {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;                  // per thread
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kScanWarps = kScanThreads / 32;
+
+template <typename K>
+__global__ void __launch_bounds__(kScanThreads)
+boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group,
+                     const uint8_t *__restrict__ flags, uint32_t *__restrict__ out_group, uint32_t *__restrict__ seg_start,
+                     uint64_t n, uint32_t *tile_counter, unsigned long long *lookback,
+                     uint32_t epoch, uint32_t *d_count, int *status)
+{
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp[kScanWarps + 1];
+    __shared__ uint32_t s_excl;
+
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * kScanTile;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint64_t wbase = base + (uint64_t)warp * (kScanItems * 32);
+
+    // flags in warp-striped order: item j of lane l sits at wbase + j*32 + l
+    uint32_t ballots[kScanItems];
+    uint32_t wtotal = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
+        bool f = false;
+        if (i < n) {
+            if (flags) {
+                f = flags[i] != 0;
+            } else if (i == 0) {
+                f = true;
+            } else {
+                if (keys) f = keys[i] != keys[i - 1];
+                if (in_group) f = f || (in_group[i] != in_group[i - 1]);
+            }
+        }
+        ballots[j] = __ballot_sync(0xFFFFFFFFu, f);
+        wtotal += __popc(ballots[j]);
+    }
+    if (lane == 0) s_warp[warp] = wtotal;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < kScanWarps; ++w) {
+            uint32_t c = s_warp[w];
+            s_warp[w] = run;
+            run += c;
+        }
+        s_warp[kScanWarps] = run;
+        // decoupled look-back over previous tiles
+        const uint32_t agg = run;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            st_volatile_u64(&lookback[0], lb_word(epoch, kFlagInclusive, agg));
+        } else {
+            st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagAggregate, agg));
+            int64_t p = (int64_t)tile - 1;
+            while (p >= 0) {
+                unsigned long long w = lb_wait(&lookback[p], epoch, status);
+                excl += (uint32_t)w;
+                if (((uint32_t)(w >> 32) & 3u) == kFlagInclusive) break;
+                --p;
+            }
+            st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
+        }
+        s_excl = excl;
+        if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
+    }
+    __syncthreads();
+    uint32_t run = s_excl + s_warp[warp];
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
+        const uint32_t b = ballots[j];
+        const uint32_t incl = run + __popc(b & (lanemask_lt() | (1u << lane)));
+        if (i < n) {
+            if (out_group) out_group[i] = incl - 1;
+            if (seg_start && ((b >> lane) & 1u)) seg_start[incl - 1] = (uint32_t)i;
+        }
+        run += __popc(b);
+    }
+    if (seg_start && base + kScanTile >= n && threadIdx.x == 0) {
+        // total written by thread 0 above into *d_count; the end sentinel
+        seg_start[s_excl + s_warp[kScanWarps]] = (uint32_t)n;
+    }
+}
+
+int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
+                      const uint8_t *flags, uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *d_count)
+{
+    if (n == 0) {
+        if (d_count) cudaMemsetAsync(d_count, 0, sizeof(uint32_t), ctx->stream);
+        if (seg_start) cudaMemsetAsync(seg_start, 0, sizeof(uint32_t), ctx->stream);
+        return FMCS_OK;
+    }
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    void *lb = nullptr, *cnt = nullptr;
+    int rc = ws_get(ctx, kSlotScanTiles, tiles * sizeof(unsigned long long), &lb, true);
+    if (rc) return rc;
+    rc = ws_get(ctx, kSlotCounters, 4096, &cnt);
+    if (rc) return rc;
+    uint32_t *tile_counter = (uint32_t *)cnt;  // word 0 of the counters slot
+    cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), ctx->stream);
+    const uint32_t epoch = ctx->epoch++;
+    const unsigned grid = (unsigned)tiles;
+    switch (keys ? key_bytes : 0) {
+    case 0:
+        { LaunchScope ls_(ctx, "boundary_scan");
+            boundary_scan_kernel<uint32_t><<<grid, kScanThreads, 0, ctx->stream>>>(
+                nullptr, in_group, flags, out_group, seg_start, n, tile_counter, (unsigned long long *)lb, epoch,
+                d_count, ctx->d_status);
+        }
+        break;
+    case 1:
+        { LaunchScope ls_(ctx, "boundary_scan");
+            boundary_scan_kernel<uint8_t><<<grid, kScanThreads, 0, ctx->stream>>>(
+                (const uint8_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
+                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
+        }
+        break;
+    case 2:
+        { LaunchScope ls_(ctx, "boundary_scan");
+            boundary_scan_kernel<uint16_t><<<grid, kScanThreads, 0, ctx->stream>>>(
+                (const uint16_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
+                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
+        }
+        break;
+    case 4:
+        { LaunchScope ls_(ctx, "boundary_scan");
+            boundary_scan_kernel<uint32_t><<<grid, kScanThreads, 0, ctx->stream>>>(
+                (const uint32_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
+                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
+        }
+        break;
+    case 8:
+        { LaunchScope ls_(ctx, "boundary_scan");
+            boundary_scan_kernel<uint64_t><<<grid, kScanThreads, 0, ctx->stream>>>(
+                (const uint64_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
+                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
+        }
+        break;
+    default:
+        return set_error(ctx, FMCS_E_INVAL, "boundary scan: bad key width");
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "boundary scan launch");
+}
+
+}  // namespace
+
+int launch_group_ids(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
+                     uint32_t *out_group, uint64_t n, uint32_t *d_ngroups)
+{
+    return run_boundary_scan(ctx, keys, key_bytes, in_group, nullptr, out_group, nullptr, n, d_ngroups);
+}
+
+int launch_segments(fmcs_ctx *ctx, const uint32_t *in_group, uint32_t *seg_start, uint32_t *d_nseg,
+                    uint64_t n)
+{
+    return run_boundary_scan(ctx, nullptr, 0, in_group, nullptr, nullptr, seg_start, n, d_nseg);
+}
+
+int launch_group_ids_segments(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
+                              uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *d_count)
+{
+    return run_boundary_scan(ctx, keys, key_bytes, in_group, nullptr, out_group, seg_start, n, d_count);
+}
+
+namespace {
+__global__ void iota_kernel(uint32_t *v, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        v[i] = (uint32_t)i;
+}
+}  // namespace
+
+int launch_iota(fmcs_ctx *ctx, uint32_t *v, uint64_t n)
+{
+    if (n == 0) return FMCS_OK;
+    { LaunchScope ls_(ctx, "iota");
+        iota_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(v, n);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "iota launch");
+}
+
+int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64_t n, uint32_t *d_count)
+{
+    return run_boundary_scan(ctx, nullptr, 0, nullptr, flags, rank, nullptr, n, d_count);
+}
+
+}  // namespace fmcs

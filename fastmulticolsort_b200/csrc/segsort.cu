@@ -1,0 +1,766 @@
+// segsort.cu -- (b) the per-round sort: a stable, segmented radix sort of
+// (bank key, oid) pairs in HBM.
+//
+// Reference: Composer::sortByGroup<T> (src/composer.cpp:1222-1408) walks the
+// previous round's groups and calls subsort -> Mergesort::avxmergesort_anytype
+// (src/mergesort.h:2878-3096) once per group: block sorts with AVX2 bitonic
+// networks, then 2-way merges, mallocing four buffers per group.  Round 0 is
+// one group of n rows.
+//
+// B200 design.  Every group is a segment [start, start+len) that is sorted in
+// place (segments never move).  Segments are binned by size:
+//   tier A  len <= 128   one warp per segment, LSD radix in registers/smem
+//   tier B  len <= 1024  one 128-thread CTA per segment, LSD radix in smem
+//   tier C  len <= 4096  one 256-thread CTA per segment, LSD radix in smem
+//   large   len >  4096  MSD radix levels: per-segment digit histogram, then a
+//                        onesweep-style stable scatter with a decoupled
+//                        look-back chained over the segment's tiles; every
+//                        non-empty bucket becomes a child segment with 8 bits
+//                        fewer, re-binned into the tiers above.
+// Each key is ranked by warp-level multi-split (match.any + popc) so every
+// pass is stable; the MSD scatter is stable too, so the whole sort is stable:
+// ties keep the oid order of the input, which is what the reference gives once
+// its ties are canonicalised to ascending oid.  Rows move only through HBM in
+// the large tier; a tier-A/B/C segment is read once and written once.
+//
+// Data sources of a segment: BUF0 (final buffer: the caller's order array and
+// the sorted-key array), BUF1 (work buffer), EXT (the round's input: the bank
+// gathered through the previous order, Composer::BATproject at
+// src/composer.cpp:608-628, or the bank itself with iota oids in round 0).
+#include "device_common.cuh"
+#include "fmcs_internal.h"
+
+#include <algorithm>
+
+namespace fmcs {
+
+namespace {
+
+constexpr uint32_t kSrcBuf0 = 0;
+constexpr uint32_t kSrcBuf1 = 1;
+constexpr uint32_t kSrcExt = 2;
+constexpr uint32_t kSkipBit = 0x100;
+
+constexpr int kCapA = 128;   // 32 lanes x 4 items
+constexpr int kItemsA = 4;
+constexpr int kNtB = 128, kItB = 8, kCapB = kNtB * kItB;    // 1024
+constexpr int kNtC = 256, kItC = 16, kCapC = kNtC * kItC;   // 4096
+constexpr int kNtM = 256, kItM = 16, kTileM = kNtM * kItM;  // MSD tile, 4096
+
+// counters slot words
+constexpr int kCtrMsdTile = 1;
+constexpr int kCtrLarge0 = 2;   // + level parity
+constexpr int kCtrLocalA = 4;
+constexpr int kCtrLocalB = 5;
+constexpr int kCtrLocalC = 6;
+constexpr int kCtrCopy = 7;
+constexpr int kCtrWords = 16;
+
+struct LargeSeg {
+    uint32_t start, len, shift, src;
+};
+
+template <typename K>
+struct Bufs {
+    K *k0, *k1;
+    uint32_t *v0, *v1;
+    const K *ext_bank;
+    const uint32_t *ext_order;   // NULL: iota
+};
+
+template <typename K>
+__device__ __forceinline__ void load_kv(const Bufs<K> &b, uint32_t src, uint64_t i, K &k, uint32_t &v)
+{
+    if (src == kSrcExt) {
+        if (b.ext_order) {
+            v = b.ext_order[i];
+            k = b.ext_bank[v];
+        } else {
+            v = (uint32_t)i;
+            k = b.ext_bank[i];
+        }
+    } else if (src == kSrcBuf1) {
+        k = b.k1[i];
+        v = b.v1[i];
+    } else {
+        k = b.k0[i];
+        v = b.v0[i];
+    }
+}
+
+template <typename K>
+__device__ __forceinline__ K load_k(const Bufs<K> &b, uint32_t src, uint64_t i)
+{
+    if (src == kSrcExt) return b.ext_order ? b.ext_bank[b.ext_order[i]] : b.ext_bank[i];
+    return src == kSrcBuf1 ? b.k1[i] : b.k0[i];
+}
+
+__device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32_t shift, uint32_t src)
+{
+    return make_uint2(start, len | (shift << 16) | (src << 24));
+}
+
+// Route a segment (child or initial) to its tier.  Segments that need no
+// sorting (one row, or no key bits left) only need to reach BUF0.
+__device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
+                                              uint32_t *ctr, int large_ctr, LargeSeg *large_out,
+                                              uint2 *la, uint2 *lb, uint2 *lc, LargeSeg *copy_out)
+{
+    if (len == 0) return;
+    if (len == 1 || shift == 0) {
+        if (src != kSrcBuf0) {
+            uint32_t slot = atomicAdd(&ctr[kCtrCopy], 1u);
+            copy_out[slot] = LargeSeg{start, len, 0, src};
+        }
+        return;
+    }
+    if (len <= (uint32_t)kCapA) {
+        la[atomicAdd(&ctr[kCtrLocalA], 1u)] = pack_local(start, len, shift, src);
+    } else if (len <= (uint32_t)kCapB) {
+        lb[atomicAdd(&ctr[kCtrLocalB], 1u)] = pack_local(start, len, shift, src);
+    } else if (len <= (uint32_t)kCapC) {
+        lc[atomicAdd(&ctr[kCtrLocalC], 1u)] = pack_local(start, len, shift, src);
+    } else {
+        large_out[atomicAdd(&ctr[large_ctr], 1u)] = LargeSeg{start, len, shift, src};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// classification of the round's initial segments
+// ---------------------------------------------------------------------------
+template <typename K>
+__global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_start, const uint32_t *d_nseg,
+                                uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, uint2 *la,
+                                uint2 *lb, uint2 *lc, LargeSeg *copy_out)
+{
+    const uint32_t nseg = seg_start ? *d_nseg : 1u;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+        const uint32_t start = seg_start ? seg_start[s] : 0u;
+        const uint32_t end = seg_start ? seg_start[s + 1] : (uint32_t)n;
+        const uint32_t len = end - start;
+        if (len == 1) {
+            // A one-row segment keeps its position: copy it straight to BUF0.
+            K k;
+            uint32_t v;
+            load_kv(b, kSrcExt, start, k, v);
+            b.k0[start] = k;
+            b.v0[start] = v;
+            continue;
+        }
+        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, la, lb, lc, copy_out);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MSD level kernels (large segments)
+// ---------------------------------------------------------------------------
+// Exclusive prefix of the tile counts of the level's large segments (one CTA).
+__global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs, const uint32_t *d_nseg,
+                                                           uint32_t *tile_prefix)
+{
+    __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t carry;
+    const uint32_t nseg = *d_nseg;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nseg; base += blockDim.x) {
+        const uint32_t s = base + threadIdx.x;
+        const uint32_t c = s < nseg ? (segs[s].len + kTileM - 1) / kTileM : 0u;
+        uint32_t incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if ((int)lane_id() >= o) incl += y;
+        }
+        if (lane_id() == 31) warp_sums[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            uint32_t v = threadIdx.x < blockDim.x / 32 ? warp_sums[threadIdx.x] : 0u;
+            uint32_t vi = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xFFFFFFFFu, vi, o);
+                if ((int)threadIdx.x >= o) vi += y;
+            }
+            warp_sums[threadIdx.x] = vi - v;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + warp_sums[threadIdx.x >> 5] + incl - c;
+        if (s < nseg) tile_prefix[s] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + c;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tile_prefix[nseg] = carry;
+}
+
+__global__ void zero_hist_kernel(uint32_t *hist, const uint32_t *d_nseg)
+{
+    const uint64_t total = (uint64_t)(*d_nseg) * kRadix;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        hist[i] = 0;
+}
+
+__device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
+{
+    uint32_t lo = 0, hi = nseg;  // tile_prefix[lo] <= t < tile_prefix[hi]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (tile_prefix[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
+                                                        const uint32_t *tile_prefix, uint32_t *hist)
+{
+    __shared__ uint32_t sh[kRadix];
+    const uint32_t nseg = *d_nseg;
+    if (nseg == 0) return;
+    const uint32_t T = tile_prefix[nseg];
+    for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
+        const uint32_t s = find_segment(tile_prefix, nseg, t);
+        const LargeSeg sg = segs[s];
+        const uint32_t k = t - tile_prefix[s];
+        const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
+        const uint32_t lo = sg.shift - width;
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) sh[d] = 0;
+        __syncthreads();
+        const uint64_t beg = (uint64_t)sg.start + (uint64_t)k * kTileM;
+        const uint64_t end = min((uint64_t)sg.start + sg.len, beg + kTileM);
+        for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+            const K key = load_k(b, sg.src, i);
+            atomicAdd(&sh[digit_of(key, lo, width)], 1u);
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x)
+            if (sh[d]) atomicAdd(&hist[(uint64_t)s * kRadix + d], sh[d]);
+        __syncthreads();
+    }
+}
+
+// Per large segment: exclusive digit offsets, skip detection, children.
+__global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const uint32_t *d_nseg,
+                                                          uint32_t *hist, uint32_t *ctr, int next_large_ctr,
+                                                          LargeSeg *large_next, uint2 *la, uint2 *lb,
+                                                          uint2 *lc, LargeSeg *copy_out)
+{
+    __shared__ uint32_t cnt[kRadix];
+    __shared__ uint32_t tmp[kRadix / 32 + 1];
+    __shared__ uint32_t s_skip;
+    const uint32_t nseg = *d_nseg;
+    for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
+        const LargeSeg sg = segs[s];
+        const uint32_t d = threadIdx.x;
+        const uint32_t c = hist[(uint64_t)s * kRadix + d];
+        cnt[d] = c;
+        if (d == 0) s_skip = 0;
+        __syncthreads();
+        if (c == sg.len) s_skip = 1;   // every row has this digit: the pass is the identity
+        uint32_t total;
+        block_exclusive_scan_radix<kRadix>(cnt, tmp, &total);
+        const uint32_t off = cnt[d];
+        hist[(uint64_t)s * kRadix + d] = off;
+        const bool skip = s_skip != 0;
+        const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
+        const uint32_t child_shift = sg.shift - width;
+        const uint32_t child_src = skip ? sg.src : (sg.src == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
+        if (c > 0)
+            route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, la, lb, lc,
+                          copy_out);
+        if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
+        __syncthreads();
+    }
+}
+
+template <typename K>
+struct MsdSmem {
+    uint32_t whist[kNtM / 32][kRadix];
+    uint32_t total[kRadix];
+    uint32_t doff[kRadix];       // tile-local exclusive digit offsets
+    long long gdst[kRadix];      // global destination base per digit
+    uint32_t tmp[kNtM / 32 + 1];
+    uint32_t tile, seg;
+    K keys[kTileM];
+    uint32_t vals[kTileM];
+};
+
+template <typename K>
+__global__ void __launch_bounds__(kNtM) msd_scatter_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
+                                                           const uint32_t *tile_prefix, const uint32_t *offs,
+                                                           uint32_t *tile_counter, unsigned long long *lookback,
+                                                           uint32_t epoch, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MsdSmem<K> &sm = *reinterpret_cast<MsdSmem<K> *>(smem_raw);
+    const uint32_t nseg = *d_nseg;
+    if (nseg == 0) return;
+    const uint32_t T = tile_prefix[nseg];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        if (threadIdx.x == 0) sm.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const uint32_t t = sm.tile;
+        if (t >= T) break;
+        const uint32_t s = find_segment(tile_prefix, nseg, t);
+        const LargeSeg sg = segs[s];
+        if (sg.src & kSkipBit) {
+            __syncthreads();
+            continue;
+        }
+        const uint32_t k = t - tile_prefix[s];
+        const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
+        const uint32_t lo = sg.shift - width;
+        const uint64_t tbeg = (uint64_t)sg.start + (uint64_t)k * kTileM;
+        const uint64_t send = (uint64_t)sg.start + sg.len;
+        const uint32_t cnt = (uint32_t)min((uint64_t)kTileM, send - tbeg);
+        for (int d = lane; d < kRadix; d += 32) sm.whist[warp][d] = 0;
+        __syncwarp();
+
+        K key[kItM];
+        uint32_t val[kItM];
+        uint32_t rank[kItM];
+        uint32_t dig[kItM];
+        const uint32_t wbase = warp * (kItM * 32);
+#pragma unroll
+        for (int j = 0; j < kItM; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (p < cnt) load_kv(b, sg.src, tbeg + p, key[j], val[j]);
+            else { key[j] = 0; val[j] = 0; }
+        }
+#pragma unroll
+        for (int j = 0; j < kItM; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            dig[j] = digit_of(key[j], lo, width);
+            rank[j] = wlms_rank(dig[j], p < cnt, sm.whist[warp]);
+        }
+        __syncthreads();
+        // per digit: exclusive over warps, tile total
+        for (int d = threadIdx.x; d < kRadix; d += kNtM) {
+            uint32_t run = 0;
+#pragma unroll
+            for (int w = 0; w < kNtM / 32; ++w) {
+                const uint32_t c = sm.whist[w][d];
+                sm.whist[w][d] = run;
+                run += c;
+            }
+            sm.total[d] = run;
+            sm.doff[d] = run;
+            unsigned long long *mine = &lookback[(uint64_t)t * kRadix + d];
+            st_volatile_u64(mine, lb_word(epoch, k == 0 ? kFlagInclusive : kFlagAggregate, run));
+        }
+        __syncthreads();
+        uint32_t tot;
+        block_exclusive_scan_radix<kNtM>(sm.doff, sm.tmp, &tot);
+        // decoupled look-back along the segment's tiles
+        for (int d = threadIdx.x; d < kRadix; d += kNtM) {
+            uint32_t excl = 0;
+            if (k > 0) {
+                int64_t p = (int64_t)t - 1;
+                for (;;) {
+                    const unsigned long long w = lb_wait(&lookback[(uint64_t)p * kRadix + d], epoch, status);
+                    excl += (uint32_t)w;
+                    if (((uint32_t)(w >> 32) & 3u) == kFlagInclusive) break;
+                    --p;
+                }
+                st_volatile_u64(&lookback[(uint64_t)t * kRadix + d],
+                                lb_word(epoch, kFlagInclusive, excl + sm.total[d]));
+            }
+            sm.gdst[d] = (long long)sg.start + (long long)offs[(uint64_t)s * kRadix + d] + (long long)excl -
+                         (long long)sm.doff[d];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kItM; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (p < cnt) {
+                const uint32_t pos = sm.doff[dig[j]] + sm.whist[warp][dig[j]] + rank[j];
+                sm.keys[pos] = key[j];
+                sm.vals[pos] = val[j];
+            }
+        }
+        __syncthreads();
+        K *dk = (sg.src == kSrcBuf1) ? b.k0 : b.k1;
+        uint32_t *dv = (sg.src == kSrcBuf1) ? b.v0 : b.v1;
+        for (uint32_t i = threadIdx.x; i < cnt; i += kNtM) {
+            const K kk = sm.keys[i];
+            const long long o = sm.gdst[digit_of(kk, lo, width)] + (long long)i;
+            dk[o] = kk;
+            dv[o] = sm.vals[i];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// local tiers
+// ---------------------------------------------------------------------------
+// Block-per-segment LSD radix sort over bits [0, shift), stable.
+template <typename K, int NT, int IT>
+struct BlockSmem {
+    uint32_t whist[NT / 32][kRadix];
+    uint32_t doff[kRadix];
+    uint32_t tmp[NT / 32 + 1];
+    uint32_t flag;
+    K keys[NT * IT];
+    uint32_t vals[NT * IT];
+};
+
+template <typename K, int NT, int IT>
+__global__ void __launch_bounds__(NT) block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BlockSmem<K, NT, IT> &sm = *reinterpret_cast<BlockSmem<K, NT, IT> *>(smem_raw);
+    const uint32_t count = *d_count;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t wbase = warp * (IT * 32);
+    for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
+        const uint2 ent = list[e];
+        const uint32_t start = ent.x;
+        const uint32_t len = ent.y & 0xFFFFu;
+        const uint32_t shift = (ent.y >> 16) & 0x7Fu;
+        const uint32_t src = (ent.y >> 24) & 3u;
+        K key[IT];
+        uint32_t val[IT];
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
+            else { key[j] = 0; val[j] = 0; }
+        }
+        for (uint32_t lo = 0; lo < shift; lo += kRadixBits) {
+            const uint32_t width = min((uint32_t)kRadixBits, shift - lo);
+            for (int d = lane; d < kRadix; d += 32) sm.whist[warp][d] = 0;
+            if (threadIdx.x == 0) sm.flag = 0;
+            __syncthreads();
+            uint32_t rank[IT];
+            uint32_t dig[IT];
+#pragma unroll
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t p = wbase + j * 32 + lane;
+                dig[j] = digit_of(key[j], lo, width);
+                rank[j] = wlms_rank(dig[j], p < len, sm.whist[warp]);
+            }
+            __syncthreads();
+            for (int d = threadIdx.x; d < kRadix; d += NT) {
+                uint32_t run = 0;
+#pragma unroll
+                for (int w = 0; w < NT / 32; ++w) {
+                    const uint32_t c = sm.whist[w][d];
+                    sm.whist[w][d] = run;
+                    run += c;
+                }
+                sm.doff[d] = run;
+                if (run == len) sm.flag = 1;   // one digit holds every row: identity pass
+            }
+            __syncthreads();
+            const bool identity = sm.flag != 0;
+            __syncthreads();
+            if (identity) continue;   // uniform across the block
+            uint32_t tot;
+            block_exclusive_scan_radix<NT>(sm.doff, sm.tmp, &tot);
+#pragma unroll
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t p = wbase + j * 32 + lane;
+                if (p < len) {
+                    const uint32_t pos = sm.doff[dig[j]] + sm.whist[warp][dig[j]] + rank[j];
+                    sm.keys[pos] = key[j];
+                    sm.vals[pos] = val[j];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t p = wbase + j * 32 + lane;
+                if (p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
+            }
+            __syncthreads();
+        }
+        // every load of this segment is done (barriers above, or below for
+        // shift-free copies) before the first store into BUF0, which may alias
+        // the EXT oids of the same range
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (p < len) {
+                b.k0[(uint64_t)start + p] = key[j];
+                b.v0[(uint64_t)start + p] = val[j];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Warp-per-segment LSD radix sort (len <= 32 * kItemsA), stable.
+template <typename K>
+struct WarpSmem {
+    uint32_t hist[kRadix];
+    K keys[32 * kItemsA];
+    uint32_t vals[32 * kItemsA];
+};
+
+template <typename K>
+__global__ void __launch_bounds__(256) warp_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
+{
+    __shared__ WarpSmem<K> all[8];
+    WarpSmem<K> &sm = all[threadIdx.x >> 5];
+    const uint32_t count = *d_count;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = gridDim.x * 8;
+    for (uint32_t e = blockIdx.x * 8 + (threadIdx.x >> 5); e < count; e += nwarps) {
+        const uint2 ent = list[e];
+        const uint32_t start = ent.x;
+        const uint32_t len = ent.y & 0xFFFFu;
+        const uint32_t shift = (ent.y >> 16) & 0x7Fu;
+        const uint32_t src = (ent.y >> 24) & 3u;
+        K key[kItemsA];
+        uint32_t val[kItemsA];
+#pragma unroll
+        for (int j = 0; j < kItemsA; ++j) {
+            const uint32_t p = j * 32 + lane;
+            if (p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
+            else { key[j] = 0; val[j] = 0; }
+        }
+        for (uint32_t lo = 0; lo < shift; lo += kRadixBits) {
+            const uint32_t width = min((uint32_t)kRadixBits, shift - lo);
+#pragma unroll
+            for (int d = lane; d < kRadix; d += 32) sm.hist[d] = 0;
+            __syncwarp();
+            uint32_t rank[kItemsA];
+            uint32_t dig[kItemsA];
+#pragma unroll
+            for (int j = 0; j < kItemsA; ++j) {
+                const uint32_t p = j * 32 + lane;
+                dig[j] = digit_of(key[j], lo, width);
+                rank[j] = wlms_rank(dig[j], p < len, sm.hist);
+            }
+            // warp exclusive scan of the 256 counters (8 per lane)
+            uint32_t c[8];
+            uint32_t sum = 0;
+            bool full = false;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                c[i] = sm.hist[lane * 8 + i];
+                full |= (c[i] == len);
+                sum += c[i];
+            }
+            if (__any_sync(0xFFFFFFFFu, full)) continue;   // identity pass
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            uint32_t run = incl - sum;
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                sm.hist[lane * 8 + i] = run;
+                run += c[i];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < kItemsA; ++j) {
+                const uint32_t p = j * 32 + lane;
+                if (p < len) {
+                    const uint32_t pos = sm.hist[dig[j]] + rank[j];
+                    sm.keys[pos] = key[j];
+                    sm.vals[pos] = val[j];
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < kItemsA; ++j) {
+                const uint32_t p = j * 32 + lane;
+                if (p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
+            }
+            __syncwarp();
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < kItemsA; ++j) {
+            const uint32_t p = j * 32 + lane;
+            if (p < len) {
+                b.k0[(uint64_t)start + p] = key[j];
+                b.v0[(uint64_t)start + p] = val[j];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Segments that need no sorting but sit outside BUF0: one warp per entry.
+template <typename K>
+__global__ void __launch_bounds__(256) copy_kernel(Bufs<K> b, const LargeSeg *list, const uint32_t *d_count)
+{
+    const uint32_t count = *d_count;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+    for (uint32_t e = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); e < count; e += nwarps) {
+        const LargeSeg sg = list[e];
+        for (uint32_t i = lane; i < sg.len; i += 32) {
+            const uint64_t r = (uint64_t)sg.start + i;
+            K k;
+            uint32_t v;
+            load_kv(b, sg.src & 3u, r, k, v);
+            b.k0[r] = k;
+            b.v0[r] = v;
+        }
+    }
+}
+
+template <typename F>
+int set_smem(fmcs_ctx *ctx, F *f, size_t bytes)
+{
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "cudaFuncSetAttribute");
+}
+
+#define FMCS_LAUNCH_CHECK(what)                                         \
+    do {                                                                \
+        cudaError_t e_ = cudaGetLastError();                            \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what);          \
+    } while (0)
+
+template <typename K>
+int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
+{
+    const uint64_t n = a.n;
+    cudaStream_t st = ctx->stream;
+    // buffers
+    Bufs<K> b;
+    b.ext_bank = (const K *)a.bank;
+    b.ext_order = a.order_in;
+    void *p = nullptr;
+    int rc;
+    if (a.keys_out) {
+        b.k0 = (K *)a.keys_out;
+    } else {
+        if ((rc = ws_get(ctx, kSlotKeys0, n * sizeof(K), &p))) return rc;
+        b.k0 = (K *)p;
+    }
+    b.v0 = a.order_out;
+    if ((rc = ws_get(ctx, kSlotKeys1, n * sizeof(K), &p))) return rc;
+    b.k1 = (K *)p;
+    if ((rc = ws_get(ctx, kSlotVals1, n * sizeof(uint32_t), &p))) return rc;
+    b.v1 = (uint32_t *)p;
+
+    // lists (capacities are bounds on disjoint segments of each tier's minimum size)
+    const uint64_t cap_large = n / (kCapC + 1) + 2;
+    const uint64_t cap_a = n / 2 + 2, cap_b = n / (kCapA + 1) + 2, cap_c = n / (kCapB + 1) + 2;
+    // copy entries: disjoint ranges; at most 256 children per large segment per
+    // level, so bounded by both n and (levels + 1) * 256 * cap_large
+    const uint64_t levels_max = (a.key_bits + kRadixBits - 1) / kRadixBits;
+    const uint64_t cap_copy = std::min<uint64_t>(n, (levels_max + 1) * kRadix * cap_large) + 2;
+    LargeSeg *large[2];
+    if ((rc = ws_get(ctx, kSlotLarge0, cap_large * sizeof(LargeSeg), &p))) return rc;
+    large[0] = (LargeSeg *)p;
+    if ((rc = ws_get(ctx, kSlotLarge1, cap_large * sizeof(LargeSeg), &p))) return rc;
+    large[1] = (LargeSeg *)p;
+    uint2 *la, *lb, *lc;
+    if ((rc = ws_get(ctx, kSlotLocalA, cap_a * sizeof(uint2), &p))) return rc;
+    la = (uint2 *)p;
+    if ((rc = ws_get(ctx, kSlotLocalB, cap_b * sizeof(uint2), &p))) return rc;
+    lb = (uint2 *)p;
+    if ((rc = ws_get(ctx, kSlotLocalC, cap_c * sizeof(uint2) + cap_copy * sizeof(LargeSeg), &p))) return rc;
+    lc = (uint2 *)p;
+    LargeSeg *copy_list = (LargeSeg *)((char *)p + ((cap_c * sizeof(uint2) + 15) & ~size_t(15)));
+    uint32_t *hist, *tile_prefix;
+    if ((rc = ws_get(ctx, kSlotSegHist, cap_large * kRadix * sizeof(uint32_t), &p))) return rc;
+    hist = (uint32_t *)p;
+    if ((rc = ws_get(ctx, kSlotTilePrefix, (cap_large + 1) * sizeof(uint32_t), &p))) return rc;
+    tile_prefix = (uint32_t *)p;
+    const uint64_t max_tiles = n / kTileM + cap_large + 1;
+    unsigned long long *lookback;
+    if ((rc = ws_get(ctx, kSlotLookback, max_tiles * kRadix * sizeof(unsigned long long), &p, true))) return rc;
+    lookback = (unsigned long long *)p;
+    uint32_t *ctr;
+    if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
+    ctr = (uint32_t *)p + 64;   // words 0..63 belong to other kernels
+    cudaMemsetAsync(ctr, 0, kCtrWords * sizeof(uint32_t), st);
+
+    const int sms = ctx->num_sms;
+    // classification of the initial segments
+    {
+        const uint32_t *seg_start = a.seg_start;
+        const uint32_t *d_nseg = a.d_nseg;
+        unsigned grid = seg_start ? (unsigned)std::min<uint64_t>((a.nseg_host + 255) / 256 + 1, (uint64_t)sms * 16)
+                                  : 1u;
+        if (seg_start && a.nseg_host == 0) grid = (unsigned)sms * 16;
+        { LaunchScope ls_(ctx, "classify");
+            classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], la, lb, lc,
+                                                     copy_list);
+        }
+        FMCS_LAUNCH_CHECK("classify");
+    }
+    // MSD levels
+    const int levels = (int)((a.key_bits + kRadixBits - 1) / kRadixBits);
+    const size_t msd_smem = sizeof(MsdSmem<K>);
+    if ((rc = set_smem(ctx, msd_scatter_kernel<K>, msd_smem))) return rc;
+    if (n > (uint64_t)kCapC) {
+        for (int lvl = 0; lvl < levels; ++lvl) {
+            const int cur = lvl & 1, nxt = cur ^ 1;
+            const uint32_t *d_cnt = &ctr[kCtrLarge0 + cur];
+            cudaMemsetAsync(&ctr[kCtrLarge0 + nxt], 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(&ctr[kCtrMsdTile], 0, sizeof(uint32_t), st);
+            { LaunchScope ls_(ctx, "tile_prefix");
+                tile_prefix_kernel<<<1, 1024, 0, st>>>(large[cur], d_cnt, tile_prefix);
+            }
+            { LaunchScope ls_(ctx, "zero_hist");
+                zero_hist_kernel<<<sms * 2, 256, 0, st>>>(hist, d_cnt);
+            }
+            { LaunchScope ls_(ctx, "msd_hist");
+                msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, large[cur], d_cnt, tile_prefix, hist);
+            }
+            { LaunchScope ls_(ctx, "msd_plan");
+                msd_plan_kernel<<<sms * 8, kRadix, 0, st>>>(large[cur], d_cnt, hist, ctr, kCtrLarge0 + nxt, large[nxt],
+                                                             la, lb, lc, copy_list);
+            }
+            { LaunchScope ls_(ctx, "msd_scatter");
+                msd_scatter_kernel<K><<<sms * 2, kNtM, msd_smem, st>>>(b, large[cur], d_cnt, tile_prefix, hist,
+                                                                         &ctr[kCtrMsdTile], lookback, ctx->epoch++,
+                                                                         ctx->d_status);
+            }
+            FMCS_LAUNCH_CHECK("msd level");
+        }
+    }
+    // local tiers
+    const size_t smem_b = sizeof(BlockSmem<K, kNtB, kItB>);
+    const size_t smem_c = sizeof(BlockSmem<K, kNtC, kItC>);
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB, kItB>, smem_b))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC, kItC>, smem_c))) return rc;
+    { LaunchScope ls_(ctx, "warp_sort");
+        warp_sort_kernel<K><<<sms * 16, 256, 0, st>>>(b, la, &ctr[kCtrLocalA]);
+    }
+    { LaunchScope ls_(ctx, "block_sort");
+        block_sort_kernel<K, kNtB, kItB><<<sms * 8, kNtB, smem_b, st>>>(b, lb, &ctr[kCtrLocalB]);
+    }
+    { LaunchScope ls_(ctx, "block_sort");
+        block_sort_kernel<K, kNtC, kItC><<<sms * 3, kNtC, smem_c, st>>>(b, lc, &ctr[kCtrLocalC]);
+    }
+    { LaunchScope ls_(ctx, "copy");
+        copy_kernel<K><<<sms * 4, 256, 0, st>>>(b, copy_list, &ctr[kCtrCopy]);
+    }
+    FMCS_LAUNCH_CHECK("local tiers");
+    return FMCS_OK;
+}
+
+}  // namespace
+
+int sort_segments(fmcs_ctx *ctx, const SortArgs &a)
+{
+    if (a.n == 0) return FMCS_OK;
+    if (a.key_bits == 0 || a.key_bits > 8 * a.bank_bytes)
+        return set_error(ctx, FMCS_E_INVAL, "sort: key_bits must be in 1..8*bank_bytes");
+    switch (a.bank_bytes) {
+    case 2: return sort_segments_t<uint16_t>(ctx, a);
+    case 4: return sort_segments_t<uint32_t>(ctx, a);
+    case 8: return sort_segments_t<uint64_t>(ctx, a);
+    default: return set_error(ctx, FMCS_E_INVAL, "sort: bank_bytes must be 2, 4 or 8");
+    }
+}
+
+}  // namespace fmcs

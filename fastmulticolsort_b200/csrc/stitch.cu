@@ -1,0 +1,153 @@
+// stitch.cu -- (a) bit stitching of one bank in ONE pass.
+//
+// The reference builds a bank slice by slice with whole-column AVX2 passes:
+// ShiftLeftBatch shifts the bank left by the next slice's width, then
+// AssembleFromColumn ORs in (src >> (origW - end)) & mask
+// (src/column.h:105-180, 208-1060; loop at src/stitch_composer.cpp:655-703).
+// That reads and writes the bank once per slice.  Here every thread owns four
+// consecutive rows, reads each source slice with one vector load per row
+// group, folds the slices in registers and writes the bank once: the kernel
+// moves exactly sum(source bytes) + bank bytes per row.
+#include "fmcs_internal.h"
+
+namespace fmcs {
+
+namespace {
+
+struct StitchParams {
+    StitchSlice s[kMaxSlices];
+    int ns;
+};
+
+__device__ __forceinline__ void load4(const void *base, uint32_t bytes, uint64_t row, bool vec,
+                                      uint64_t n, uint64_t v[4])
+{
+    if (vec) {
+        switch (bytes) {
+        case 1: {
+            uint32_t x = *reinterpret_cast<const uint32_t *>((const uint8_t *)base + row);
+            v[0] = x & 0xFF; v[1] = (x >> 8) & 0xFF; v[2] = (x >> 16) & 0xFF; v[3] = x >> 24;
+            return;
+        }
+        case 2: {
+            uint2 x = *reinterpret_cast<const uint2 *>((const uint16_t *)base + row);
+            v[0] = x.x & 0xFFFF; v[1] = x.x >> 16; v[2] = x.y & 0xFFFF; v[3] = x.y >> 16;
+            return;
+        }
+        case 4: {
+            uint4 x = *reinterpret_cast<const uint4 *>((const uint32_t *)base + row);
+            v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+            return;
+        }
+        default: {
+            const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>((const uint64_t *)base + row);
+            ulonglong2 a = p[0], b = p[1];
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+            return;
+        }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint64_t r = row + k;
+        if (r >= n) { v[k] = 0; continue; }
+        switch (bytes) {
+        case 1: v[k] = ((const uint8_t *)base)[r]; break;
+        case 2: v[k] = ((const uint16_t *)base)[r]; break;
+        case 4: v[k] = ((const uint32_t *)base)[r]; break;
+        default: v[k] = ((const uint64_t *)base)[r]; break;
+        }
+    }
+}
+
+template <typename B>
+__device__ __forceinline__ void store4(B *bank, uint64_t row, bool vec, uint64_t n, const uint64_t a[4])
+{
+    if (vec) {
+        if constexpr (sizeof(B) == 1) {
+            uint32_t x = (uint32_t)(a[0] & 0xFF) | (uint32_t)(a[1] & 0xFF) << 8 |
+                         (uint32_t)(a[2] & 0xFF) << 16 | (uint32_t)(a[3] & 0xFF) << 24;
+            *reinterpret_cast<uint32_t *>(bank + row) = x;
+        } else if constexpr (sizeof(B) == 2) {
+            uint2 x;
+            x.x = (uint32_t)(a[0] & 0xFFFF) | (uint32_t)(a[1] & 0xFFFF) << 16;
+            x.y = (uint32_t)(a[2] & 0xFFFF) | (uint32_t)(a[3] & 0xFFFF) << 16;
+            *reinterpret_cast<uint2 *>(bank + row) = x;
+        } else if constexpr (sizeof(B) == 4) {
+            *reinterpret_cast<uint4 *>(bank + row) =
+                make_uint4((uint32_t)a[0], (uint32_t)a[1], (uint32_t)a[2], (uint32_t)a[3]);
+        } else {
+            ulonglong2 *p = reinterpret_cast<ulonglong2 *>(bank + row);
+            p[0] = make_ulonglong2(a[0], a[1]);
+            p[1] = make_ulonglong2(a[2], a[3]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (row + k < n) bank[row + k] = (B)a[k];
+}
+
+template <typename B>
+__global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ StitchParams p, B *bank,
+                                                     uint64_t n, bool aligned)
+{
+    const uint64_t groups = (n + 3) / 4;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t row = g * 4;
+        const bool vec = aligned && row + 4 <= n;
+        uint64_t acc[4] = {0, 0, 0, 0};
+        for (int s = 0; s < p.ns; ++s) {
+            const StitchSlice sl = p.s[s];
+            uint64_t v[4];
+            load4(sl.src, sl.src_bytes, row, vec, n, v);
+            const uint64_t mask = sl.width >= 64 ? ~0ull : ((1ull << sl.width) - 1);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint64_t x = (v[k] >> sl.rshift) & mask;
+                acc[k] = (s == 0 || sl.width >= 64) ? x : ((acc[k] << sl.width) | x);
+            }
+        }
+        store4<B>(bank, row, vec, n, acc);
+    }
+}
+
+}  // namespace
+
+int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
+                  uint64_t n)
+{
+    if (ns < 1 || ns > kMaxSlices) return set_error(ctx, FMCS_E_INVAL, "stitch: 1..32 slices");
+    if (n == 0) return FMCS_OK;
+    StitchParams p;
+    bool aligned = ((uintptr_t)bank % 16) == 0;
+    for (int i = 0; i < ns; ++i) {
+        p.s[i] = sl[i];
+        aligned = aligned && ((uintptr_t)sl[i].src % 16) == 0;
+    }
+    p.ns = ns;
+    const uint64_t groups = (n + 3) / 4;
+    uint64_t blocks = (groups + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    switch (bank_bytes) {
+    case 1: { LaunchScope ls_(ctx, "stitch");
+        stitch_kernel<uint8_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint8_t *)bank, n, aligned);
+    } break;
+    case 2: { LaunchScope ls_(ctx, "stitch");
+        stitch_kernel<uint16_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint16_t *)bank, n, aligned);
+    } break;
+    case 4: { LaunchScope ls_(ctx, "stitch");
+        stitch_kernel<uint32_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint32_t *)bank, n, aligned);
+    } break;
+    case 8: { LaunchScope ls_(ctx, "stitch");
+        stitch_kernel<uint64_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint64_t *)bank, n, aligned);
+    } break;
+    default: return set_error(ctx, FMCS_E_INVAL, "stitch: bank_bytes must be 1, 2, 4 or 8");
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "stitch launch");
+}
+
+}  // namespace fmcs

@@ -1,0 +1,145 @@
+/*
+ * fmcs_capi.h -- C ABI of the B200 multi-column sort path.
+ *
+ * The reference (FastMultiColSort) has no FFI: it is a static C++ library whose
+ * swap points are the Composer virtuals SortAllColumns_Nonpack / HashAllColumns
+ * (src/composer.h:59-68) and StitchComposer::run_single_plan, which hard-codes a
+ * CPU ChainComposer (src/stitch_composer.cpp:745, 1009).  Each entry point below
+ * names the reference code it replaces.  The C++ classes in include/fmcs/ that
+ * mirror the reference's Column / ChainComposer / StitchComposer API sit on top
+ * of this ABI.
+ *
+ * Conventions
+ *   - Row ids (oids), order and group vectors are uint32 (surrogate_t,
+ *     src/params.h:9-13); n < 2^32.
+ *   - Banks are 1, 2, 4 or 8 bytes per row (sort rounds: 2, 4 or 8).
+ *   - Pointers may be device pointers or host pointers (pageable or pinned);
+ *     host data is staged through the context's device buffers, so a host
+ *     call pays its own copies.  Inputs are never modified.
+ *   - All calls are stream-ordered on the context's stream and return after the
+ *     results are complete (host outputs) or enqueued (device outputs; call
+ *     fmcs_synchronize before reading them from another stream).
+ *   - Status codes: FMCS_OK 0, FMCS_E_INVAL -1, FMCS_E_OOM -2,
+ *     FMCS_E_TIMEOUT -3 (a bounded device-side wait gave up), FMCS_E_CUDA -4.
+ *     fmcs_last_error() gives the message of the last failure.
+ *   - A context is not thread-safe; use one per host thread.
+ */
+#ifndef FMCS_CAPI_H
+#define FMCS_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FMCS_API __attribute__((visibility("default")))
+#else
+#define FMCS_API
+#endif
+
+#define FMCS_OK 0
+#define FMCS_E_INVAL (-1)
+#define FMCS_E_OOM (-2)
+#define FMCS_E_TIMEOUT (-3)
+#define FMCS_E_CUDA (-4)
+
+typedef struct fmcs_ctx fmcs_ctx;
+
+/* Create a context on `device`.  hbm_budget_bytes caps the context's device
+ * workspace (0 = no cap).  Replaces the reference's per-call malloc_aligned
+ * (src/common.h:18-31). */
+FMCS_API int fmcs_create(fmcs_ctx **ctx, int device, size_t hbm_budget_bytes);
+FMCS_API void fmcs_destroy(fmcs_ctx *ctx);
+FMCS_API const char *fmcs_last_error(const fmcs_ctx *ctx);
+/* Wait for all work of the context (its stream). */
+FMCS_API int fmcs_synchronize(fmcs_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work against it. */
+FMCS_API void *fmcs_stream(fmcs_ctx *ctx);
+/* Device bytes the context currently holds in its workspace. */
+FMCS_API size_t fmcs_workspace_bytes(const fmcs_ctx *ctx);
+
+/* Kernel profiler (no reference counterpart; the reference times sections with
+ * rdtsc, src/hybrid_timer.h:16-56).  While enabled, every kernel launch of the
+ * context is bracketed by CUDA events on its stream.  fmcs_profile_report
+ * synchronizes and writes a JSON object {"kernel": {"launches": n, "ms": t}}
+ * for the launches since the last report, then forgets them. */
+FMCS_API int fmcs_profile(fmcs_ctx *ctx, int enable);
+FMCS_API int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len);
+/* Number of kernels this context has launched since it was created. */
+FMCS_API unsigned long long fmcs_launch_count(const fmcs_ctx *ctx);
+
+/* One slice of a source column: bits [start, end], 1-based from the MSB of the
+ * declared width src_bits (construct_entry_t, src/types.h:42-46). */
+typedef struct {
+    const void *src;
+    uint32_t src_bytes; /* 1, 2, 4 or 8 */
+    uint32_t src_bits;  /* declared width of the source column, <= 8*src_bytes */
+    uint32_t start;
+    uint32_t end;
+} fmcs_slice;
+
+/* (a) Bit stitching of one bank: ShiftLeftBatch + AssembleFromColumn for every
+ * slice (src/column.h:105-180, 208-1060; loop at src/stitch_composer.cpp:655-703).
+ * bank: n rows of bank_bytes. */
+FMCS_API int fmcs_stitch(fmcs_ctx *ctx, const fmcs_slice *slices, uint32_t nslices,
+                void *bank, uint32_t bank_bytes, uint64_t n);
+
+/* (c) out[i] = bank[order[i]] (Composer::BATproject, src/composer.cpp:608-628). */
+FMCS_API int fmcs_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes,
+                const uint32_t *order, void *out, uint64_t n);
+
+/* (b)+(d) One sort round (Composer::sortByGroup<T>, src/composer.cpp:1222-1408,
+ * with subsort (:558-589) and extractGroupInfo (:630-678)).
+ *   in_group == NULL: round 0; order is output only (the reference starts
+ *                     from iota, :60-63) and receives the stable argsort of bank.
+ *   in_group != NULL: order is input and output; the round sorts bank[order[i]]
+ *                     stably inside every run of equal in_group.
+ *   key_bits:         significant bits of the bank (1..8*bank_bytes); bits above
+ *                     must be zero.
+ *   out_group:        dense group ids in sorted order, or NULL for a last round
+ *                     (isLastRound, :1388-1390).
+ *   sorted_bank:      optional (NULL): receives the sorted bank values.
+ *   ngroups:          optional: receives the group count (0 if out_group NULL).
+ * Ties keep their input order, which equals the reference's result with ties
+ * canonicalised to ascending oid. */
+FMCS_API int fmcs_sort_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits,
+                    uint32_t *order, const uint32_t *in_group, uint32_t *out_group,
+                    void *sorted_bank, uint64_t n, uint32_t *ngroups);
+
+/* (e) One hash-grouping round (Composer::hashByGroup_reordered<T>,
+ * src/composer.cpp:814-976; Hashing::subgroup_range, src/hashing.h:289-385;
+ * Partition::histogram_based_reordering, src/partition.h:44-161).
+ *   in_group == NULL: round 0, order output only (starts as iota).
+ *   group ids are dense, numbered by first appearance inside each run of equal
+ *   in_group, runs in position order (startGrpIdx accumulates).
+ *   last_round == 0:  order and out_group are re-clustered by group id, stably.
+ *   last_round != 0:  order is left as is; out_group gets the per-position group
+ *                     ids (intermediate_group_idx).
+ * The reference's remainder-block defect (src/hashing.h:345) is not reproduced. */
+FMCS_API int fmcs_hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes,
+                    uint32_t *order, const uint32_t *in_group, uint32_t *out_group,
+                    uint64_t n, int last_round, uint32_t *ngroups);
+
+/* Whole massaged plan (StitchComposer::run_single_plan,
+ * src/stitch_composer.cpp:555-806 + multiRoundSorting, src/composer.cpp:48-135,
+ * or with hash != 0 run_single_plan_hash, :808-1079 + multiRoundHashing_reordered,
+ * src/composer.cpp:137-227).
+ *   cols[c]:    n rows of col_bytes[c] bytes, declared width bw[c];
+ *               col_order (NULL = 0..ncols-1) is the reference's columnOrder.
+ *   split:      bank widths in bits (sum == sum of bw), e.g. {50} or {6,44}.
+ *   order_out:  final order; group_out: group vector of the last round
+ *               (always computed; NULL to skip).  ngroups optional. */
+FMCS_API int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes,
+                  const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
+                  const uint32_t *split, uint32_t nbanks, uint64_t n, int hash,
+                  uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMCS_CAPI_H */
