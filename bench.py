@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 multi-column sort path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fmcs|reference]
+
+Workload (one step): the massaged single-round plan [50] over 16,777,216 rows
+of 17-bit codes (8,192 distinct values, uint32) and 33-bit codes (uint64):
+stitch both columns into one 64-bit bank, sort (bank, oid) stably, emit the
+group ids -- StitchComposer::run_single_plan with split {50}.  Inputs are
+seeded synthetic data with the shapes of the reference's 17B33 experiment.
+
+value:  M rows/s with the columns resident in HBM (device pointers through
+        the C ABI), N GPUs = N independent replicas (weak scaling).
+e2e:    the same call with pinned HOST buffers: the host->device copy of the
+        columns and the device->host copy of order + group ids are inside the
+        timed region.
+roofline: the dominant kernel's algorithmic bytes per launch / its CUDA-event
+        launch time, timed inside the library on the stream it runs on.
+cpu_baseline: the reference's own composer (oracle/_ref, compiled from the
+        reference sources) on the same workload, 1 host thread (its only live
+        sort path is single-threaded).
+
+--impl reference times that CPU implementation alone (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("M rows/s & HBM GB/s vs peak: batched/massaged vs plain GPU sort; "
+          "p50/p99 latency")
+N_ROWS = 16_777_216
+SPLIT = [50]
+PLAIN_SPLIT = [17, 33]
+WORKLOAD = "17B33 massaged single-round plan [50], 16,777,216 rows"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------------------
+# byte model (algorithmic bytes per row): stitch = sources + bank;
+# sort pass = 2 * (bank + oid); histogram = bank; boundary = bank + 4 (round 0)
+# or bank + 8 (later rounds); gather (rounds > 0) = 4 + 2 * bank.
+# --------------------------------------------------------------------------
+def bank_bytes(bits: int) -> int:
+    """Bank width of a sort-path split entry (src/stitch_composer.cpp:622-650)."""
+    return 2 if bits <= 16 else (4 if bits <= 32 else 8)
+
+
+def plan_model_bytes_per_row(col_bytes, bw, split):
+    per_row = 0.0
+    # stitch counted unless the bank is exactly one column at its own width
+    bit = 0
+    starts = np.cumsum([0] + list(bw))
+    for r, w in enumerate(split):
+        B = bank_bytes(w)
+        lo, hi = bit, bit + w
+        src = [c for c in range(len(bw)) if starts[c] < hi and starts[c + 1] > lo]
+        exact = len(src) == 1 and starts[src[0]] == lo and starts[src[0] + 1] == hi and col_bytes[src[0]] == B
+        if not exact:
+            per_row += sum(col_bytes[c] for c in src) + B
+        if r > 0:
+            per_row += 4 + 2 * B
+        per_row += -(-w // 8) * 2 * (B + 4) + B
+        per_row += B + (4 if r == 0 else 8)
+        bit = hi
+    return per_row
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="fmcs_clocks_", suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sm, mx, reasons = [], [], set()
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, flag in zip(self.NAMES, parts[5:9]):
+                    if flag.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def visible_gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# --------------------------------------------------------------------------
+# distributed plumbing (replicas only: no collective on the data path)
+# --------------------------------------------------------------------------
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_done(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference's own composer (or the oracle port)
+# --------------------------------------------------------------------------
+def cpu_baseline(cols, bw, split, runs: int):
+    from oracle import oracle as O
+    n = cols[0].shape[0]
+    if O.ref_available():
+        secs = []
+        for _ in range(runs):
+            _, _, s = O.ref_run_plan_sort(cols, bw, split, final_groups=False)
+            secs.append(s)
+        kind = "reference"
+    else:
+        secs = []
+        for _ in range(runs):
+            t = time.perf_counter()
+            O.run_plan_sort(cols, bw, split)
+            secs.append(time.perf_counter() - t)
+        kind = "port"
+    mean = sum(secs) / len(secs)
+    return {"value": n / mean / 1e6, "unit": "M rows/s", "cores": 1, "kind": kind,
+            "sample": f"{runs} runs of the full {n:,}-row plan {split} (stitch + sort rounds), "
+                      f"mean {mean:.3f} s per run, 1 thread",
+            "seconds": secs}
+
+
+def run_reference(args):
+    rank, world, local = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return 0
+    from fastmulticolsort_b200 import workloads as W
+    from oracle import oracle as O
+    cols, bw = W.cols_17b33(N_ROWS)
+    kind = "reference" if O.ref_available() else "port"
+    secs = []
+    for i in range(args.warmup + args.steps):
+        if kind == "reference":
+            _, _, s = O.ref_run_plan_sort(cols, bw, SPLIT, final_groups=False)
+        else:
+            t = time.perf_counter()
+            O.run_plan_sort(cols, bw, SPLIT)
+            s = time.perf_counter() - t
+        if i >= args.warmup:
+            secs.append(s)
+    mean = sum(secs) / len(secs)
+    value = N_ROWS / mean / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "M rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded PRNG)",
+        "config": {"workload": WORKLOAD, "rows": N_ROWS, "plan": SPLIT},
+        "cpu_baseline": {"value": value, "unit": "M rows/s", "cores": 1, "kind": kind,
+                         "sample": f"each step one full {N_ROWS:,}-row plan {SPLIT} through the "
+                                   f"{'reference composer (oracle/_ref)' if kind == 'reference' else 'oracle port'}"
+                                   ", 1 thread (the reference's only live sort path is single-threaded)"},
+        "e2e": {"value": value, "unit": "M rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def kernel_bytes_per_unit(name: str, bank_bytes: int):
+    """Algorithmic bytes per row for kernels whose launches report rows."""
+    if name == "msd_scatter":
+        return 2 * (bank_bytes + 4)
+    return None
+
+
+def time_steps(ctx, stream, fn, steps):
+    import torch
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for k in range(steps):
+        fn()
+        evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    total = evs[0].elapsed_time(evs[-1])
+    return total, per
+
+
+def run_fmcs(args):
+    import torch
+    from fastmulticolsort_b200 import capi
+    from fastmulticolsort_b200 import workloads as W
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    cols, bw = W.cols_17b33(N_ROWS)
+    n = N_ROWS
+    col_bytes = [c.dtype.itemsize for c in cols]
+    dcols = [torch.from_numpy(c.view(np.int32 if c.dtype == np.uint32 else np.int64)).cuda() for c in cols]
+    dorder = torch.empty(n, dtype=torch.int32, device="cuda")
+    dgroup = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx = capi.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        ctx.run_plan(dcols, bw, SPLIT, dorder, dgroup)
+
+    def plain_step():
+        ctx.run_plan(dcols, bw, PLAIN_SPLIT, dorder, dgroup)
+
+    clocks = ClockSampler(visible_gpu_index(local))
+    clocks.start()
+    t_load = time.perf_counter()
+    for _ in range(args.warmup):
+        step()
+    # keep the GPU busy for at least ~1 s before the timed region so that the
+    # clock samples describe the loaded state
+    while not args.only_steps and time.perf_counter() - t_load < 1.0:
+        step()
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    launches0 = ctx.launch_count()
+    total_ms, per_ms = time_steps(ctx, stream, step, args.steps)
+    launches = ctx.launch_count() - launches0
+    prof = ctx.profile_report()
+    ctx.profile(False)
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clk = clocks.stop()
+    total_ms = dist_max(total_ms, world)
+    ms_per_step = total_ms / args.steps
+    value = world * n / (ms_per_step / 1e3) / 1e6
+    if args.only_steps:
+        ctx.close()
+        dist_done(world)
+        if rank == 0:
+            print(json.dumps({"only_steps": True, "value": value, "ms_per_step": ms_per_step,
+                              "kernels": prof}), flush=True)
+        return 0
+
+    # plain one-sort-per-column comparator on the same data
+    for _ in range(3):
+        plain_step()
+    plain_total, _ = time_steps(ctx, stream, plain_step, max(3, args.steps // 2))
+    plain_ms = dist_max(plain_total / max(3, args.steps // 2), world)
+
+    # end to end: pinned host buffers, copies inside the timed region
+    hcols = []
+    for c in cols:
+        t = torch.empty(c.shape[0], dtype=torch.int32 if c.dtype == np.uint32 else torch.int64, pin_memory=True)
+        t.numpy()[:] = c.view(t.numpy().dtype)
+        hcols.append(t.numpy().view(c.dtype))
+    horder = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    hgroup = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+
+    def e2e_step():
+        ctx.run_plan(hcols, bw, SPLIT, horder, hgroup)
+
+    for _ in range(2):
+        e2e_step()
+    e2e_steps = max(3, min(args.steps, 20))
+    e2e_total, _ = time_steps(ctx, stream, e2e_step, e2e_steps)
+    e2e_ms = dist_max(e2e_total / e2e_steps, world)
+    e2e_value = world * n / (e2e_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel that reports its rows
+    hbm_peak, peak_kind = peaks()
+    dom, dom_ms = None, 0.0
+    for name, rec in prof.items():
+        if kernel_bytes_per_unit(name, 8) and rec["units"] > 0 and rec["ms"] > dom_ms:
+            dom, dom_ms = name, rec["ms"]
+    roofline = None
+    if dom:
+        rec = prof[dom]
+        bytes_total = rec["units"] * kernel_bytes_per_unit(dom, 8)
+        achieved = bytes_total / (rec["ms"] / 1e3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                traffic = json.load(f).get(dom, {}).get("bytes_per_launch_full_size")
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                    "traffic": traffic,
+                    "bytes_per_launch": bytes_total / rec["launches"],
+                    "launch_ms": rec["ms"] / rec["launches"], "launches": rec["launches"]}
+    model_bpr = plan_model_bytes_per_row(col_bytes, bw, SPLIT)
+    plan_gbs = model_bpr * n / (ms_per_step / 1e3) / 1e9
+    total_kernel_ms = sum(r["ms"] for r in prof.values())
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "M rows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded PRNG; 17-bit codes from 8,192 distinct values + uniform 33-bit codes)",
+        "config": {"workload": WORKLOAD, "rows": n, "plan": SPLIT, "columns": "u32 (17 bits) + u64 (33 bits)",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (192 MB of columns)"},
+        "latency_ms": {"p50": round(float(np.percentile(per_ms, 50)), 4),
+                       "p99": round(float(np.percentile(per_ms, 99)), 4)},
+        "plan_hbm": {"model_bytes_per_row": model_bpr, "achieved_gbs": round(plan_gbs, 1),
+                     "frac_of_peak": round(plan_gbs / hbm_peak, 4)},
+        "plain_gpu": {"plan": PLAIN_SPLIT, "value": round(world * n / (plain_ms / 1e3) / 1e6, 2),
+                      "ms_per_step": round(plain_ms, 4),
+                      "speedup_of_massaged": round(plain_ms / ms_per_step, 3)},
+        "roofline": roofline,
+        "kernels": {k: {"launches_per_step": v["launches"] / args.steps, "ms_per_step": round(v["ms"] / args.steps, 4)}
+                    for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
+        "kernel_ms_per_step": round(total_kernel_ms / args.steps, 4),
+        "e2e": {"value": round(e2e_value, 2), "unit": "M rows/s", "ms_per_step": round(e2e_ms, 4),
+                "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)), "d2h_bytes_per_step": int(8 * n)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cols, bw, SPLIT, args.cpu_runs)
+        line["cpu_baseline"].pop("seconds", None)
+    ctx.close()
+    dist_done(world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fmcs", choices=["fmcs", "reference"])
+    ap.add_argument("--cpu-runs", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-steps", action="store_true",
+                    help="warm-up and timed steps only (no comparators, e2e or CPU baseline): "
+                         "the command the ncu captures profile")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_fmcs(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

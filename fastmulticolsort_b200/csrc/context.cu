@@ -110,11 +110,16 @@ LaunchScope::LaunchScope(fmcs_ctx *ctx, const char *name) : ctx_(ctx)
 {
     ctx->launches++;
     if (!ctx->prof_on) return;
-    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx)};
+    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx), 0.0};
     if (!r.a || !r.b) return;
     cudaEventRecord(r.a, ctx->stream);
     rec_ = (int)ctx->prof.size();
     ctx->prof.push_back(r);
+}
+
+void LaunchScope::set_units(double u)
+{
+    if (rec_ >= 0) ctx_->prof[rec_].units = u;
 }
 
 LaunchScope::~LaunchScope()
@@ -159,6 +164,7 @@ extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
     if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, 256);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_status, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_small, 64 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_level, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
         fmcs_destroy(ctx);
@@ -184,6 +190,7 @@ extern "C" void fmcs_destroy(fmcs_ctx *ctx)
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
+    if (ctx->ev_level) cudaEventDestroy(ctx->ev_level);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -223,6 +230,7 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         std::string name;
         unsigned long long n = 0;
         double ms = 0;
+        double units = 0;
     };
     std::vector<Agg> agg;
     for (auto &r : ctx->prof) {
@@ -236,6 +244,7 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         if (k == agg.size()) agg.push_back(Agg{r.name});
         agg[k].n++;
         agg[k].ms += ms;
+        agg[k].units += r.units;
         ctx->ev_pool.push_back(r.a);
         ctx->ev_pool.push_back(r.b);
     }
@@ -243,8 +252,8 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
     std::string out = "{";
     for (size_t k = 0; k < agg.size(); ++k) {
         char tmp[256];
-        snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f}", k ? ", " : "",
-                 agg[k].name.c_str(), agg[k].n, agg[k].ms);
+        snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"units\": %.0f}",
+                 k ? ", " : "", agg[k].name.c_str(), agg[k].n, agg[k].ms, agg[k].units);
         out += tmp;
     }
     out += "}";

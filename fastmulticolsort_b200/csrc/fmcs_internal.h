@@ -60,6 +60,7 @@ struct Workspace {
 struct fmcs_prof_rec {
     const char *name;
     cudaEvent_t a, b;
+    double units;   // work items of the launch (rows), when the launcher knows them
 };
 
 struct fmcs_ctx {
@@ -79,6 +80,7 @@ struct fmcs_ctx {
     std::vector<fmcs_prof_rec> prof;
     std::vector<cudaEvent_t> ev_pool;
     unsigned long long launches = 0;   // kernels launched by this context
+    cudaEvent_t ev_level = nullptr;    // host-side read-back point of the sort levels
 };
 
 namespace fmcs {
@@ -96,6 +98,7 @@ class LaunchScope {
   public:
     LaunchScope(fmcs_ctx *ctx, const char *name);
     ~LaunchScope();
+    void set_units(double u);
 
   private:
     fmcs_ctx *ctx_;
@@ -132,6 +135,7 @@ struct SortArgs {
     uint32_t *order_out;       // device, n (may alias order_in)
     void *keys_out;            // device, n keys, or NULL
     uint64_t n;
+    bool fixed_launches = false;  // launch every level (no host read-back), e.g. under graph capture
 };
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
 

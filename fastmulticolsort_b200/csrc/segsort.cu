@@ -54,6 +54,7 @@ constexpr int kCtrLocalA = 4;
 constexpr int kCtrLocalB = 5;
 constexpr int kCtrLocalC = 6;
 constexpr int kCtrCopy = 7;
+constexpr int kCtrMoved = 8;    // rows the current level's scatter moves
 constexpr int kCtrWords = 16;
 
 struct LargeSeg {
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const 
             route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, la, lb, lc,
                           copy_out);
         if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
+        if (d == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
         __syncthreads();
     }
 }
@@ -701,11 +703,23 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const size_t msd_smem = sizeof(MsdSmem<K>);
     if ((rc = set_smem(ctx, msd_scatter_kernel<K>, msd_smem))) return rc;
     if (n > (uint64_t)kCapC) {
-        for (int lvl = 0; lvl < levels; ++lvl) {
+        // Host-known count of the level's large segments (exact unless the
+        // caller asked for a fixed launch sequence, e.g. for graph capture).
+        uint32_t nlarge = 1;
+        if (a.fixed_launches) {
+            nlarge = 1;
+        } else if (a.seg_start) {
+            cudaMemcpyAsync(ctx->h_small + 8, &ctr[kCtrLarge0], sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level count");
+            nlarge = ctx->h_small[8];
+        }
+        for (int lvl = 0; lvl < levels && nlarge > 0; ++lvl) {
             const int cur = lvl & 1, nxt = cur ^ 1;
             const uint32_t *d_cnt = &ctr[kCtrLarge0 + cur];
             cudaMemsetAsync(&ctr[kCtrLarge0 + nxt], 0, sizeof(uint32_t), st);
             cudaMemsetAsync(&ctr[kCtrMsdTile], 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(&ctr[kCtrMoved], 0, sizeof(uint32_t), st);
             { LaunchScope ls_(ctx, "tile_prefix");
                 tile_prefix_kernel<<<1, 1024, 0, st>>>(large[cur], d_cnt, tile_prefix);
             }
@@ -719,10 +733,23 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                 msd_plan_kernel<<<sms * 8, kRadix, 0, st>>>(large[cur], d_cnt, hist, ctr, kCtrLarge0 + nxt, large[nxt],
                                                              la, lb, lc, copy_list);
             }
-            { LaunchScope ls_(ctx, "msd_scatter");
+            if (!a.fixed_launches) {
+                // read the next level's count while the scatter runs
+                cudaMemcpyAsync(ctx->h_small + 8, &ctr[kCtrLarge0 + nxt], sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(ctx->h_small + 9, &ctr[kCtrMoved], sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+                cudaEventRecord(ctx->ev_level, st);
+            }
+            {
+                LaunchScope ls_(ctx, "msd_scatter");
                 msd_scatter_kernel<K><<<sms * 2, kNtM, msd_smem, st>>>(b, large[cur], d_cnt, tile_prefix, hist,
                                                                          &ctr[kCtrMsdTile], lookback, ctx->epoch++,
                                                                          ctx->d_status);
+                if (!a.fixed_launches) {
+                    cudaError_t e = cudaEventSynchronize(ctx->ev_level);
+                    if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level event");
+                    nlarge = ctx->h_small[8];
+                    ls_.set_units((double)ctx->h_small[9]);
+                }
             }
             FMCS_LAUNCH_CHECK("msd level");
         }

@@ -65,8 +65,10 @@ FMCS_API size_t fmcs_workspace_bytes(const fmcs_ctx *ctx);
 /* Kernel profiler (no reference counterpart; the reference times sections with
  * rdtsc, src/hybrid_timer.h:16-56).  While enabled, every kernel launch of the
  * context is bracketed by CUDA events on its stream.  fmcs_profile_report
- * synchronizes and writes a JSON object {"kernel": {"launches": n, "ms": t}}
- * for the launches since the last report, then forgets them. */
+ * synchronizes and writes a JSON object
+ * {"kernel": {"launches": n, "ms": t, "units": u}} for the launches since the
+ * last report, then forgets them; units are the rows the launches processed
+ * where the launcher knows them (the MSD scatter passes), else 0. */
 FMCS_API int fmcs_profile(fmcs_ctx *ctx, int enable);
 FMCS_API int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len);
 /* Number of kernels this context has launched since it was created. */
