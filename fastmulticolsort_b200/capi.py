@@ -29,6 +29,7 @@ EXPORTS = (
     "fmcs_create", "fmcs_destroy", "fmcs_last_error", "fmcs_synchronize", "fmcs_stream",
     "fmcs_workspace_bytes", "fmcs_stitch", "fmcs_gather", "fmcs_sort_round", "fmcs_hash_round",
     "fmcs_run_plan", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
+    "fmcs_group_ids_noalloc",
 )
 
 
@@ -76,6 +77,7 @@ def load(path: str = LIB_PATH):
     L.fmcs_profile_report.argtypes = [vp, C.c_char_p, C.c_size_t]
     L.fmcs_launch_count.argtypes = [vp]
     L.fmcs_launch_count.restype = C.c_ulonglong
+    L.fmcs_group_ids_noalloc.argtypes = [vp, vp, u32, vp, vp, u64, u32p]
     _lib = L
     return L
 
@@ -105,6 +107,20 @@ def _len(a) -> int:
 
 def _u32arr(xs: Sequence[int]):
     return (C.c_uint32 * len(xs))(*[int(x) for x in xs])
+
+
+def group_ids_noalloc(keys, out_group, in_group=None, stream: int = 0) -> int:
+    """fmcs_group_ids_noalloc: dense group ids of sorted device keys with no
+    device allocation (scratch in the library's static device array, at most
+    67,108,864 rows).  keys / in_group / out_group must be device tensors;
+    returns the group count."""
+    L = load()
+    ng = C.c_uint32(0)
+    rc = L.fmcs_group_ids_noalloc(C.c_void_p(stream or None), _addr(keys), _itemsize(keys),
+                                  _addr(in_group), _addr(out_group), _len(keys), C.byref(ng))
+    if rc != FMCS_OK:
+        raise FmcsError(rc, "fmcs_group_ids_noalloc failed")
+    return ng.value
 
 
 class Context:

@@ -11,6 +11,8 @@
 #include "device_common.cuh"
 #include "fmcs_internal.h"
 
+#include <mutex>
+
 namespace fmcs {
 
 namespace {
@@ -212,3 +214,127 @@ int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64
 }
 
 }  // namespace fmcs
+
+// ---------------------------------------------------------------------------
+// Allocation-free group ids.
+//
+// Some callers cannot let a library allocate device memory: query engines
+// that reserve all of HBM up front in their own pool (a cudaMalloc from inside
+// the library would fail or fragment that pool), and latency-critical callers
+// that cannot afford the device-wide synchronization that cudaMalloc/cudaFree
+// imply.  fmcs_group_ids_noalloc serves them: the same one-pass boundary scan
+// as the group ids of a sort round, with its scratch (the decoupled look-back
+// words, the tile counter, the group count and the wait status) in the
+// file-scope device array below instead of the context's workspace.  The
+// caller passes device inputs and outputs; no context is needed.
+//
+// The array is modest (kNoAllocTiles look-back words, 128 KiB) and every GPU
+// that loads the library holds it until the process exits.  It bounds n at
+// kNoAllocTiles * 4096 = 67,108,864 rows.  All calls share it and it keeps the
+// last call's contents, so each call clears the words that must start at zero;
+// calls whose work overlaps on the GPU (two streams, or two host threads)
+// race on it and must be serialized by the caller.
+// ---------------------------------------------------------------------------
+namespace fmcs {
+namespace {
+
+constexpr uint64_t kNoAllocTiles = 16384;
+constexpr uint64_t kNoAllocMaxRows = kNoAllocTiles * kScanTile;
+// layout (64-bit words): [0, kNoAllocTiles) look-back; then the tile counter,
+// the group count and the status word, one 64-bit word each
+constexpr uint64_t kNoAllocWords = kNoAllocTiles + 4;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long *g_noalloc_ptr[kMaxDevices] = {};
+
+// Host code cannot use g_noalloc_scratch's name as a device address: resolve
+// the device address once per device, with that device current.
+int noalloc_scratch(unsigned long long **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FMCS_E_CUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return FMCS_E_CUDA;
+        }
+        g_noalloc_ptr[dev] = (unsigned long long *)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return FMCS_OK;
+}
+
+}  // namespace
+
+}  // namespace fmcs
+
+extern "C" int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t key_bytes,
+                                      const uint32_t *in_group, uint32_t *out_group, uint64_t n,
+                                      uint32_t *ngroups)
+{
+    using namespace fmcs;
+    if (ngroups) *ngroups = 0;
+    if (!(key_bytes == 1 || key_bytes == 2 || key_bytes == 4 || key_bytes == 8)) return FMCS_E_INVAL;
+    if (n > kNoAllocMaxRows) return FMCS_E_INVAL;   // beyond the static scratch: 67,108,864 rows
+    if (n == 0) return FMCS_OK;
+    if (!keys || !out_group || !is_device_ptr(keys) || !is_device_ptr(out_group) ||
+        (in_group && !is_device_ptr(in_group)))
+        return FMCS_E_INVAL;   // device pointers only: staging host data would allocate
+    unsigned long long *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    unsigned long long *lookback = scratch;
+    uint32_t *tile_counter = (uint32_t *)(scratch + kNoAllocTiles);
+    uint32_t *d_count = (uint32_t *)(scratch + kNoAllocTiles + 1);
+    int *status = (int *)(scratch + kNoAllocTiles + 2);
+    // the previous call's words: look-back of the tiles this call uses, counter,
+    // count and status all start at zero
+    cudaError_t e = cudaMemsetAsync(lookback, 0, tiles * sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tile_counter, 0, 3 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return FMCS_E_CUDA;
+    const uint32_t epoch = 1;
+    const unsigned grid = (unsigned)tiles;
+    switch (key_bytes) {
+    case 1:
+        boundary_scan_kernel<uint8_t><<<grid, kScanThreads, 0, st>>>((const uint8_t *)keys, in_group, nullptr,
+                                                                      out_group, nullptr, n, tile_counter, lookback,
+                                                                      epoch, d_count, status);
+        break;
+    case 2:
+        boundary_scan_kernel<uint16_t><<<grid, kScanThreads, 0, st>>>((const uint16_t *)keys, in_group, nullptr,
+                                                                       out_group, nullptr, n, tile_counter, lookback,
+                                                                       epoch, d_count, status);
+        break;
+    case 4:
+        boundary_scan_kernel<uint32_t><<<grid, kScanThreads, 0, st>>>((const uint32_t *)keys, in_group, nullptr,
+                                                                       out_group, nullptr, n, tile_counter, lookback,
+                                                                       epoch, d_count, status);
+        break;
+    default:
+        boundary_scan_kernel<uint64_t><<<grid, kScanThreads, 0, st>>>((const uint64_t *)keys, in_group, nullptr,
+                                                                       out_group, nullptr, n, tile_counter, lookback,
+                                                                       epoch, d_count, status);
+        break;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return FMCS_E_CUDA;
+    // read the count and the wait status back (into the caller's stack: no
+    // allocation) and finish the call
+    uint32_t back[3] = {0, 0, 0};
+    e = cudaMemcpyAsync(back, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(back + 1, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return FMCS_E_CUDA;
+    if ((int)back[1] == kDevTimeout) return FMCS_E_TIMEOUT;
+    if (back[1] != 0) return FMCS_E_CUDA;
+    if (ngroups) *ngroups = back[0];
+    return FMCS_OK;
+}

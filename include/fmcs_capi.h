@@ -140,6 +140,30 @@ FMCS_API int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_
                   const uint32_t *split, uint32_t nbanks, uint64_t n, int hash,
                   uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 
+/* Allocation-free group ids (no counterpart in the reference, which mallocs
+ * on every call).  For callers that cannot let a library allocate device
+ * memory: engines that reserve all of HBM in their own pool up front, and
+ * latency-critical callers that cannot take the device-wide synchronization of
+ * cudaMalloc/cudaFree.  Computes the same dense group ids as the group vector
+ * of fmcs_sort_round, from keys that are already sorted inside each run of
+ * equal in_group (in_group may be NULL):
+ *   out_group[0] = 0; out_group[i] = out_group[i-1] +
+ *       (keys[i] != keys[i-1] || in_group[i] != in_group[i-1]).
+ * keys, in_group and out_group must be DEVICE pointers (host pointers are
+ * rejected: staging them would allocate); stream is a cudaStream_t (NULL = the
+ * default stream); *ngroups (optional, host) receives the group count.  The
+ * call returns when the result is complete.
+ * Scratch lives in a file-scope device array of the library (128 KiB, held by
+ * every GPU that loads the library until exit), so n is limited to
+ * 67,108,864 rows; larger n returns FMCS_E_INVAL.  The first call on a device
+ * resolves that array's device address, so make a first call on each device
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU race and must be serialized by the caller.  Nothing is allocated:
+ * no cudaMalloc, no cudaFree, no allocating library routine. */
+FMCS_API int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t key_bytes,
+                                    const uint32_t *in_group, uint32_t *out_group, uint64_t n,
+                                    uint32_t *ngroups);
+
 #ifdef __cplusplus
 }
 #endif
