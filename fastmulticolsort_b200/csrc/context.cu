@@ -5,6 +5,7 @@
 #include "fmcs_internal.h"
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace fmcs {
@@ -171,6 +172,7 @@ extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
         return FMCS_E_CUDA;
     }
     *ctx->h_status = 0;
+    if (const char *m = getenv("FMCS_RANK_MODE")) ctx->rank_mode = (m[0] == 'b' || m[0] == '1') ? 1 : 0;
     *out = ctx;
     return FMCS_OK;
 }

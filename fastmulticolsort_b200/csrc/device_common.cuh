@@ -63,10 +63,38 @@ __device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, uint32_t f
 // lane order), returns each valid item's rank among the warp's items with the
 // same digit seen so far, and advances the warp's per-digit counters `whist`.
 // Invalid lanes (valid == false) take no rank and leave the counters alone.
-__device__ __forceinline__ uint32_t wlms_rank(uint32_t digit, bool valid, uint32_t *whist)
+// Two ways to find the lanes holding the same digit ("peers"):
+//   kRankMatch:  one match.any.sync on the digit;
+//   kRankBallot: one ballot per digit bit, peers = AND over bits of the
+//                ballot or its complement (the ballot-based multisplit).
+constexpr int kRankMatch = 0;
+constexpr int kRankBallot = 1;
+
+template <int MODE>
+__device__ __forceinline__ uint32_t peers_of(uint32_t digit, bool valid, uint32_t width)
 {
-    const uint32_t key = valid ? digit : 0xFFFFFFFFu;
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+    if constexpr (MODE == kRankMatch) {
+        return __match_any_sync(0xFFFFFFFFu, valid ? digit : 0xFFFFFFFFu);
+    } else {
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+        if (!valid) peers = ~peers;
+#pragma unroll
+        for (uint32_t b = 0; b < (uint32_t)kRadixBits; ++b) {
+            if (b < width) {
+                const bool bit = (digit >> b) & 1u;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+                peers &= bit ? bal : ~bal;
+            }
+        }
+        return peers;
+    }
+}
+
+template <int MODE = kRankMatch>
+__device__ __forceinline__ uint32_t wlms_rank(uint32_t digit, bool valid, uint32_t *whist,
+                                              uint32_t width = kRadixBits)
+{
+    const uint32_t peers = peers_of<MODE>(digit, valid, width);
     const uint32_t leader = __ffs(peers) - 1;
     uint32_t base = 0;
     if (valid && lane_id() == leader) {

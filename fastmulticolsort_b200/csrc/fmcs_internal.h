@@ -81,6 +81,7 @@ struct fmcs_ctx {
     std::vector<cudaEvent_t> ev_pool;
     unsigned long long launches = 0;   // kernels launched by this context
     cudaEvent_t ev_level = nullptr;    // host-side read-back point of the sort levels
+    int rank_mode = 0;                 // 0: match.any multi-split, 1: ballot multi-split
 };
 
 namespace fmcs {

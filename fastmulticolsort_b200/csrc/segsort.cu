@@ -41,20 +41,27 @@ constexpr uint32_t kSrcBuf1 = 1;
 constexpr uint32_t kSrcExt = 2;
 constexpr uint32_t kSkipBit = 0x100;
 
-constexpr int kCapA = 128;   // 32 lanes x 4 items
+// Local tiers: a segment goes to the smallest tier whose capacity holds it, so
+// that each kernel's unrolled item steps match the segment (few idle steps).
+constexpr int kCapA = 128;   // warp per segment: 32 lanes x 4 items
 constexpr int kItemsA = 4;
-constexpr int kNtB = 128, kItB = 8, kCapB = kNtB * kItB;    // 1024
-constexpr int kNtC = 256, kItC = 16, kCapC = kNtC * kItC;   // 4096
-constexpr int kNtM = 256, kItM = 16, kTileM = kNtM * kItM;  // MSD tile, 4096
+constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
+constexpr int kNtB2 = 128, kItB2 = 8, kCapB2 = kNtB2 * kItB2;   // 1024
+constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
+constexpr int kNtC2 = 256, kItC2 = 16, kCapC2 = kNtC2 * kItC2;  // 4096
+constexpr int kCapLocal = kCapC2;                               // larger: MSD levels
+constexpr int kNtM = 256, kItM = 8, kTileM = kNtM * kItM;       // MSD tile, 2048 rows
 
 // counters slot words
 constexpr int kCtrMsdTile = 1;
 constexpr int kCtrLarge0 = 2;   // + level parity
 constexpr int kCtrLocalA = 4;
-constexpr int kCtrLocalB = 5;
-constexpr int kCtrLocalC = 6;
+constexpr int kCtrLocalB1 = 5;
+constexpr int kCtrLocalB2 = 6;
 constexpr int kCtrCopy = 7;
 constexpr int kCtrMoved = 8;    // rows the current level's scatter moves
+constexpr int kCtrLocalC1 = 9;
+constexpr int kCtrLocalC2 = 10;
 constexpr int kCtrWords = 16;
 
 struct LargeSeg {
@@ -101,29 +108,31 @@ __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32
     return make_uint2(start, len | (shift << 16) | (src << 24));
 }
 
+struct Lists {
+    uint2 *a, *b1, *b2, *c1, *c2;
+    LargeSeg *copy;
+};
+
 // Route a segment (child or initial) to its tier.  Segments that need no
 // sorting (one row, or no key bits left) only need to reach BUF0.
 __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
-                                              uint32_t *ctr, int large_ctr, LargeSeg *large_out,
-                                              uint2 *la, uint2 *lb, uint2 *lc, LargeSeg *copy_out)
+                                              uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L)
 {
     if (len == 0) return;
     if (len == 1 || shift == 0) {
         if (src != kSrcBuf0) {
             uint32_t slot = atomicAdd(&ctr[kCtrCopy], 1u);
-            copy_out[slot] = LargeSeg{start, len, 0, src};
+            L.copy[slot] = LargeSeg{start, len, 0, src};
         }
         return;
     }
-    if (len <= (uint32_t)kCapA) {
-        la[atomicAdd(&ctr[kCtrLocalA], 1u)] = pack_local(start, len, shift, src);
-    } else if (len <= (uint32_t)kCapB) {
-        lb[atomicAdd(&ctr[kCtrLocalB], 1u)] = pack_local(start, len, shift, src);
-    } else if (len <= (uint32_t)kCapC) {
-        lc[atomicAdd(&ctr[kCtrLocalC], 1u)] = pack_local(start, len, shift, src);
-    } else {
-        large_out[atomicAdd(&ctr[large_ctr], 1u)] = LargeSeg{start, len, shift, src};
-    }
+    const uint2 e = pack_local(start, len, shift, src);
+    if (len <= (uint32_t)kCapA) L.a[atomicAdd(&ctr[kCtrLocalA], 1u)] = e;
+    else if (len <= (uint32_t)kCapB1) L.b1[atomicAdd(&ctr[kCtrLocalB1], 1u)] = e;
+    else if (len <= (uint32_t)kCapB2) L.b2[atomicAdd(&ctr[kCtrLocalB2], 1u)] = e;
+    else if (len <= (uint32_t)kCapC1) L.c1[atomicAdd(&ctr[kCtrLocalC1], 1u)] = e;
+    else if (len <= (uint32_t)kCapC2) L.c2[atomicAdd(&ctr[kCtrLocalC2], 1u)] = e;
+    else large_out[atomicAdd(&ctr[large_ctr], 1u)] = LargeSeg{start, len, shift, src};
 }
 
 // ---------------------------------------------------------------------------
@@ -131,8 +140,7 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
 // ---------------------------------------------------------------------------
 template <typename K>
 __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_start, const uint32_t *d_nseg,
-                                uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, uint2 *la,
-                                uint2 *lb, uint2 *lc, LargeSeg *copy_out)
+                                uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, Lists lists)
 {
     const uint32_t nseg = seg_start ? *d_nseg : 1u;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
@@ -148,7 +156,7 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
             b.v0[start] = v;
             continue;
         }
-        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, la, lb, lc, copy_out);
+        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, lists);
     }
 }
 
@@ -243,8 +251,7 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSe
 // Per large segment: exclusive digit offsets, skip detection, children.
 __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const uint32_t *d_nseg,
                                                           uint32_t *hist, uint32_t *ctr, int next_large_ctr,
-                                                          LargeSeg *large_next, uint2 *la, uint2 *lb,
-                                                          uint2 *lc, LargeSeg *copy_out)
+                                                          LargeSeg *large_next, Lists lists)
 {
     __shared__ uint32_t cnt[kRadix];
     __shared__ uint32_t tmp[kRadix / 32 + 1];
@@ -267,8 +274,7 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const 
         const uint32_t child_shift = sg.shift - width;
         const uint32_t child_src = skip ? sg.src : (sg.src == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
         if (c > 0)
-            route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, la, lb, lc,
-                          copy_out);
+            route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, lists);
         if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
         if (d == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
         __syncthreads();
@@ -287,8 +293,8 @@ struct MsdSmem {
     uint32_t vals[kTileM];
 };
 
-template <typename K>
-__global__ void __launch_bounds__(kNtM) msd_scatter_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
+template <typename K, int RANK>
+__global__ void __launch_bounds__(kNtM, 4) msd_scatter_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
                                                            const uint32_t *tile_prefix, const uint32_t *offs,
                                                            uint32_t *tile_counter, unsigned long long *lookback,
                                                            uint32_t epoch, int *status)
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(kNtM) msd_scatter_kernel(Bufs<K> b, const Larg
         for (int j = 0; j < kItM; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             dig[j] = digit_of(key[j], lo, width);
-            rank[j] = wlms_rank(dig[j], p < cnt, sm.whist[warp]);
+            rank[j] = wlms_rank<RANK>(dig[j], p < cnt, sm.whist[warp], width);
         }
         __syncthreads();
         // per digit: exclusive over warps, tile total
@@ -398,98 +404,185 @@ __global__ void __launch_bounds__(kNtM) msd_scatter_kernel(Bufs<K> b, const Larg
 // ---------------------------------------------------------------------------
 // local tiers
 // ---------------------------------------------------------------------------
-// Block-per-segment LSD radix sort over bits [0, shift), stable.
+// Block-per-segment stable sort over key bits [0, shift).
+//
+// Strategy (all in shared memory, one HBM read and one HBM write per row):
+//   1. one stable split on the top digit (bits [shift-8, shift)), ranked by
+//      warp-level multi-split: rows land in 256 buckets in key order;
+//   2. if every bucket holds <= kCountRankMax rows, each row's final place is
+//      bucket start + the number of rows of its bucket that sort before it
+//      (smaller key, or equal key and earlier position): a short loop over
+//      the bucket with broadcast shared-memory reads, no further passes;
+//   3. otherwise (skewed keys) LSD passes over bits [0, shift-8) and a last
+//      pass on the top digit finish the sort from the split order.
+// Every step is stable, so ties keep their input order.
+constexpr uint32_t kCountRankMax = 64;
+
 template <typename K, int NT, int IT>
 struct BlockSmem {
     uint32_t whist[NT / 32][kRadix];
     uint32_t doff[kRadix];
+    uint32_t cnt[kRadix];
     uint32_t tmp[NT / 32 + 1];
     uint32_t flag;
+    uint32_t maxb;
     K keys[NT * IT];
     uint32_t vals[NT * IT];
 };
 
-template <typename K, int NT, int IT>
-__global__ void __launch_bounds__(NT) block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
+// One stable counting pass of the block over digit bits [lo, lo + width):
+// rows move (through shared memory) from their current sequence position to
+// their place in digit order.  Returns false when every row has the same digit
+// (nothing moves).  Leaves the digit counts in sm.cnt and the exclusive digit
+// offsets in sm.doff.  `to_smem_only`: rows stay in shared memory (the caller
+// reads them there) instead of being reloaded into registers.
+template <typename K, int NT, int IT, int RANK>
+__device__ __forceinline__ bool block_pass(BlockSmem<K, NT, IT> &sm, K (&key)[IT], uint32_t (&val)[IT],
+                                           uint32_t steps, uint32_t wbase, uint32_t len, uint32_t lo,
+                                           uint32_t width, bool to_smem_only)
+{
+    constexpr int NW = NT / 32;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int d = lane; d < kRadix; d += 32) sm.whist[warp][d] = 0;
+    if (threadIdx.x == 0) {
+        sm.flag = 0;
+        sm.maxb = 0;
+    }
+    __syncthreads();
+    uint32_t rank[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        if (j < (int)steps) {   // uniform across the block
+            const uint32_t p = wbase + j * 32 + lane;
+            rank[j] = wlms_rank<RANK>(digit_of(key[j], lo, width), p < len, sm.whist[warp], width);
+        }
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += NT) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const uint32_t c = sm.whist[w][d];
+            sm.whist[w][d] = run;
+            run += c;
+        }
+        sm.doff[d] = run;
+        sm.cnt[d] = run;
+        if (run == len) sm.flag = 1;   // one digit holds every row: identity pass
+        if (run) atomicMax(&sm.maxb, run);
+    }
+    __syncthreads();
+    const bool identity = sm.flag != 0;
+    __syncthreads();
+    if (identity) return false;   // uniform across the block
+    uint32_t tot;
+    block_exclusive_scan_radix<NT>(sm.doff, sm.tmp, &tot);
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t p = wbase + j * 32 + lane;
+        if (j < (int)steps && p < len) {
+            const uint32_t d = digit_of(key[j], lo, width);
+            const uint32_t pos = sm.doff[d] + sm.whist[warp][d] + rank[j];
+            sm.keys[pos] = key[j];
+            sm.vals[pos] = val[j];
+        }
+    }
+    __syncthreads();
+    if (!to_smem_only) {
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (j < (int)steps && p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+template <typename K, int NT, int IT, int RANK>
+__global__ void __launch_bounds__(NT, (NT * IT >= 4096 ? 2 : (NT * IT >= 2048 ? 3 : 4)))
+block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BlockSmem<K, NT, IT> &sm = *reinterpret_cast<BlockSmem<K, NT, IT> *>(smem_raw);
+    constexpr int NW = NT / 32;
     const uint32_t count = *d_count;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const uint32_t wbase = warp * (IT * 32);
     for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
         const uint2 ent = list[e];
         const uint32_t start = ent.x;
         const uint32_t len = ent.y & 0xFFFFu;
         const uint32_t shift = (ent.y >> 16) & 0x7Fu;
         const uint32_t src = (ent.y >> 24) & 3u;
+        // Spread the segment evenly over the warps: warp w owns positions
+        // [w*steps*32, (w+1)*steps*32); a step is one item per lane.
+        const uint32_t steps = (len + NW * 32 - 1) / (NW * 32);
+        const uint32_t wbase = warp * steps * 32;
         K key[IT];
         uint32_t val[IT];
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
-            if (p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
-            else { key[j] = 0; val[j] = 0; }
+            key[j] = 0;
+            val[j] = 0;
+            if (j < (int)steps && p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
         }
-        for (uint32_t lo = 0; lo < shift; lo += kRadixBits) {
-            const uint32_t width = min((uint32_t)kRadixBits, shift - lo);
-            for (int d = lane; d < kRadix; d += 32) sm.whist[warp][d] = 0;
-            if (threadIdx.x == 0) sm.flag = 0;
-            __syncthreads();
-            uint32_t rank[IT];
-            uint32_t dig[IT];
-#pragma unroll
-            for (int j = 0; j < IT; ++j) {
-                const uint32_t p = wbase + j * 32 + lane;
-                dig[j] = digit_of(key[j], lo, width);
-                rank[j] = wlms_rank(dig[j], p < len, sm.whist[warp]);
-            }
-            __syncthreads();
-            for (int d = threadIdx.x; d < kRadix; d += NT) {
-                uint32_t run = 0;
-#pragma unroll
-                for (int w = 0; w < NT / 32; ++w) {
-                    const uint32_t c = sm.whist[w][d];
-                    sm.whist[w][d] = run;
-                    run += c;
+        bool written = false;
+        uint32_t lsd_top = shift;   // LSD passes cover [0, lsd_top)
+        if (shift > (uint32_t)kRadixBits) {
+            const uint32_t top = shift - kRadixBits;
+            const bool moved = block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, top, kRadixBits, true);
+            if (!moved) {
+                lsd_top = top;   // the top digit is constant: sort the bits below it
+            } else if (sm.maxb <= kCountRankMax) {
+                // rows are in smem in top-digit order; rank each row inside its bucket
+                for (uint32_t p = threadIdx.x; p < len; p += NT) {
+                    const K k = sm.keys[p];
+                    const uint32_t v = sm.vals[p];
+                    const uint32_t d = digit_of(k, top, kRadixBits);
+                    const uint32_t b0 = sm.doff[d];
+                    const uint32_t b1 = b0 + sm.cnt[d];
+                    uint32_t r = 0;
+                    for (uint32_t q = b0; q < b1; ++q) {
+                        const K kq = sm.keys[q];
+                        r += (kq < k) || (kq == k && q < p);
+                    }
+                    b.k0[(uint64_t)start + b0 + r] = k;
+                    b.v0[(uint64_t)start + b0 + r] = v;
                 }
-                sm.doff[d] = run;
-                if (run == len) sm.flag = 1;   // one digit holds every row: identity pass
-            }
-            __syncthreads();
-            const bool identity = sm.flag != 0;
-            __syncthreads();
-            if (identity) continue;   // uniform across the block
-            uint32_t tot;
-            block_exclusive_scan_radix<NT>(sm.doff, sm.tmp, &tot);
+                written = true;
+            } else {
+                // skewed: continue from the split order with LSD passes below the
+                // top digit, then the top digit again
 #pragma unroll
-            for (int j = 0; j < IT; ++j) {
-                const uint32_t p = wbase + j * 32 + lane;
-                if (p < len) {
-                    const uint32_t pos = sm.doff[dig[j]] + sm.whist[warp][dig[j]] + rank[j];
-                    sm.keys[pos] = key[j];
-                    sm.vals[pos] = val[j];
+                for (int j = 0; j < IT; ++j) {
+                    const uint32_t p = wbase + j * 32 + lane;
+                    if (j < (int)steps && p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
                 }
+                __syncthreads();
+                for (uint32_t lo = 0; lo < top; lo += kRadixBits)
+                    block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, lo, min((uint32_t)kRadixBits, top - lo),
+                                                false);
+                block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, top, kRadixBits, false);
+                lsd_top = 0;
             }
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < IT; ++j) {
-                const uint32_t p = wbase + j * 32 + lane;
-                if (p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
-            }
-            __syncthreads();
         }
-        // every load of this segment is done (barriers above, or below for
-        // shift-free copies) before the first store into BUF0, which may alias
-        // the EXT oids of the same range
-        __syncthreads();
+        if (!written) {
+            for (uint32_t lo = 0; lo < lsd_top; lo += kRadixBits)
+                block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, lo, min((uint32_t)kRadixBits, lsd_top - lo),
+                                            false);
+            // every load of this segment is done (barriers above) before the
+            // first store into BUF0, which may alias the EXT oids of the range
+            __syncthreads();
 #pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            if (p < len) {
-                b.k0[(uint64_t)start + p] = key[j];
-                b.v0[(uint64_t)start + p] = val[j];
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t p = wbase + j * 32 + lane;
+                if (j < (int)steps && p < len) {
+                    b.k0[(uint64_t)start + p] = key[j];
+                    b.v0[(uint64_t)start + p] = val[j];
+                }
             }
         }
         __syncthreads();
@@ -504,7 +597,7 @@ struct WarpSmem {
     uint32_t vals[32 * kItemsA];
 };
 
-template <typename K>
+template <typename K, int RANK>
 __global__ void __launch_bounds__(256) warp_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
     __shared__ WarpSmem<K> all[8];
@@ -537,7 +630,7 @@ __global__ void __launch_bounds__(256) warp_sort_kernel(Bufs<K> b, const uint2 *
             for (int j = 0; j < kItemsA; ++j) {
                 const uint32_t p = j * 32 + lane;
                 dig[j] = digit_of(key[j], lo, width);
-                rank[j] = wlms_rank(dig[j], p < len, sm.hist);
+                rank[j] = wlms_rank<RANK>(dig[j], p < len, sm.hist, width);
             }
             // warp exclusive scan of the 256 counters (8 per lane)
             uint32_t c[8];
@@ -627,7 +720,7 @@ int set_smem(fmcs_ctx *ctx, F *f, size_t bytes)
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what);          \
     } while (0)
 
-template <typename K>
+template <typename K, int RANK>
 int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
 {
     const uint64_t n = a.n;
@@ -651,8 +744,9 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     b.v1 = (uint32_t *)p;
 
     // lists (capacities are bounds on disjoint segments of each tier's minimum size)
-    const uint64_t cap_large = n / (kCapC + 1) + 2;
-    const uint64_t cap_a = n / 2 + 2, cap_b = n / (kCapA + 1) + 2, cap_c = n / (kCapB + 1) + 2;
+    const uint64_t cap_large = n / (kCapLocal + 1) + 2;
+    const uint64_t cap_a = n / 2 + 2, cap_b1 = n / (kCapA + 1) + 2, cap_b2 = n / (kCapB1 + 1) + 2;
+    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2;
     // copy entries: disjoint ranges; at most 256 children per large segment per
     // level, so bounded by both n and (levels + 1) * 256 * cap_large
     const uint64_t levels_max = (a.key_bits + kRadixBits - 1) / kRadixBits;
@@ -662,14 +756,18 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     large[0] = (LargeSeg *)p;
     if ((rc = ws_get(ctx, kSlotLarge1, cap_large * sizeof(LargeSeg), &p))) return rc;
     large[1] = (LargeSeg *)p;
-    uint2 *la, *lb, *lc;
-    if ((rc = ws_get(ctx, kSlotLocalA, cap_a * sizeof(uint2), &p))) return rc;
-    la = (uint2 *)p;
-    if ((rc = ws_get(ctx, kSlotLocalB, cap_b * sizeof(uint2), &p))) return rc;
-    lb = (uint2 *)p;
-    if ((rc = ws_get(ctx, kSlotLocalC, cap_c * sizeof(uint2) + cap_copy * sizeof(LargeSeg), &p))) return rc;
-    lc = (uint2 *)p;
-    LargeSeg *copy_list = (LargeSeg *)((char *)p + ((cap_c * sizeof(uint2) + 15) & ~size_t(15)));
+    Lists lists;
+    {
+        const uint64_t tot = cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2;
+        if ((rc = ws_get(ctx, kSlotLocalA, tot * sizeof(uint2), &p))) return rc;
+        lists.a = (uint2 *)p;
+        lists.b1 = lists.a + cap_a;
+        lists.b2 = lists.b1 + cap_b1;
+        lists.c1 = lists.b2 + cap_b2;
+        lists.c2 = lists.c1 + cap_c1;
+        if ((rc = ws_get(ctx, kSlotLocalC, cap_copy * sizeof(LargeSeg), &p))) return rc;
+        lists.copy = (LargeSeg *)p;
+    }
     uint32_t *hist, *tile_prefix;
     if ((rc = ws_get(ctx, kSlotSegHist, cap_large * kRadix * sizeof(uint32_t), &p))) return rc;
     hist = (uint32_t *)p;
@@ -693,16 +791,15 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                                   : 1u;
         if (seg_start && a.nseg_host == 0) grid = (unsigned)sms * 16;
         { LaunchScope ls_(ctx, "classify");
-            classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], la, lb, lc,
-                                                     copy_list);
+            classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists);
         }
         FMCS_LAUNCH_CHECK("classify");
     }
     // MSD levels
     const int levels = (int)((a.key_bits + kRadixBits - 1) / kRadixBits);
     const size_t msd_smem = sizeof(MsdSmem<K>);
-    if ((rc = set_smem(ctx, msd_scatter_kernel<K>, msd_smem))) return rc;
-    if (n > (uint64_t)kCapC) {
+    if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK>, msd_smem))) return rc;
+    if (n > (uint64_t)kCapLocal) {
         // Host-known count of the level's large segments (exact unless the
         // caller asked for a fixed launch sequence, e.g. for graph capture).
         uint32_t nlarge = 1;
@@ -731,7 +828,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             }
             { LaunchScope ls_(ctx, "msd_plan");
                 msd_plan_kernel<<<sms * 8, kRadix, 0, st>>>(large[cur], d_cnt, hist, ctr, kCtrLarge0 + nxt, large[nxt],
-                                                             la, lb, lc, copy_list);
+                                                             lists);
             }
             if (!a.fixed_launches) {
                 // read the next level's count while the scatter runs
@@ -741,7 +838,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             }
             {
                 LaunchScope ls_(ctx, "msd_scatter");
-                msd_scatter_kernel<K><<<sms * 2, kNtM, msd_smem, st>>>(b, large[cur], d_cnt, tile_prefix, hist,
+                msd_scatter_kernel<K, RANK><<<sms * 4, kNtM, msd_smem, st>>>(b, large[cur], d_cnt, tile_prefix, hist,
                                                                          &ctr[kCtrMsdTile], lookback, ctx->epoch++,
                                                                          ctx->d_status);
                 if (!a.fixed_launches) {
@@ -755,21 +852,31 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         }
     }
     // local tiers
-    const size_t smem_b = sizeof(BlockSmem<K, kNtB, kItB>);
-    const size_t smem_c = sizeof(BlockSmem<K, kNtC, kItC>);
-    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB, kItB>, smem_b))) return rc;
-    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC, kItC>, smem_c))) return rc;
+    const size_t smem_b1 = sizeof(BlockSmem<K, kNtB1, kItB1>);
+    const size_t smem_b2 = sizeof(BlockSmem<K, kNtB2, kItB2>);
+    const size_t smem_c1 = sizeof(BlockSmem<K, kNtC1, kItC1>);
+    const size_t smem_c2 = sizeof(BlockSmem<K, kNtC2, kItC2>);
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB1, kItB1, RANK>, smem_b1))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB2, kItB2, RANK>, smem_b2))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1, kItC1, RANK>, smem_c1))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
     { LaunchScope ls_(ctx, "warp_sort");
-        warp_sort_kernel<K><<<sms * 16, 256, 0, st>>>(b, la, &ctr[kCtrLocalA]);
+        warp_sort_kernel<K, RANK><<<sms * 16, 256, 0, st>>>(b, lists.a, &ctr[kCtrLocalA]);
     }
-    { LaunchScope ls_(ctx, "block_sort");
-        block_sort_kernel<K, kNtB, kItB><<<sms * 8, kNtB, smem_b, st>>>(b, lb, &ctr[kCtrLocalB]);
+    { LaunchScope ls_(ctx, "block_sort_512");
+        block_sort_kernel<K, kNtB1, kItB1, RANK><<<sms * 12, kNtB1, smem_b1, st>>>(b, lists.b1, &ctr[kCtrLocalB1]);
     }
-    { LaunchScope ls_(ctx, "block_sort");
-        block_sort_kernel<K, kNtC, kItC><<<sms * 3, kNtC, smem_c, st>>>(b, lc, &ctr[kCtrLocalC]);
+    { LaunchScope ls_(ctx, "block_sort_1024");
+        block_sort_kernel<K, kNtB2, kItB2, RANK><<<sms * 8, kNtB2, smem_b2, st>>>(b, lists.b2, &ctr[kCtrLocalB2]);
+    }
+    { LaunchScope ls_(ctx, "block_sort_2048");
+        block_sort_kernel<K, kNtC1, kItC1, RANK><<<sms * 5, kNtC1, smem_c1, st>>>(b, lists.c1, &ctr[kCtrLocalC1]);
+    }
+    { LaunchScope ls_(ctx, "block_sort_4096");
+        block_sort_kernel<K, kNtC2, kItC2, RANK><<<sms * 3, kNtC2, smem_c2, st>>>(b, lists.c2, &ctr[kCtrLocalC2]);
     }
     { LaunchScope ls_(ctx, "copy");
-        copy_kernel<K><<<sms * 4, 256, 0, st>>>(b, copy_list, &ctr[kCtrCopy]);
+        copy_kernel<K><<<sms * 4, 256, 0, st>>>(b, lists.copy, &ctr[kCtrCopy]);
     }
     FMCS_LAUNCH_CHECK("local tiers");
     return FMCS_OK;
@@ -783,9 +890,12 @@ int sort_segments(fmcs_ctx *ctx, const SortArgs &a)
     if (a.key_bits == 0 || a.key_bits > 8 * a.bank_bytes)
         return set_error(ctx, FMCS_E_INVAL, "sort: key_bits must be in 1..8*bank_bytes");
     switch (a.bank_bytes) {
-    case 2: return sort_segments_t<uint16_t>(ctx, a);
-    case 4: return sort_segments_t<uint32_t>(ctx, a);
-    case 8: return sort_segments_t<uint64_t>(ctx, a);
+    case 2: return ctx->rank_mode ? sort_segments_t<uint16_t, kRankBallot>(ctx, a)
+                                  : sort_segments_t<uint16_t, kRankMatch>(ctx, a);
+    case 4: return ctx->rank_mode ? sort_segments_t<uint32_t, kRankBallot>(ctx, a)
+                                  : sort_segments_t<uint32_t, kRankMatch>(ctx, a);
+    case 8: return ctx->rank_mode ? sort_segments_t<uint64_t, kRankBallot>(ctx, a)
+                                  : sort_segments_t<uint64_t, kRankMatch>(ctx, a);
     default: return set_error(ctx, FMCS_E_INVAL, "sort: bank_bytes must be 2, 4 or 8");
     }
 }
