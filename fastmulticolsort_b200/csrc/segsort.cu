@@ -116,7 +116,8 @@ struct Lists {
 // Route a segment (child or initial) to its tier.  Segments that need no
 // sorting (one row, or no key bits left) only need to reach BUF0.
 __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
-                                              uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L)
+                                              uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L,
+                                              uint32_t *hist_out)
 {
     if (len == 0) return;
     if (len == 1 || shift == 0) {
@@ -132,7 +133,14 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
     else if (len <= (uint32_t)kCapB2) L.b2[atomicAdd(&ctr[kCtrLocalB2], 1u)] = e;
     else if (len <= (uint32_t)kCapC1) L.c1[atomicAdd(&ctr[kCtrLocalC1], 1u)] = e;
     else if (len <= (uint32_t)kCapC2) L.c2[atomicAdd(&ctr[kCtrLocalC2], 1u)] = e;
-    else large_out[atomicAdd(&ctr[large_ctr], 1u)] = LargeSeg{start, len, shift, src};
+    else {
+        // a large segment: its digit histogram row starts at zero
+        const uint32_t slot = atomicAdd(&ctr[large_ctr], 1u);
+        large_out[slot] = LargeSeg{start, len, shift, src};
+        uint4 *row = reinterpret_cast<uint4 *>(hist_out + (uint64_t)slot * kRadix);
+#pragma unroll 4
+        for (int i = 0; i < kRadix / 4; ++i) row[i] = make_uint4(0, 0, 0, 0);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -140,7 +148,8 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
 // ---------------------------------------------------------------------------
 template <typename K>
 __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_start, const uint32_t *d_nseg,
-                                uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, Lists lists)
+                                uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, Lists lists,
+                                uint32_t *hist0)
 {
     const uint32_t nseg = seg_start ? *d_nseg : 1u;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
@@ -156,7 +165,7 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
             b.v0[start] = v;
             continue;
         }
-        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, lists);
+        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, lists, hist0);
     }
 }
 
@@ -164,12 +173,20 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
 // MSD level kernels (large segments)
 // ---------------------------------------------------------------------------
 // Exclusive prefix of the tile counts of the level's large segments (one CTA).
+// Also resets the level's counters (tile counter, rows moved, next-level
+// count) so that no separate memsets are needed.
 __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs, const uint32_t *d_nseg,
-                                                           uint32_t *tile_prefix)
+                                                           uint32_t *tile_prefix, uint32_t *reset0,
+                                                           uint32_t *reset1, uint32_t *reset2)
 {
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry;
     const uint32_t nseg = *d_nseg;
+    if (threadIdx.x == 0) {
+        *reset0 = 0;
+        *reset1 = 0;
+        *reset2 = 0;
+    }
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (uint32_t base = 0; base < nseg; base += blockDim.x) {
@@ -201,13 +218,6 @@ __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs,
     if (threadIdx.x == 0) tile_prefix[nseg] = carry;
 }
 
-__global__ void zero_hist_kernel(uint32_t *hist, const uint32_t *d_nseg)
-{
-    const uint64_t total = (uint64_t)(*d_nseg) * kRadix;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x)
-        hist[i] = 0;
-}
 
 __device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
 {
@@ -251,7 +261,7 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSe
 // Per large segment: exclusive digit offsets, skip detection, children.
 __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const uint32_t *d_nseg,
                                                           uint32_t *hist, uint32_t *ctr, int next_large_ctr,
-                                                          LargeSeg *large_next, Lists lists)
+                                                          LargeSeg *large_next, Lists lists, uint32_t *hist_next)
 {
     __shared__ uint32_t cnt[kRadix];
     __shared__ uint32_t tmp[kRadix / 32 + 1];
@@ -274,7 +284,8 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const 
         const uint32_t child_shift = sg.shift - width;
         const uint32_t child_src = skip ? sg.src : (sg.src == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
         if (c > 0)
-            route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, lists);
+            route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, lists,
+                          hist_next);
         if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
         if (d == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
         __syncthreads();
@@ -768,9 +779,10 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         if ((rc = ws_get(ctx, kSlotLocalC, cap_copy * sizeof(LargeSeg), &p))) return rc;
         lists.copy = (LargeSeg *)p;
     }
-    uint32_t *hist, *tile_prefix;
-    if ((rc = ws_get(ctx, kSlotSegHist, cap_large * kRadix * sizeof(uint32_t), &p))) return rc;
-    hist = (uint32_t *)p;
+    uint32_t *hists[2], *tile_prefix;
+    if ((rc = ws_get(ctx, kSlotSegHist, 2 * cap_large * kRadix * sizeof(uint32_t), &p))) return rc;
+    hists[0] = (uint32_t *)p;
+    hists[1] = hists[0] + cap_large * kRadix;
     if ((rc = ws_get(ctx, kSlotTilePrefix, (cap_large + 1) * sizeof(uint32_t), &p))) return rc;
     tile_prefix = (uint32_t *)p;
     const uint64_t max_tiles = n / kTileM + cap_large + 1;
@@ -791,7 +803,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                                   : 1u;
         if (seg_start && a.nseg_host == 0) grid = (unsigned)sms * 16;
         { LaunchScope ls_(ctx, "classify");
-            classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists);
+            classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists,
+                                                     hists[0]);
         }
         FMCS_LAUNCH_CHECK("classify");
     }
@@ -814,21 +827,17 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         for (int lvl = 0; lvl < levels && nlarge > 0; ++lvl) {
             const int cur = lvl & 1, nxt = cur ^ 1;
             const uint32_t *d_cnt = &ctr[kCtrLarge0 + cur];
-            cudaMemsetAsync(&ctr[kCtrLarge0 + nxt], 0, sizeof(uint32_t), st);
-            cudaMemsetAsync(&ctr[kCtrMsdTile], 0, sizeof(uint32_t), st);
-            cudaMemsetAsync(&ctr[kCtrMoved], 0, sizeof(uint32_t), st);
             { LaunchScope ls_(ctx, "tile_prefix");
-                tile_prefix_kernel<<<1, 1024, 0, st>>>(large[cur], d_cnt, tile_prefix);
+                tile_prefix_kernel<<<1, 1024, 0, st>>>(large[cur], d_cnt, tile_prefix, &ctr[kCtrLarge0 + nxt],
+                                                       &ctr[kCtrMsdTile], &ctr[kCtrMoved]);
             }
-            { LaunchScope ls_(ctx, "zero_hist");
-                zero_hist_kernel<<<sms * 2, 256, 0, st>>>(hist, d_cnt);
-            }
+            uint32_t *hist = hists[cur];
             { LaunchScope ls_(ctx, "msd_hist");
                 msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, large[cur], d_cnt, tile_prefix, hist);
             }
             { LaunchScope ls_(ctx, "msd_plan");
                 msd_plan_kernel<<<sms * 8, kRadix, 0, st>>>(large[cur], d_cnt, hist, ctr, kCtrLarge0 + nxt, large[nxt],
-                                                             lists);
+                                                             lists, hists[nxt]);
             }
             if (!a.fixed_launches) {
                 // read the next level's count while the scatter runs
