@@ -29,7 +29,7 @@ EXPORTS = (
     "fmcs_create", "fmcs_destroy", "fmcs_last_error", "fmcs_synchronize", "fmcs_stream",
     "fmcs_workspace_bytes", "fmcs_stitch", "fmcs_gather", "fmcs_sort_round", "fmcs_hash_round",
     "fmcs_run_plan", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
-    "fmcs_group_ids_noalloc",
+    "fmcs_group_ids_noalloc", "fmcs_shift_left", "fmcs_assemble", "fmcs_hash_round_unordered",
 )
 
 
@@ -78,6 +78,9 @@ def load(path: str = LIB_PATH):
     L.fmcs_launch_count.argtypes = [vp]
     L.fmcs_launch_count.restype = C.c_ulonglong
     L.fmcs_group_ids_noalloc.argtypes = [vp, vp, u32, vp, vp, u64, u32p]
+    L.fmcs_shift_left.argtypes = [vp, vp, u32, u64, u32]
+    L.fmcs_assemble.argtypes = [vp, vp, u32, u64, C.POINTER(Slice)]
+    L.fmcs_hash_round_unordered.argtypes = [vp, vp, u32, vp, vp, u64, u32p]
     _lib = L
     return L
 
@@ -191,6 +194,17 @@ class Context:
         for i, (a, bits, s, e) in enumerate(slices):
             arr[i] = Slice(_addr(a), _itemsize(a), bits, s, e)
         self._check(self._L.fmcs_stitch(self._h, arr, len(slices), _addr(bank), _itemsize(bank), n))
+        return bank
+
+    def shift_left(self, bank, nbits: int):
+        """bank <<= nbits in place (ShiftLeftBatch)."""
+        self._check(self._L.fmcs_shift_left(self._h, _addr(bank), _itemsize(bank), _len(bank), nbits))
+        return bank
+
+    def assemble(self, bank, src, src_bits: int, start: int, end: int):
+        """bank |= slice of src (AssembleFromColumn)."""
+        sl = Slice(_addr(src), _itemsize(src), src_bits, start, end)
+        self._check(self._L.fmcs_assemble(self._h, _addr(bank), _itemsize(bank), _len(bank), C.byref(sl)))
         return bank
 
     # -- (c) --------------------------------------------------------------

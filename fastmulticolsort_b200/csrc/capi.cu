@@ -172,6 +172,52 @@ extern "C" int fmcs_stitch(fmcs_ctx *ctx, const fmcs_slice *slices, uint32_t nsl
     return finish(ctx, "fmcs_stitch", nullptr, nullptr);
 }
 
+extern "C" int fmcs_shift_left(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t nbits)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (!valid_bank(bank_bytes) || (n && !bank)) return set_error(ctx, FMCS_E_INVAL, "fmcs_shift_left: invalid arguments");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_shift_left: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    int rc;
+    void *dbank;
+    bool host;
+    if ((rc = stage_out(ctx, bank, n * bank_bytes, kSlotStageOut0, &dbank, &host))) return rc;
+    if (host) {
+        cudaError_t e = cudaMemcpyAsync(dbank, bank, n * bank_bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_shift_left stage");
+    }
+    if ((rc = launch_bank_update(ctx, dbank, bank_bytes, n, nbits, nullptr, 0, 0, 0))) return rc;
+    if (host && (rc = copy_out(ctx, bank, dbank, n * bank_bytes))) return rc;
+    return finish(ctx, "fmcs_shift_left", nullptr, nullptr);
+}
+
+extern "C" int fmcs_assemble(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, const fmcs_slice *s)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (!valid_bank(bank_bytes) || !s || (n && (!bank || !s->src)) || !valid_bank(s->src_bytes) || s->src_bits == 0 ||
+        s->src_bits > 8 * s->src_bytes || s->start < 1 || s->end < s->start || s->end > s->src_bits)
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_assemble: invalid arguments");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_assemble: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    int rc;
+    const void *dsrc = nullptr;
+    if ((rc = stage_in(ctx, s->src, n * s->src_bytes, kSlotStageIn0, &dsrc))) return rc;
+    void *dbank;
+    bool host;
+    if ((rc = stage_out(ctx, bank, n * bank_bytes, kSlotStageOut0, &dbank, &host))) return rc;
+    if (host) {
+        cudaError_t e = cudaMemcpyAsync(dbank, bank, n * bank_bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_assemble stage");
+    }
+    if ((rc = launch_bank_update(ctx, dbank, bank_bytes, n, 0, dsrc, s->src_bytes, s->src_bits - s->end,
+                                 s->end - s->start + 1)))
+        return rc;
+    if (host && (rc = copy_out(ctx, bank, dbank, n * bank_bytes))) return rc;
+    return finish(ctx, "fmcs_assemble", nullptr, nullptr);
+}
+
 extern "C" int fmcs_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order, void *out,
                            uint64_t n)
 {
@@ -274,6 +320,34 @@ extern "C" int fmcs_hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_by
     return finish(ctx, "fmcs_hash_round", ngroups, d_ng);
 }
 
+extern "C" int fmcs_hash_round_unordered(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes,
+                                         const uint32_t *in_group, uint32_t *out_group, uint64_t n,
+                                         uint32_t *ngroups)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (ngroups) *ngroups = 0;
+    if (!valid_bank(bank_bytes) || (n && (!bank || !out_group)))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round_unordered: invalid arguments");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round_unordered: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    int rc;
+    const void *dbank = nullptr, *dig = nullptr;
+    if ((rc = stage_in(ctx, bank, n * bank_bytes, kSlotStageIn0, &dbank))) return rc;
+    if ((rc = stage_in(ctx, in_group, n * 4, kSlotStageIn1, &dig))) return rc;
+    void *dgroup;
+    bool h_group;
+    if ((rc = stage_out(ctx, out_group, n * 4, kSlotStageOut1, &dgroup, &h_group))) return rc;
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    if ((rc = hash_round(ctx, dbank, bank_bytes, nullptr, nullptr, (const uint32_t *)dig, (uint32_t *)dgroup, n, true,
+                         d_ng, true)))
+        return rc;
+    if (h_group && (rc = copy_out(ctx, out_group, dgroup, n * 4))) return rc;
+    return finish(ctx, "fmcs_hash_round_unordered", ngroups, d_ng);
+}
+
 extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
                              uint32_t ncols, const uint32_t *col_order, const uint32_t *split, uint32_t nbanks,
                              uint64_t n, int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
@@ -345,6 +419,7 @@ extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint3
     for (uint32_t b = 0; b < nbanks; ++b) {
         const BankPlan &bp = plan.banks[b];
         const bool last = (b + 1 == nbanks);
+        ctx->prof_round = (int)b;
         // (a) stitch the bank
         void *bank;
         if ((rc = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, &bank))) return rc;
@@ -375,6 +450,7 @@ extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint3
         }
         in_group = og;
     }
+    ctx->prof_round = -1;
     if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
     if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
     return finish(ctx, "fmcs_run_plan", ngroups, d_ng);

@@ -111,7 +111,7 @@ LaunchScope::LaunchScope(fmcs_ctx *ctx, const char *name) : ctx_(ctx)
 {
     ctx->launches++;
     if (!ctx->prof_on) return;
-    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx), 0.0};
+    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx), 0.0, ctx->prof_round};
     if (!r.a || !r.b) return;
     cudaEventRecord(r.a, ctx->stream);
     rec_ = (int)ctx->prof.size();
@@ -235,6 +235,7 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         double units = 0;
     };
     std::vector<Agg> agg;
+    std::vector<double> round_ms;
     for (auto &r : ctx->prof) {
         float ms = 0;
         if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) {
@@ -247,6 +248,11 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         agg[k].n++;
         agg[k].ms += ms;
         agg[k].units += r.units;
+        // per-round totals of the sort/hash work (the stitch is reported apart)
+        if (r.round >= 0 && strcmp(r.name, "stitch") != 0) {
+            if ((int)round_ms.size() <= r.round) round_ms.resize(r.round + 1, 0.0);
+            round_ms[r.round] += ms;
+        }
         ctx->ev_pool.push_back(r.a);
         ctx->ev_pool.push_back(r.b);
     }
@@ -257,6 +263,15 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"units\": %.0f}",
                  k ? ", " : "", agg[k].name.c_str(), agg[k].n, agg[k].ms, agg[k].units);
         out += tmp;
+    }
+    if (!round_ms.empty()) {
+        out += agg.empty() ? "\"_round_ms\": [" : ", \"_round_ms\": [";
+        for (size_t r = 0; r < round_ms.size(); ++r) {
+            char tmp[64];
+            snprintf(tmp, sizeof(tmp), "%s%.6f", r ? ", " : "", round_ms[r]);
+            out += tmp;
+        }
+        out += "]";
     }
     out += "}";
     if (out.size() + 1 > len) return set_error(ctx, FMCS_E_INVAL, "fmcs_profile_report: buffer too small");

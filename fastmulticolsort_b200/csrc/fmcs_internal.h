@@ -61,6 +61,7 @@ struct fmcs_prof_rec {
     const char *name;
     cudaEvent_t a, b;
     double units;   // work items of the launch (rows), when the launcher knows them
+    int round;      // sort/hash round of a plan the launch belongs to (-1: none)
 };
 
 struct fmcs_ctx {
@@ -82,6 +83,7 @@ struct fmcs_ctx {
     unsigned long long launches = 0;   // kernels launched by this context
     cudaEvent_t ev_level = nullptr;    // host-side read-back point of the sort levels
     int rank_mode = 0;                 // 0: match.any multi-split, 1: ballot multi-split
+    int prof_round = -1;               // round tag of the launches being profiled
 };
 
 namespace fmcs {
@@ -119,6 +121,10 @@ struct StitchSlice {
 constexpr int kMaxSlices = 32;
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
                   uint64_t n);
+
+// bank[i] <<= lshift (src == NULL) or bank[i] |= (src[i] >> rshift) & mask(width)
+int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,
+                       const void *src, uint32_t src_bytes, uint32_t rshift, uint32_t width);
 
 // ---------------------------------------------------------------- gather
 int launch_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order,
@@ -163,6 +169,6 @@ int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64
 // ---------------------------------------------------------------- hash grouping
 int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
                uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n,
-               bool last_round, uint32_t *d_ngroups);
+               bool last_round, uint32_t *d_ngroups, bool group_is_key = false);
 
 }  // namespace fmcs

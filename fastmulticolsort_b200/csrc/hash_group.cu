@@ -121,7 +121,7 @@ int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const ui
 
 int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
                uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n, bool last_round,
-               uint32_t *d_ngroups)
+               uint32_t *d_ngroups, bool group_is_key)
 {
     if (n == 0) return FMCS_OK;
     cudaStream_t st = ctx->stream;
@@ -142,14 +142,21 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     uint32_t *d_cnt = (uint32_t *)p + 32;   // words 32..39 belong to the hash round
     uint32_t *seg_start = nullptr;
-    if (in_group) {
+    // The key of a row is (its parent run, its value): the run id from a
+    // boundary scan of in_group, or -- when the previous ids are not clustered
+    // (group_is_key) -- the previous id itself, over one numbering in row order.
+    const uint32_t *keyrun = nullptr;
+    if (in_group && group_is_key) {
+        keyrun = in_group;
+    } else if (in_group) {
         if ((rc = launch_group_ids(ctx, nullptr, 0, in_group, run, n, nullptr))) return rc;
+        keyrun = run;
     }
     switch (bank_bytes) {
-    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
-    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
-    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
-    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, in_group ? run : nullptr, n, rep, minpos, cap - 1, slot_of); break;
+    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
+    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
+    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
+    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
     default: return set_error(ctx, FMCS_E_INVAL, "hash round: bank_bytes must be 1, 2, 4 or 8");
     }
     if (rc) return rc;

@@ -10,6 +10,8 @@
 // moves exactly sum(source bytes) + bank bytes per row.
 #include "fmcs_internal.h"
 
+#include <algorithm>
+
 namespace fmcs {
 
 namespace {
@@ -113,7 +115,46 @@ __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ Sti
     }
 }
 
+// Slice-at-a-time primitives (the reference's ShiftLeftBatch / AssembleFromColumn).
+template <typename B>
+__global__ void __launch_bounds__(256) bank_update_kernel(B *bank, uint64_t n, uint32_t lshift, const void *src,
+                                                          uint32_t src_bytes, uint32_t rshift, uint32_t width)
+{
+    const uint64_t mask = width >= 64 ? ~0ull : ((1ull << width) - 1);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (!src) {
+            bank[i] = lshift >= 8 * sizeof(B) ? B(0) : (B)((uint64_t)bank[i] << lshift);
+        } else {
+            uint64_t v;
+            switch (src_bytes) {
+            case 1: v = ((const uint8_t *)src)[i]; break;
+            case 2: v = ((const uint16_t *)src)[i]; break;
+            case 4: v = ((const uint32_t *)src)[i]; break;
+            default: v = ((const uint64_t *)src)[i]; break;
+            }
+            bank[i] = (B)((uint64_t)bank[i] | ((v >> rshift) & mask));
+        }
+    }
+}
+
 }  // namespace
+
+int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,
+                       const void *src, uint32_t src_bytes, uint32_t rshift, uint32_t width)
+{
+    if (n == 0) return FMCS_OK;
+    const unsigned grid = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    LaunchScope ls_(ctx, src ? "assemble" : "shift_left");
+    switch (bank_bytes) {
+    case 1: bank_update_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>((uint8_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 2: bank_update_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>((uint16_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 4: bank_update_kernel<uint32_t><<<grid, 256, 0, ctx->stream>>>((uint32_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 8: bank_update_kernel<uint64_t><<<grid, 256, 0, ctx->stream>>>((uint64_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    default: return set_error(ctx, FMCS_E_INVAL, "bank_bytes must be 1, 2, 4 or 8");
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "bank update launch");
+}
 
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
                   uint64_t n)

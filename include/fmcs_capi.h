@@ -90,6 +90,17 @@ typedef struct {
 FMCS_API int fmcs_stitch(fmcs_ctx *ctx, const fmcs_slice *slices, uint32_t nslices,
                 void *bank, uint32_t bank_bytes, uint64_t n);
 
+/* Slice-at-a-time bank building, exactly the reference's two whole-column
+ * primitives (for code that builds banks itself; fmcs_stitch is the fused
+ * one-pass form):
+ *   fmcs_shift_left: bank[i] <<= nbits, truncated to the bank width
+ *                    (SpecialiedColumn<T>::ShiftLeftBatch, src/column.h:105-180);
+ *   fmcs_assemble:   bank[i] |= (src[i] >> (src_bits - end)) & mask(end-start+1)
+ *                    (SpecialiedColumn<T>::AssembleFromColumn, src/column.h:208-1060). */
+FMCS_API int fmcs_shift_left(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t nbits);
+FMCS_API int fmcs_assemble(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n,
+                           const fmcs_slice *slice);
+
 /* (c) out[i] = bank[order[i]] (Composer::BATproject, src/composer.cpp:608-628). */
 FMCS_API int fmcs_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes,
                 const uint32_t *order, void *out, uint64_t n);
@@ -125,6 +136,15 @@ FMCS_API int fmcs_sort_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_byte
 FMCS_API int fmcs_hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes,
                     uint32_t *order, const uint32_t *in_group, uint32_t *out_group,
                     uint64_t n, int last_round, uint32_t *ngroups);
+
+/* (e) One hash-grouping round WITHOUT re-clustering (hash_type 0:
+ * Composer::hashByGroup_non_reordered, src/composer.cpp:1153-1219, with
+ * Hashing::subgroup_first_round / subgroup_non_first_round, src/hashing.h:387-422,
+ * 96-148): out_group[i] = dense id of the pair (in_group[i], bank[i]) numbered
+ * by first appearance in ROW order (in_group NULL: of bank[i] alone). */
+FMCS_API int fmcs_hash_round_unordered(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes,
+                                       const uint32_t *in_group, uint32_t *out_group, uint64_t n,
+                                       uint32_t *ngroups);
 
 /* Whole massaged plan (StitchComposer::run_single_plan,
  * src/stitch_composer.cpp:555-806 + multiRoundSorting, src/composer.cpp:48-135,

@@ -305,6 +305,40 @@ int orc_hash_round(const void *bank, uint32_t bank_bytes, uint32_t *order,
 }
 
 /* ------------------------------------------------------------------------ */
+/* hash grouping without re-clustering, src/hashing.h:96-148, 387-422         */
+/* ------------------------------------------------------------------------ */
+int orc_hash_unordered(const void *bank, uint32_t bank_bytes, const uint32_t *in_group,
+                       uint32_t *out_group, uint64_t n, uint32_t *ngroups)
+{
+    if (!valid_bytes(bank_bytes)) return -1;
+    if (ngroups) *ngroups = 0;
+    if (n == 0) return 0;
+    uint64_t ts = 16;
+    while (ts < 2 * n) ts <<= 1;
+    uint32_t *slot_row = (uint32_t *)malloc(ts * sizeof(uint32_t));
+    if (!slot_row) return -2;
+    memset(slot_row, 0xFF, ts * sizeof(uint32_t));
+    uint32_t next = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        uint64_t k = ld(bank, bank_bytes, i);
+        uint32_t g = in_group ? in_group[i] : 0;
+        uint64_t h = mix64(k ^ ((uint64_t)g * 0x9E3779B97F4A7C15ULL)) & (ts - 1);
+        for (;;) {
+            uint32_t r = slot_row[h];
+            if (r == 0xFFFFFFFFu) { slot_row[h] = (uint32_t)i; out_group[i] = next++; break; }
+            if (ld(bank, bank_bytes, r) == k && (!in_group || in_group[r] == g)) {
+                out_group[i] = out_group[r];
+                break;
+            }
+            h = (h + 1) & (ts - 1);
+        }
+    }
+    if (ngroups) *ngroups = next;
+    free(slot_row);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* whole plans                                                               */
 /* ------------------------------------------------------------------------ */
 static int build_banks(const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,

@@ -92,6 +92,14 @@ int orc_hash_round(const void *bank, uint32_t bank_bytes, uint32_t *order,
                    uint32_t *group_idx, uint64_t n, int last_round,
                    uint32_t *ngroups);
 
+/* Hash grouping without re-clustering (hash_type 0; Composer::
+ * hashByGroup_non_reordered, src/composer.cpp:1153-1219, Hashing::
+ * subgroup_first_round / subgroup_non_first_round, src/hashing.h:387-422 and
+ * 96-148): out_group[i] = id of (in_group[i], bank[i]) (in_group NULL: bank[i])
+ * numbered by first appearance in row order. */
+int orc_hash_unordered(const void *bank, uint32_t bank_bytes, const uint32_t *in_group,
+                       uint32_t *out_group, uint64_t n, uint32_t *ngroups);
+
 /* Whole plan, sort path: stitch each bank then chain the rounds
  * (run_single_plan, src/stitch_composer.cpp:555-806 + multiRoundSorting,
  * src/composer.cpp:48-135).  cols[c] has col_bytes[c] bytes per row and

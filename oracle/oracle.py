@@ -57,6 +57,7 @@ def lib():
                                      C.c_void_p, C.c_uint64, _u32p]
         L.orc_hash_round.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_uint64, C.c_int, _u32p]
+        L.orc_hash_unordered.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, _u32p]
         for f in (L.orc_run_plan_sort, L.orc_run_plan_hash):
             f.argtypes = [C.POINTER(C.c_void_p), _u32p, _u32p, C.c_uint32, _u32p, C.c_uint32,
                           C.c_uint64, C.c_void_p, C.c_void_p, _u32p]
@@ -165,6 +166,17 @@ def hash_round(bank: np.ndarray, order=None, in_group=None, last_round=False):
                                 _ptr(ig), _ptr(out_group), _ptr(idx), n, 1 if last_round else 0,
                                 C.byref(ng)), "orc_hash_round")
     return order, out_group, idx, ng.value
+
+
+def hash_unordered(bank: np.ndarray, in_group=None):
+    """Returns (group ids in row order, ngroups)."""
+    n = bank.shape[0]
+    out = np.zeros(n, np.uint32)
+    ng = C.c_uint32(0)
+    ig = None if in_group is None else np.ascontiguousarray(in_group, np.uint32)
+    _check(lib().orc_hash_unordered(_ptr(np.ascontiguousarray(bank)), bank.dtype.itemsize, _ptr(ig), _ptr(out), n,
+                                    C.byref(ng)), "orc_hash_unordered")
+    return out, ng.value
 
 
 def _plan_args(cols, bw, split):

@@ -174,3 +174,47 @@ def test_invalid_arguments(ctx):
     # the context keeps working after errors
     ng = ctx.sort_round(np.arange(10, dtype=np.uint64)[::-1].copy(), 8, order, out_group=np.zeros(10, np.uint32))
     assert ng == 10 and list(order) == list(range(9, -1, -1))
+
+
+@pytest.mark.parametrize("bank_bytes", [1, 2, 4, 8])
+def test_shift_left_and_assemble(ctx, bank_bytes):
+    rng = np.random.default_rng(bank_bytes + 100)
+    n = 70001
+    dt = np.dtype(f"u{bank_bytes}")
+    bank = rng.integers(0, 255, size=n, dtype=np.uint64).astype(dt)
+    src = rng.integers(0, 1 << 20, size=n, dtype=np.uint64).astype(np.uint32)
+    b = bank.copy()
+    ctx.shift_left(b, 3)
+    assert np.array_equal(b, (bank.astype(np.uint64) << np.uint64(3)).astype(dt))
+    ctx.assemble(b, src, 20, 18, 20)   # the low 3 bits of a 20-bit column
+    exp = ((bank.astype(np.uint64) << np.uint64(3)) | (src.astype(np.uint64) & np.uint64(7))).astype(dt)
+    assert np.array_equal(b, exp)
+
+
+@pytest.mark.parametrize("bank_bytes,distinct", [(1, 30), (4, 5000), (8, 100000)])
+def test_hash_round_unordered(ctx, bank_bytes, distinct):
+    from fastmulticolsort_b200 import capi
+    rng = np.random.default_rng(distinct)
+    n = 150000
+    pool = rng.integers(0, 1 << (8 * bank_bytes - 1), size=distinct, dtype=np.uint64)
+    bank = pool[rng.integers(0, distinct, size=n)].astype(np.dtype(f"u{bank_bytes}"))
+    prev = rng.integers(0, 40, size=n, dtype=np.uint32)
+    for ig in (None, prev):
+        out = np.zeros(n, np.uint32)
+        ng = C_hash_unordered(ctx, bank, ig, out)
+        ref, ng_ref = O.hash_unordered(bank, ig)
+        assert ng == ng_ref and np.array_equal(out, ref)
+
+
+def C_hash_unordered(ctx, bank, in_group, out):
+    import ctypes
+    from fastmulticolsort_b200 import capi
+    L = capi.load()
+    L.fmcs_hash_round_unordered.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]
+    ng = ctypes.c_uint32(0)
+    rc = L.fmcs_hash_round_unordered(ctx.handle, bank.ctypes.data, bank.dtype.itemsize,
+                                     None if in_group is None else in_group.ctypes.data, out.ctypes.data,
+                                     bank.shape[0], ctypes.byref(ng))
+    assert rc == 0
+    return ng.value
