@@ -275,6 +275,47 @@ def time_steps(ctx, stream, fn, steps):
     return total, per
 
 
+def zipf_segmented(ctx, stream, n: int, reps: int):
+    """Zipf-skewed segmented workload: col0 20-bit codes drawn Zipf(1.0) over 2^20
+    values, col1 uniform 24-bit, col2 uniform 40-bit.  Plain comparator: one
+    full-array LSD sort per column (fmcs_sort_round_plain, no segments, no
+    binning); segmented: the same three rounds through the size-binned engine;
+    massaged: the cost model's plan through fmcs_run_plan."""
+    import torch
+    from fastmulticolsort_b200 import capi
+    from fastmulticolsort_b200 import workloads as W
+    cols, bw = W.cols_zipf(n)
+    dcols = [torch.from_numpy(c.view(np.int32 if c.dtype == np.uint32 else np.int64)).cuda() for c in cols]
+    order = torch.empty(n, dtype=torch.int32, device="cuda")
+    group = torch.empty(n, dtype=torch.int32, device="cuda")
+    g2 = torch.empty_like(group)
+    sizes = np.bincount(cols[0].astype(np.int64), minlength=1 << 20)
+    card = [int((sizes > 0).sum()), 1 << 24, min(n, 1 << 40)]
+    plan, _, est = capi.optimize_plan(bw, card, [4, 4, 8], n)
+
+    def plain():
+        ctx.sort_round_plain(dcols[0], 20, order, out_group=group)
+        ctx.sort_round_plain(dcols[1], 24, order, in_group=group, out_group=g2)
+        ctx.sort_round_plain(dcols[2], 40, order, in_group=g2, out_group=group)
+
+    def segmented():
+        ctx.run_plan(dcols, bw, [20, 24, 40], order, group)
+
+    def massaged():
+        ctx.run_plan(dcols, bw, plan, order, group)
+
+    out = {"rows": n, "columns": "20-bit Zipf(1.0) over 2^20 codes (u32), 24-bit (u32), 40-bit (u64)",
+           "largest_group": int(sizes.max()), "groups_col0": card[0], "plan_chosen": plan}
+    for name, fn in (("plain_ms", plain), ("segmented_ms", segmented), ("massaged_ms", massaged)):
+        fn()
+        total, per = time_steps(ctx, stream, fn, reps)
+        out[name] = round(total / reps, 3)
+    best = min(out["segmented_ms"], out["massaged_ms"])
+    out["speedup_vs_plain"] = round(out["plain_ms"] / best, 3)
+    out["value_mrows_s"] = round(n / (best / 1e3) / 1e6, 1)
+    return out
+
+
 def run_fmcs(args):
     import torch
     from fastmulticolsort_b200 import capi
@@ -401,6 +442,8 @@ def run_fmcs(args):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if not args.no_zipf:
+        line["zipf_segmented"] = zipf_segmented(ctx, stream, args.zipf_rows, max(3, min(args.steps, 10)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cols, bw, SPLIT, args.cpu_runs)
         line["cpu_baseline"].pop("seconds", None)
@@ -419,6 +462,8 @@ def main():
     ap.add_argument("--impl", default="fmcs", choices=["fmcs", "reference"])
     ap.add_argument("--cpu-runs", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-zipf", action="store_true", help="skip the Zipf segmented comparison")
+    ap.add_argument("--zipf-rows", type=int, default=67_108_864)
     ap.add_argument("--only-steps", action="store_true",
                     help="warm-up and timed steps only (no comparators, e2e or CPU baseline): "
                          "the command the ncu captures profile")

@@ -30,6 +30,7 @@ EXPORTS = (
     "fmcs_workspace_bytes", "fmcs_stitch", "fmcs_gather", "fmcs_sort_round", "fmcs_hash_round",
     "fmcs_run_plan", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
     "fmcs_group_ids_noalloc", "fmcs_shift_left", "fmcs_assemble", "fmcs_hash_round_unordered",
+    "fmcs_sort_round_plain", "fmcs_optimize_plan", "fmcs_set_tuning", "fmcs_get_tuning",
 )
 
 
@@ -81,6 +82,12 @@ def load(path: str = LIB_PATH):
     L.fmcs_shift_left.argtypes = [vp, vp, u32, u64, u32]
     L.fmcs_assemble.argtypes = [vp, vp, u32, u64, C.POINTER(Slice)]
     L.fmcs_hash_round_unordered.argtypes = [vp, vp, u32, vp, vp, u64, u32p]
+    L.fmcs_sort_round_plain.argtypes = [vp, vp, u32, u32, vp, vp, vp, vp, u64, u32p]
+    L.fmcs_set_tuning.argtypes = [vp, C.c_char_p, C.c_longlong]
+    L.fmcs_get_tuning.argtypes = [vp, C.c_char_p]
+    L.fmcs_get_tuning.restype = C.c_longlong
+    L.fmcs_optimize_plan.argtypes = [u32p, C.POINTER(C.c_uint64), u32p, u32, u64, i32, u32p, u32, u32p, u32p,
+                                     C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -124,6 +131,21 @@ def group_ids_noalloc(keys, out_group, in_group=None, stream: int = 0) -> int:
     if rc != FMCS_OK:
         raise FmcsError(rc, "fmcs_group_ids_noalloc failed")
     return ng.value
+
+
+def optimize_plan(bw, cardinality, col_bytes, n: int, ordered: bool = True):
+    """Cost-model plan search; returns (split, column order, estimated ms)."""
+    L = load()
+    k = len(bw)
+    split = (C.c_uint32 * 64)()
+    nb = C.c_uint32(0)
+    order = (C.c_uint32 * k)()
+    est = C.c_double(0)
+    rc = L.fmcs_optimize_plan(_u32arr(bw), (C.c_uint64 * k)(*[int(c) for c in cardinality]), _u32arr(col_bytes),
+                              k, n, 1 if ordered else 0, split, 64, C.byref(nb), order, C.byref(est))
+    if rc != FMCS_OK:
+        raise FmcsError(rc, "fmcs_optimize_plan failed")
+    return [split[i] for i in range(nb.value)], [order[i] for i in range(k)], est.value
 
 
 class Context:
@@ -183,6 +205,12 @@ class Context:
     def launch_count(self) -> int:
         return int(self._L.fmcs_launch_count(self._h))
 
+    def set_tuning(self, key: str, value: int):
+        self._check(self._L.fmcs_set_tuning(self._h, key.encode(), int(value)))
+
+    def get_tuning(self, key: str) -> int:
+        return int(self._L.fmcs_get_tuning(self._h, key.encode()))
+
     def workspace_bytes(self) -> int:
         return int(self._L.fmcs_workspace_bytes(self._h))
 
@@ -220,6 +248,21 @@ class Context:
         self._check(self._L.fmcs_sort_round(self._h, _addr(bank), _itemsize(bank), key_bits,
                                             _addr(order), _addr(in_group), _addr(out_group),
                                             _addr(sorted_bank), _len(bank), C.byref(ng)))
+        return ng.value
+
+    def sort_round_plain(self, bank, key_bits: int, order, in_group=None, out_group=None,
+                         sorted_bank=None) -> int:
+        """The unsegmented comparator round (full-array LSD passes)."""
+        ng = C.c_uint32(0)
+        self._check(self._L.fmcs_sort_round_plain(self._h, _addr(bank), _itemsize(bank), key_bits,
+                                                  _addr(order), _addr(in_group), _addr(out_group),
+                                                  _addr(sorted_bank), _len(bank), C.byref(ng)))
+        return ng.value
+
+    def hash_round_unordered(self, bank, out_group, in_group=None) -> int:
+        ng = C.c_uint32(0)
+        self._check(self._L.fmcs_hash_round_unordered(self._h, _addr(bank), _itemsize(bank), _addr(in_group),
+                                                      _addr(out_group), _len(bank), C.byref(ng)))
         return ng.value
 
     # -- (e) --------------------------------------------------------------

@@ -278,6 +278,73 @@ extern "C" int fmcs_sort_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_by
     return finish(ctx, "fmcs_sort_round", ngroups, out_group ? d_ng : nullptr);
 }
 
+extern "C" int fmcs_sort_round_plain(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits,
+                                     uint32_t *order, const uint32_t *in_group, uint32_t *out_group,
+                                     void *sorted_bank, uint64_t n, uint32_t *ngroups)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (ngroups) *ngroups = 0;
+    if (!(bank_bytes == 2 || bank_bytes == 4 || bank_bytes == 8) || key_bits == 0 || key_bits > 8 * bank_bytes)
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round_plain: bad bank width or key_bits");
+    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round_plain: n must be < 2^32");
+    if (n == 0) return FMCS_OK;
+    if (!bank || !order) return set_error(ctx, FMCS_E_INVAL, "fmcs_sort_round_plain: bank and order are required");
+    int rc;
+    void *p;
+    const void *dbank = nullptr, *dig = nullptr;
+    if ((rc = stage_in(ctx, bank, n * bank_bytes, kSlotStageIn0, &dbank))) return rc;
+    if ((rc = stage_in(ctx, in_group, n * 4, kSlotStageIn1, &dig))) return rc;
+    void *dorder, *dgroup, *dkeys;
+    bool h_order, h_group, h_keys;
+    if ((rc = stage_out(ctx, order, n * 4, kSlotStageOut0, &dorder, &h_order))) return rc;
+    if (h_order && in_group) {
+        cudaError_t e = cudaMemcpyAsync(dorder, order, n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_sort_round_plain stage order");
+    }
+    if ((rc = stage_out(ctx, out_group, n * 4, kSlotStageOut1, &dgroup, &h_group))) return rc;
+    if ((rc = stage_out(ctx, sorted_bank, n * bank_bytes, kSlotStageOut2, &dkeys, &h_keys))) return rc;
+    void *kg;
+    if ((rc = ws_get(ctx, kSlotKeys0, n * bank_bytes, &kg))) return rc;
+    if ((rc = ws_get(ctx, kSlotMisc, 3 * n * sizeof(uint32_t), &p))) return rc;
+    uint32_t *pos = (uint32_t *)p, *grp = pos + n, *tmp = grp + n;
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    cudaStream_t st = ctx->stream;
+    // keys of this round in the previous order, positions as payload
+    if (in_group) {
+        if ((rc = launch_gather(ctx, dbank, bank_bytes, (const uint32_t *)dorder, kg, n))) return rc;
+    } else {
+        cudaMemcpyAsync(kg, dbank, n * bank_bytes, cudaMemcpyDeviceToDevice, st);
+    }
+    if ((rc = launch_iota(ctx, pos, n))) return rc;
+    // full-array passes over the key, then (later rounds) over the group id
+    if ((rc = lsd_sort_full(ctx, kg, bank_bytes, pos, n, key_bits))) return rc;
+    if (in_group) {
+        if ((rc = launch_gather(ctx, dig, 4, pos, grp, n))) return rc;
+        cudaMemcpyAsync(ctx->h_small + 2, (const uint32_t *)dig + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_sort_round_plain sync");
+        uint32_t gbits = 1;
+        while (gbits < 32 && (1ull << gbits) <= (uint64_t)ctx->h_small[2]) gbits++;
+        if ((rc = lsd_sort_full(ctx, grp, 4, pos, n, gbits))) return rc;
+        // order_out[i] = order_in[pos[i]]
+        cudaMemcpyAsync(tmp, dorder, n * 4, cudaMemcpyDeviceToDevice, st);
+        if ((rc = launch_gather(ctx, tmp, 4, pos, dorder, n))) return rc;
+        if ((rc = launch_gather(ctx, dbank, bank_bytes, (const uint32_t *)dorder, kg, n))) return rc;
+    } else {
+        cudaMemcpyAsync(dorder, pos, n * 4, cudaMemcpyDeviceToDevice, st);
+    }
+    if (dkeys) cudaMemcpyAsync(dkeys, kg, n * bank_bytes, cudaMemcpyDeviceToDevice, st);
+    if (dgroup && (rc = launch_group_ids(ctx, kg, bank_bytes, in_group ? grp : nullptr, (uint32_t *)dgroup, n, d_ng)))
+        return rc;
+    if (h_order && (rc = copy_out(ctx, order, dorder, n * 4))) return rc;
+    if (h_group && (rc = copy_out(ctx, out_group, dgroup, n * 4))) return rc;
+    if (h_keys && (rc = copy_out(ctx, sorted_bank, dkeys, n * bank_bytes))) return rc;
+    return finish(ctx, "fmcs_sort_round_plain", ngroups, out_group ? d_ng : nullptr);
+}
+
 extern "C" int fmcs_hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t *order,
                                const uint32_t *in_group, uint32_t *out_group, uint64_t n, int last_round,
                                uint32_t *ngroups)

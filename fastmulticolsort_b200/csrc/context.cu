@@ -4,8 +4,12 @@
 // bounded waits report through, and error strings.
 #include "fmcs_internal.h"
 
+#include <dlfcn.h>
+
 #include <cstdio>
 #include <cstdlib>
+#include <fstream>
+#include <sstream>
 #include <cstring>
 
 namespace fmcs {
@@ -140,6 +144,46 @@ bool is_device_ptr(const void *p)
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
+// Knobs of the autotuner's JSON (tuning/b200.json next to the library, or the
+// file FMCS_TUNING names): "rank_mode", "local_max", "msd_items".
+static bool json_number(const std::string &txt, const char *key, double *out)
+{
+    const std::string pat = std::string("\"") + key + "\"";
+    size_t p = txt.find(pat);
+    if (p == std::string::npos) return false;
+    p = txt.find(':', p);
+    if (p == std::string::npos) return false;
+    char *end = nullptr;
+    const double v = strtod(txt.c_str() + p + 1, &end);
+    if (end == txt.c_str() + p + 1) return false;
+    *out = v;
+    return true;
+}
+
+static void load_tuning(fmcs_ctx *ctx)
+{
+    std::string path;
+    if (const char *env = getenv("FMCS_TUNING")) {
+        path = env;
+    } else {
+        Dl_info info;
+        if (dladdr((void *)&load_tuning, &info) && info.dli_fname) {
+            std::string f = info.dli_fname;
+            size_t sl = f.rfind('/');
+            path = (sl == std::string::npos ? std::string(".") : f.substr(0, sl)) + "/tuning/b200.json";
+        }
+    }
+    std::ifstream f(path);
+    if (!f) return;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string txt = ss.str();
+    double v;
+    if (json_number(txt, "rank_mode", &v)) ctx->rank_mode = v != 0.0 ? 1 : 0;
+    if (json_number(txt, "local_max", &v) && v >= 128 && v <= 4096) ctx->local_max = (uint32_t)v;
+    if (json_number(txt, "msd_items", &v)) ctx->msd_items = v >= 16 ? 16 : 8;
+}
+
 }  // namespace fmcs
 
 using namespace fmcs;
@@ -172,6 +216,7 @@ extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
         return FMCS_E_CUDA;
     }
     *ctx->h_status = 0;
+    load_tuning(ctx);
     if (const char *m = getenv("FMCS_RANK_MODE")) ctx->rank_mode = (m[0] == 'b' || m[0] == '1') ? 1 : 0;
     *out = ctx;
     return FMCS_OK;
@@ -277,4 +322,32 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
     if (out.size() + 1 > len) return set_error(ctx, FMCS_E_INVAL, "fmcs_profile_report: buffer too small");
     memcpy(buf, out.c_str(), out.size() + 1);
     return FMCS_OK;
+}
+
+extern "C" int fmcs_set_tuning(fmcs_ctx *ctx, const char *key, long long value)
+{
+    if (!ctx || !key) return FMCS_E_INVAL;
+    const std::string k(key);
+    if (k == "rank_mode") {
+        ctx->rank_mode = value ? 1 : 0;
+    } else if (k == "local_max") {
+        if (value < 128 || value > 4096) return set_error(ctx, FMCS_E_INVAL, "local_max must be in 128..4096");
+        ctx->local_max = (uint32_t)value;
+    } else if (k == "msd_items") {
+        if (value != 8 && value != 16) return set_error(ctx, FMCS_E_INVAL, "msd_items must be 8 or 16");
+        ctx->msd_items = (uint32_t)value;
+    } else {
+        return set_error(ctx, FMCS_E_INVAL, "unknown tuning key " + k);
+    }
+    return FMCS_OK;
+}
+
+extern "C" long long fmcs_get_tuning(const fmcs_ctx *ctx, const char *key)
+{
+    if (!ctx || !key) return -1;
+    const std::string k(key);
+    if (k == "rank_mode") return ctx->rank_mode;
+    if (k == "local_max") return ctx->local_max;
+    if (k == "msd_items") return ctx->msd_items;
+    return -1;
 }

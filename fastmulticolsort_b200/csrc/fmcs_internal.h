@@ -82,7 +82,10 @@ struct fmcs_ctx {
     std::vector<cudaEvent_t> ev_pool;
     unsigned long long launches = 0;   // kernels launched by this context
     cudaEvent_t ev_level = nullptr;    // host-side read-back point of the sort levels
+    // tuned knobs (the autotuner's tuning/b200.json, FMCS_TUNING, or fmcs_set_tuning)
     int rank_mode = 0;                 // 0: match.any multi-split, 1: ballot multi-split
+    uint32_t local_max = 4096;         // segments above this many rows take the MSD levels
+    uint32_t msd_items = 8;            // items per thread of an MSD tile (8 or 16)
     int prof_round = -1;               // round tag of the launches being profiled
 };
 
@@ -145,6 +148,9 @@ struct SortArgs {
     bool fixed_launches = false;  // launch every level (no host read-back), e.g. under graph capture
 };
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
+// Stable full-array LSD radix sort of (keys, vals) in place by key bits
+// [0, bits): the plain, unsegmented comparator path.
+int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits);
 
 // ---------------------------------------------------------------- group ids / segments
 // out_group[i] = number of boundaries in (0, i], boundary at i when

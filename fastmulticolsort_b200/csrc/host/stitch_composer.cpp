@@ -579,3 +579,45 @@ void StitchComposer::TwoRoundsExhaustive_hash()
 }
 
 }  // namespace multiAttrSort
+
+// ================================================================ C ABI
+extern "C" FMCS_API int fmcs_optimize_plan(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes,
+                                           uint32_t ncols, uint64_t n, int ordered, uint32_t *split_out,
+                                           uint32_t max_banks, uint32_t *nbanks_out, uint32_t *col_order_out,
+                                           double *est_ms)
+{
+    using namespace multiAttrSort;
+    if (!bw || !cardinality || !col_bytes || !split_out || !nbanks_out || ncols == 0 || ncols > 64)
+        return FMCS_E_INVAL;
+    try {
+        std::vector<SpecialiedColumn<uint64_t>> cols(ncols);   // statistics only: no data is touched
+        std::vector<Column *> ptrs(ncols);
+        std::vector<uint32_t> widths(bw, bw + ncols);
+        uint32_t sum = 0;
+        for (uint32_t c = 0; c < ncols; ++c) {
+            if (bw[c] == 0 || bw[c] > 64) return FMCS_E_INVAL;
+            cols[c].SetWidth(col_bytes[c]);
+            cols[c].SetCardinality(cardinality[c]);
+            ptrs[c] = &cols[c];
+            sum += bw[c];
+        }
+        compose_params_t params;
+        params.bitwidth = widths.data();
+        params.colwidth_sum = sum;
+        params.ordered = ordered ? 1 : 0;
+        setting_t setting;
+        StitchComposer sc(setting, ncols, n, params, ptrs.data());
+        std::vector<uint32_t> order;
+        double est = 0.0;
+        std::vector<uint32_t> plan = sc.OptimizePlan(&order, &est);
+        if (plan.empty() || plan.size() > max_banks) return FMCS_E_INVAL;
+        for (size_t i = 0; i < plan.size(); ++i) split_out[i] = plan[i];
+        *nbanks_out = (uint32_t)plan.size();
+        if (col_order_out)
+            for (uint32_t c = 0; c < ncols; ++c) col_order_out[c] = order[c];
+        if (est_ms) *est_ms = est;
+        return FMCS_OK;
+    } catch (...) {
+        return FMCS_E_INVAL;
+    }
+}

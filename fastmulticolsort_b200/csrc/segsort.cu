@@ -43,14 +43,16 @@ constexpr uint32_t kSkipBit = 0x100;
 
 // Local tiers: a segment goes to the smallest tier whose capacity holds it, so
 // that each kernel's unrolled item steps match the segment (few idle steps).
+constexpr int kCapT = 16;    // thread per segment: registers, odd-even transposition network
 constexpr int kCapA = 128;   // warp per segment: 32 lanes x 4 items
 constexpr int kItemsA = 4;
 constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
 constexpr int kNtB2 = 128, kItB2 = 8, kCapB2 = kNtB2 * kItB2;   // 1024
 constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
 constexpr int kNtC2 = 256, kItC2 = 16, kCapC2 = kNtC2 * kItC2;  // 4096
-constexpr int kCapLocal = kCapC2;                               // larger: MSD levels
-constexpr int kNtM = 256, kItM = 8, kTileM = kNtM * kItM;       // MSD tile, 2048 rows
+constexpr int kCapLocal = kCapC2;   // largest segment a local tier can take; larger: MSD levels
+constexpr int kNtM = 256;           // MSD tile: 256 threads x IT items (IT = 8 or 16, tuned)
+constexpr int kTileMin = kNtM * 8;
 
 // counters slot words
 constexpr int kCtrMsdTile = 1;
@@ -62,6 +64,10 @@ constexpr int kCtrCopy = 7;
 constexpr int kCtrMoved = 8;    // rows the current level's scatter moves
 constexpr int kCtrLocalC1 = 9;
 constexpr int kCtrLocalC2 = 10;
+constexpr int kCtrLocalT = 11;
+constexpr int kCtrCopyLarge = 12;   // copy entries larger than kCopySplit rows
+constexpr int kCtrCopyTile = 13;
+constexpr uint32_t kCopySplit = 4096;
 constexpr int kCtrWords = 16;
 
 struct LargeSeg {
@@ -109,8 +115,10 @@ __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32
 }
 
 struct Lists {
-    uint2 *a, *b1, *b2, *c1, *c2;
-    LargeSeg *copy;
+    uint2 *t, *a, *b1, *b2, *c1, *c2;
+    LargeSeg *copy;        // segments that only need to reach BUF0, <= kCopySplit rows (warp each)
+    LargeSeg *copy_large;  // the same, larger: copied by tiles across the grid
+    uint32_t local_max;   // segments above this size take the MSD levels (tuned, <= kCapLocal)
 };
 
 // Route a segment (child or initial) to its tier.  Segments that need no
@@ -119,16 +127,32 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
                                               uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L,
                                               uint32_t *hist_out)
 {
+    const uint32_t local_max = L.local_max;
     if (len == 0) return;
     if (len == 1 || shift == 0) {
         if (src != kSrcBuf0) {
-            uint32_t slot = atomicAdd(&ctr[kCtrCopy], 1u);
-            L.copy[slot] = LargeSeg{start, len, 0, src};
+            if (len > kCopySplit) {
+                const uint32_t slot = atomicAdd(&ctr[kCtrCopyLarge], 1u);
+                L.copy_large[slot] = LargeSeg{start, len, 0, src};
+            } else {
+                const uint32_t slot = atomicAdd(&ctr[kCtrCopy], 1u);
+                L.copy[slot] = LargeSeg{start, len, 0, src};
+            }
         }
         return;
     }
     const uint2 e = pack_local(start, len, shift, src);
-    if (len <= (uint32_t)kCapA) L.a[atomicAdd(&ctr[kCtrLocalA], 1u)] = e;
+    if (len > local_max) {
+        // a large segment: its digit histogram row starts at zero
+        const uint32_t slot = atomicAdd(&ctr[large_ctr], 1u);
+        large_out[slot] = LargeSeg{start, len, shift, src};
+        uint4 *row = reinterpret_cast<uint4 *>(hist_out + (uint64_t)slot * kRadix);
+#pragma unroll 4
+        for (int i = 0; i < kRadix / 4; ++i) row[i] = make_uint4(0, 0, 0, 0);
+        return;
+    }
+    if (len <= (uint32_t)kCapT) L.t[atomicAdd(&ctr[kCtrLocalT], 1u)] = e;
+    else if (len <= (uint32_t)kCapA) L.a[atomicAdd(&ctr[kCtrLocalA], 1u)] = e;
     else if (len <= (uint32_t)kCapB1) L.b1[atomicAdd(&ctr[kCtrLocalB1], 1u)] = e;
     else if (len <= (uint32_t)kCapB2) L.b2[atomicAdd(&ctr[kCtrLocalB2], 1u)] = e;
     else if (len <= (uint32_t)kCapC1) L.c1[atomicAdd(&ctr[kCtrLocalC1], 1u)] = e;
@@ -177,7 +201,7 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
 // count) so that no separate memsets are needed.
 __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs, const uint32_t *d_nseg,
                                                            uint32_t *tile_prefix, uint32_t *reset0,
-                                                           uint32_t *reset1, uint32_t *reset2)
+                                                           uint32_t *reset1, uint32_t *reset2, uint32_t tile_rows)
 {
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry;
@@ -191,7 +215,7 @@ __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs,
     __syncthreads();
     for (uint32_t base = 0; base < nseg; base += blockDim.x) {
         const uint32_t s = base + threadIdx.x;
-        const uint32_t c = s < nseg ? (segs[s].len + kTileM - 1) / kTileM : 0u;
+        const uint32_t c = s < nseg ? (segs[s].len + tile_rows - 1) / tile_rows : 0u;
         uint32_t incl = c;
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -231,7 +255,7 @@ __device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, ui
 
 template <typename K>
 __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
-                                                        const uint32_t *tile_prefix, uint32_t *hist)
+                                                        const uint32_t *tile_prefix, uint32_t *hist, uint32_t tile_rows)
 {
     __shared__ uint32_t sh[kRadix];
     const uint32_t nseg = *d_nseg;
@@ -245,8 +269,8 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSe
         const uint32_t lo = sg.shift - width;
         for (int d = threadIdx.x; d < kRadix; d += blockDim.x) sh[d] = 0;
         __syncthreads();
-        const uint64_t beg = (uint64_t)sg.start + (uint64_t)k * kTileM;
-        const uint64_t end = min((uint64_t)sg.start + sg.len, beg + kTileM);
+        const uint64_t beg = (uint64_t)sg.start + (uint64_t)k * tile_rows;
+        const uint64_t end = min((uint64_t)sg.start + sg.len, beg + tile_rows);
         for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
             const K key = load_k(b, sg.src, i);
             atomicAdd(&sh[digit_of(key, lo, width)], 1u);
@@ -261,7 +285,8 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSe
 // Per large segment: exclusive digit offsets, skip detection, children.
 __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const uint32_t *d_nseg,
                                                           uint32_t *hist, uint32_t *ctr, int next_large_ctr,
-                                                          LargeSeg *large_next, Lists lists, uint32_t *hist_next)
+                                                          LargeSeg *large_next, Lists lists, uint32_t *hist_next,
+                                                          bool emit_children = true)
 {
     __shared__ uint32_t cnt[kRadix];
     __shared__ uint32_t tmp[kRadix / 32 + 1];
@@ -283,7 +308,7 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const 
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
         const uint32_t child_shift = sg.shift - width;
         const uint32_t child_src = skip ? sg.src : (sg.src == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
-        if (c > 0)
+        if (emit_children && c > 0)
             route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, lists,
                           hist_next);
         if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
@@ -292,7 +317,7 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const 
     }
 }
 
-template <typename K>
+template <typename K, int IT>
 struct MsdSmem {
     uint32_t whist[kNtM / 32][kRadix];
     uint32_t total[kRadix];
@@ -300,18 +325,19 @@ struct MsdSmem {
     long long gdst[kRadix];      // global destination base per digit
     uint32_t tmp[kNtM / 32 + 1];
     uint32_t tile, seg;
-    K keys[kTileM];
-    uint32_t vals[kTileM];
+    K keys[kNtM * IT];
+    uint32_t vals[kNtM * IT];
 };
 
-template <typename K, int RANK>
-__global__ void __launch_bounds__(kNtM, 4) msd_scatter_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
+template <typename K, int RANK, int IT>
+__global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
                                                            const uint32_t *tile_prefix, const uint32_t *offs,
                                                            uint32_t *tile_counter, unsigned long long *lookback,
                                                            uint32_t epoch, int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MsdSmem<K> &sm = *reinterpret_cast<MsdSmem<K> *>(smem_raw);
+    MsdSmem<K, IT> &sm = *reinterpret_cast<MsdSmem<K, IT> *>(smem_raw);
+    constexpr uint32_t kTileM = kNtM * IT;
     const uint32_t nseg = *d_nseg;
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
@@ -337,19 +363,19 @@ __global__ void __launch_bounds__(kNtM, 4) msd_scatter_kernel(Bufs<K> b, const L
         for (int d = lane; d < kRadix; d += 32) sm.whist[warp][d] = 0;
         __syncwarp();
 
-        K key[kItM];
-        uint32_t val[kItM];
-        uint32_t rank[kItM];
-        uint32_t dig[kItM];
-        const uint32_t wbase = warp * (kItM * 32);
+        K key[IT];
+        uint32_t val[IT];
+        uint32_t rank[IT];
+        uint32_t dig[IT];
+        const uint32_t wbase = warp * (IT * 32);
 #pragma unroll
-        for (int j = 0; j < kItM; ++j) {
+        for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             if (p < cnt) load_kv(b, sg.src, tbeg + p, key[j], val[j]);
             else { key[j] = 0; val[j] = 0; }
         }
 #pragma unroll
-        for (int j = 0; j < kItM; ++j) {
+        for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             dig[j] = digit_of(key[j], lo, width);
             rank[j] = wlms_rank<RANK>(dig[j], p < cnt, sm.whist[warp], width);
@@ -391,7 +417,7 @@ __global__ void __launch_bounds__(kNtM, 4) msd_scatter_kernel(Bufs<K> b, const L
         }
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < kItM; ++j) {
+        for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             if (p < cnt) {
                 const uint32_t pos = sm.doff[dig[j]] + sm.whist[warp][dig[j]] + rank[j];
@@ -600,6 +626,60 @@ block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
     }
 }
 
+// Thread-per-segment sort of tiny segments (2..kCapT rows): the rows sit in
+// registers and an odd-even transposition network of N rounds sorts them.
+// It swaps only strictly inverted neighbours, so equal keys keep their order
+// (stable); the padding slots hold the largest key and stay behind the rows.
+template <typename K, int N>
+__device__ __forceinline__ void sort_tiny(const Bufs<K> &b, uint32_t start, uint32_t len, uint32_t src)
+{
+    K k[N];
+    uint32_t v[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        k[i] = ~K(0);
+        v[i] = 0;
+        if (i < (int)len) load_kv(b, src, (uint64_t)start + i, k[i], v[i]);
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+#pragma unroll
+        for (int i = r & 1; i + 1 < N; i += 2) {
+            if (k[i] > k[i + 1]) {
+                const K tk = k[i];
+                k[i] = k[i + 1];
+                k[i + 1] = tk;
+                const uint32_t tv = v[i];
+                v[i] = v[i + 1];
+                v[i + 1] = tv;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (i < (int)len) {
+            b.k0[(uint64_t)start + i] = k[i];
+            b.v0[(uint64_t)start + i] = v[i];
+        }
+    }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) thread_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
+{
+    const uint32_t count = *d_count;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const uint2 ent = list[e];
+        const uint32_t start = ent.x;
+        const uint32_t len = ent.y & 0xFFFFu;
+        const uint32_t src = (ent.y >> 24) & 3u;
+        if (len <= 2) sort_tiny<K, 2>(b, start, len, src);
+        else if (len <= 4) sort_tiny<K, 4>(b, start, len, src);
+        else if (len <= 8) sort_tiny<K, 8>(b, start, len, src);
+        else sort_tiny<K, 16>(b, start, len, src);
+    }
+}
+
 // Warp-per-segment LSD radix sort (len <= 32 * kItemsA), stable.
 template <typename K>
 struct WarpSmem {
@@ -718,6 +798,30 @@ __global__ void __launch_bounds__(256) copy_kernel(Bufs<K> b, const LargeSeg *li
     }
 }
 
+// Large segments that only need to reach BUF0: tiles of kCopySplit rows
+// spread over the whole grid (tile -> segment by binary search).
+template <typename K>
+__global__ void __launch_bounds__(256) copy_tiles_kernel(Bufs<K> b, const LargeSeg *list, const uint32_t *d_count,
+                                                         const uint32_t *tile_prefix)
+{
+    const uint32_t count = *d_count;
+    if (count == 0) return;
+    const uint32_t T = tile_prefix[count];
+    for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
+        const uint32_t s = find_segment(tile_prefix, count, t);
+        const LargeSeg sg = list[s];
+        const uint64_t beg = (uint64_t)sg.start + (uint64_t)(t - tile_prefix[s]) * kCopySplit;
+        const uint64_t end = min((uint64_t)sg.start + sg.len, beg + kCopySplit);
+        for (uint64_t r = beg + threadIdx.x; r < end; r += blockDim.x) {
+            K k;
+            uint32_t v;
+            load_kv(b, sg.src & 3u, r, k, v);
+            b.k0[r] = k;
+            b.v0[r] = v;
+        }
+    }
+}
+
 template <typename F>
 int set_smem(fmcs_ctx *ctx, F *f, size_t bytes)
 {
@@ -731,7 +835,7 @@ int set_smem(fmcs_ctx *ctx, F *f, size_t bytes)
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what);          \
     } while (0)
 
-template <typename K, int RANK>
+template <typename K, int RANK, int IT>
 int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
 {
     const uint64_t n = a.n;
@@ -755,8 +859,11 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     b.v1 = (uint32_t *)p;
 
     // lists (capacities are bounds on disjoint segments of each tier's minimum size)
-    const uint64_t cap_large = n / (kCapLocal + 1) + 2;
-    const uint64_t cap_a = n / 2 + 2, cap_b1 = n / (kCapA + 1) + 2, cap_b2 = n / (kCapB1 + 1) + 2;
+    const uint32_t local_max = std::max<uint32_t>(kCapA, std::min<uint32_t>(ctx->local_max, kCapLocal));
+    const uint32_t tile_rows = kNtM * IT;
+    const uint64_t cap_large = n / (local_max + 1) + 2;
+    const uint64_t cap_t = n / 2 + 2, cap_a = n / (kCapT + 1) + 2, cap_b1 = n / (kCapA + 1) + 2;
+    const uint64_t cap_b2 = n / (kCapB1 + 1) + 2;
     const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2;
     // copy entries: disjoint ranges; at most 256 children per large segment per
     // level, so bounded by both n and (levels + 1) * 256 * cap_large
@@ -769,15 +876,18 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     large[1] = (LargeSeg *)p;
     Lists lists;
     {
-        const uint64_t tot = cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2;
+        const uint64_t tot = cap_t + cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2;
         if ((rc = ws_get(ctx, kSlotLocalA, tot * sizeof(uint2), &p))) return rc;
-        lists.a = (uint2 *)p;
+        lists.t = (uint2 *)p;
+        lists.a = lists.t + cap_t;
         lists.b1 = lists.a + cap_a;
         lists.b2 = lists.b1 + cap_b1;
         lists.c1 = lists.b2 + cap_b2;
         lists.c2 = lists.c1 + cap_c1;
-        if ((rc = ws_get(ctx, kSlotLocalC, cap_copy * sizeof(LargeSeg), &p))) return rc;
+        if ((rc = ws_get(ctx, kSlotLocalC, (cap_copy + cap_large) * sizeof(LargeSeg), &p))) return rc;
         lists.copy = (LargeSeg *)p;
+        lists.copy_large = lists.copy + cap_copy;
+        lists.local_max = local_max;
     }
     uint32_t *hists[2], *tile_prefix;
     if ((rc = ws_get(ctx, kSlotSegHist, 2 * cap_large * kRadix * sizeof(uint32_t), &p))) return rc;
@@ -785,7 +895,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     hists[1] = hists[0] + cap_large * kRadix;
     if ((rc = ws_get(ctx, kSlotTilePrefix, (cap_large + 1) * sizeof(uint32_t), &p))) return rc;
     tile_prefix = (uint32_t *)p;
-    const uint64_t max_tiles = n / kTileM + cap_large + 1;
+    const uint64_t max_tiles = n / tile_rows + cap_large + 1;
     unsigned long long *lookback;
     if ((rc = ws_get(ctx, kSlotLookback, max_tiles * kRadix * sizeof(unsigned long long), &p, true))) return rc;
     lookback = (unsigned long long *)p;
@@ -810,9 +920,9 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     }
     // MSD levels
     const int levels = (int)((a.key_bits + kRadixBits - 1) / kRadixBits);
-    const size_t msd_smem = sizeof(MsdSmem<K>);
-    if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK>, msd_smem))) return rc;
-    if (n > (uint64_t)kCapLocal) {
+    const size_t msd_smem = sizeof(MsdSmem<K, IT>);
+    if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK, IT>, msd_smem))) return rc;
+    if (n > (uint64_t)local_max) {
         // Host-known count of the level's large segments (exact unless the
         // caller asked for a fixed launch sequence, e.g. for graph capture).
         uint32_t nlarge = 1;
@@ -829,11 +939,11 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             const uint32_t *d_cnt = &ctr[kCtrLarge0 + cur];
             { LaunchScope ls_(ctx, "tile_prefix");
                 tile_prefix_kernel<<<1, 1024, 0, st>>>(large[cur], d_cnt, tile_prefix, &ctr[kCtrLarge0 + nxt],
-                                                       &ctr[kCtrMsdTile], &ctr[kCtrMoved]);
+                                                       &ctr[kCtrMsdTile], &ctr[kCtrMoved], tile_rows);
             }
             uint32_t *hist = hists[cur];
             { LaunchScope ls_(ctx, "msd_hist");
-                msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, large[cur], d_cnt, tile_prefix, hist);
+                msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, large[cur], d_cnt, tile_prefix, hist, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
                 msd_plan_kernel<<<sms * 8, kRadix, 0, st>>>(large[cur], d_cnt, hist, ctr, kCtrLarge0 + nxt, large[nxt],
@@ -847,7 +957,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             }
             {
                 LaunchScope ls_(ctx, "msd_scatter");
-                msd_scatter_kernel<K, RANK><<<sms * 4, kNtM, msd_smem, st>>>(b, large[cur], d_cnt, tile_prefix, hist,
+                msd_scatter_kernel<K, RANK, IT><<<sms * (IT >= 16 ? 2 : 4), kNtM, msd_smem, st>>>(b, large[cur], d_cnt,
+                                                                         tile_prefix, hist,
                                                                          &ctr[kCtrMsdTile], lookback, ctx->epoch++,
                                                                          ctx->d_status);
                 if (!a.fixed_launches) {
@@ -869,6 +980,9 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB2, kItB2, RANK>, smem_b2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1, kItC1, RANK>, smem_c1))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
+    { LaunchScope ls_(ctx, "thread_sort");
+        thread_sort_kernel<K><<<sms * 8, 256, 0, st>>>(b, lists.t, &ctr[kCtrLocalT]);
+    }
     { LaunchScope ls_(ctx, "warp_sort");
         warp_sort_kernel<K, RANK><<<sms * 16, 256, 0, st>>>(b, lists.a, &ctr[kCtrLocalA]);
     }
@@ -887,11 +1001,141 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     { LaunchScope ls_(ctx, "copy");
         copy_kernel<K><<<sms * 4, 256, 0, st>>>(b, lists.copy, &ctr[kCtrCopy]);
     }
+    { LaunchScope ls_(ctx, "tile_prefix");
+        tile_prefix_kernel<<<1, 1024, 0, st>>>(lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix, &ctr[kCtrCopyTile],
+                                               &ctr[kCtrCopyTile], &ctr[kCtrCopyTile], kCopySplit);
+    }
+    { LaunchScope ls_(ctx, "copy_tiles");
+        copy_tiles_kernel<K><<<sms * 8, 256, 0, st>>>(b, lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix);
+    }
     FMCS_LAUNCH_CHECK("local tiers");
     return FMCS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Full-array LSD radix sort (the plain comparator path: no segments, no
+// binning).  One pass per 8 key bits, each pass the MSD level kernels applied
+// to a single segment [0, n) with the digit at bits [shift-8, shift).  Passes
+// where every row has the same digit are skipped on the device, so the buffer
+// holding the result is tracked on the device and a final copy puts it in
+// BUF0.
+// ---------------------------------------------------------------------------
+__global__ void lsd_set_pass_kernel(LargeSeg *seg, uint32_t *hist_row, uint32_t *nseg, uint32_t n, uint32_t shift,
+                                    int first)
+{
+    if (threadIdx.x == 0) {
+        uint32_t src = kSrcBuf0;
+        if (!first) {
+            const LargeSeg prev = seg[0];
+            src = (prev.src & kSkipBit) ? (prev.src & 3u) : ((prev.src & 3u) == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
+        }
+        seg[0] = LargeSeg{0, n, shift, src};
+        *nseg = 1;
+    }
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist_row[d] = 0;
+}
+
+template <typename K>
+__global__ void lsd_finalize_kernel(Bufs<K> b, const LargeSeg *seg, uint64_t n)
+{
+    const LargeSeg last = seg[0];
+    const uint32_t where = (last.src & kSkipBit) ? (last.src & 3u) : ((last.src & 3u) == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
+    if (where != kSrcBuf1) return;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        b.k0[i] = b.k1[i];
+        b.v0[i] = b.v1[i];
+    }
+}
+
+template <typename K, int RANK, int IT>
+int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint32_t bits)
+{
+    cudaStream_t st = ctx->stream;
+    int rc;
+    void *p;
+    Bufs<K> b;
+    b.k0 = (K *)keys;
+    b.v0 = vals;
+    b.ext_bank = nullptr;
+    b.ext_order = nullptr;
+    if ((rc = ws_get(ctx, kSlotKeys1, n * sizeof(K), &p))) return rc;
+    b.k1 = (K *)p;
+    if ((rc = ws_get(ctx, kSlotVals1, n * sizeof(uint32_t), &p))) return rc;
+    b.v1 = (uint32_t *)p;
+    LargeSeg *seg;
+    if ((rc = ws_get(ctx, kSlotLarge0, sizeof(LargeSeg) * 2, &p))) return rc;
+    seg = (LargeSeg *)p;
+    uint32_t *hist, *tile_prefix;
+    if ((rc = ws_get(ctx, kSlotSegHist, 2 * kRadix * sizeof(uint32_t), &p))) return rc;
+    hist = (uint32_t *)p;
+    if ((rc = ws_get(ctx, kSlotTilePrefix, 4 * sizeof(uint32_t), &p))) return rc;
+    tile_prefix = (uint32_t *)p;
+    const uint32_t tile_rows = kNtM * IT;
+    const uint64_t max_tiles = n / tile_rows + 2;
+    unsigned long long *lookback;
+    if ((rc = ws_get(ctx, kSlotLookback, max_tiles * kRadix * sizeof(unsigned long long), &p, true))) return rc;
+    lookback = (unsigned long long *)p;
+    uint32_t *ctr;
+    if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
+    ctr = (uint32_t *)p + 64;
+    const size_t msd_smem = sizeof(MsdSmem<K, IT>);
+    if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK, IT>, msd_smem))) return rc;
+    const int sms = ctx->num_sms;
+    Lists none{};
+    int pass = 0;
+    for (uint32_t lo = 0; lo < bits; lo += kRadixBits, ++pass) {
+        const uint32_t shift = std::min(bits, lo + kRadixBits);
+        { LaunchScope ls_(ctx, "lsd_set_pass");
+            lsd_set_pass_kernel<<<1, 256, 0, st>>>(seg, hist, &ctr[kCtrLarge0], (uint32_t)n, shift, pass == 0);
+        }
+        { LaunchScope ls_(ctx, "tile_prefix");
+            tile_prefix_kernel<<<1, 1024, 0, st>>>(seg, &ctr[kCtrLarge0], tile_prefix, &ctr[kCtrLarge0 + 1],
+                                                   &ctr[kCtrMsdTile], &ctr[kCtrMoved], tile_rows);
+        }
+        { LaunchScope ls_(ctx, "msd_hist");
+            msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, seg, &ctr[kCtrLarge0], tile_prefix, hist, tile_rows);
+        }
+        { LaunchScope ls_(ctx, "msd_plan");
+            msd_plan_kernel<<<1, kRadix, 0, st>>>(seg, &ctr[kCtrLarge0], hist, ctr, kCtrLarge0 + 1, seg + 1, none,
+                                                  hist + kRadix, false);
+        }
+        { LaunchScope ls_(ctx, "msd_scatter");
+            msd_scatter_kernel<K, RANK, IT><<<sms * (IT >= 16 ? 2 : 4), kNtM, msd_smem, st>>>(b, seg, &ctr[kCtrLarge0],
+                                                                                           tile_prefix, hist,
+                                                                       &ctr[kCtrMsdTile], lookback, ctx->epoch++,
+                                                                       ctx->d_status);
+        }
+        FMCS_LAUNCH_CHECK("lsd pass");
+    }
+    if (pass > 0) {
+        LaunchScope ls_(ctx, "lsd_finalize");
+        lsd_finalize_kernel<K><<<sms * 8, 256, 0, st>>>(b, seg, n);
+    }
+    FMCS_LAUNCH_CHECK("lsd finalize");
+    return FMCS_OK;
+}
+
 }  // namespace
+
+int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits)
+{
+    if (n <= 1 || bits == 0) return FMCS_OK;
+    switch (key_bytes) {
+    case 4: return lsd_sort_full_t<uint32_t, kRankMatch, 8>(ctx, keys, vals, n, bits);
+    case 8: return lsd_sort_full_t<uint64_t, kRankMatch, 8>(ctx, keys, vals, n, bits);
+    case 2: return lsd_sort_full_t<uint16_t, kRankMatch, 8>(ctx, keys, vals, n, bits);
+    default: return set_error(ctx, FMCS_E_INVAL, "lsd sort: key bytes must be 2, 4 or 8");
+    }
+}
+
+template <typename K>
+static int sort_dispatch(fmcs_ctx *ctx, const SortArgs &a)
+{
+    const bool big = ctx->msd_items >= 16;
+    if (ctx->rank_mode)
+        return big ? sort_segments_t<K, kRankBallot, 16>(ctx, a) : sort_segments_t<K, kRankBallot, 8>(ctx, a);
+    return big ? sort_segments_t<K, kRankMatch, 16>(ctx, a) : sort_segments_t<K, kRankMatch, 8>(ctx, a);
+}
 
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a)
 {
@@ -899,12 +1143,9 @@ int sort_segments(fmcs_ctx *ctx, const SortArgs &a)
     if (a.key_bits == 0 || a.key_bits > 8 * a.bank_bytes)
         return set_error(ctx, FMCS_E_INVAL, "sort: key_bits must be in 1..8*bank_bytes");
     switch (a.bank_bytes) {
-    case 2: return ctx->rank_mode ? sort_segments_t<uint16_t, kRankBallot>(ctx, a)
-                                  : sort_segments_t<uint16_t, kRankMatch>(ctx, a);
-    case 4: return ctx->rank_mode ? sort_segments_t<uint32_t, kRankBallot>(ctx, a)
-                                  : sort_segments_t<uint32_t, kRankMatch>(ctx, a);
-    case 8: return ctx->rank_mode ? sort_segments_t<uint64_t, kRankBallot>(ctx, a)
-                                  : sort_segments_t<uint64_t, kRankMatch>(ctx, a);
+    case 2: return sort_dispatch<uint16_t>(ctx, a);
+    case 4: return sort_dispatch<uint32_t>(ctx, a);
+    case 8: return sort_dispatch<uint64_t>(ctx, a);
     default: return set_error(ctx, FMCS_E_INVAL, "sort: bank_bytes must be 2, 4 or 8");
     }
 }

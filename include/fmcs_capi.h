@@ -74,6 +74,17 @@ FMCS_API int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len);
 /* Number of kernels this context has launched since it was created. */
 FMCS_API unsigned long long fmcs_launch_count(const fmcs_ctx *ctx);
 
+/* Tuned knobs of the sort engine (no reference counterpart; the reference's
+ * block sizes are compile-time constants, src/params.h:127-143).  A context
+ * starts from the autotuner's file (tuning/b200.json next to the library, or
+ * the file FMCS_TUNING names), else the built-in defaults.  Keys:
+ *   "rank_mode"  0: match.any multi-split ranking, 1: ballot multi-split;
+ *   "local_max"  128..4096: segments with more rows take the HBM radix levels;
+ *   "msd_items"  8 or 16: items per thread of an HBM radix tile.
+ * fmcs_get_tuning returns -1 for an unknown key. */
+FMCS_API int fmcs_set_tuning(fmcs_ctx *ctx, const char *key, long long value);
+FMCS_API long long fmcs_get_tuning(const fmcs_ctx *ctx, const char *key);
+
 /* One slice of a source column: bits [start, end], 1-based from the MSB of the
  * declared width src_bits (construct_entry_t, src/types.h:42-46). */
 typedef struct {
@@ -123,6 +134,17 @@ FMCS_API int fmcs_sort_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_byte
                     uint32_t *order, const uint32_t *in_group, uint32_t *out_group,
                     void *sorted_bank, uint64_t n, uint32_t *ngroups);
 
+/* The plain comparator of one sort round: same inputs, outputs and results
+ * as fmcs_sort_round, computed WITHOUT segments -- a full-array stable LSD
+ * radix sort by the key, then (later rounds) a full-array stable LSD radix
+ * sort by the previous group id.  This is the "one sort per column" GPU path
+ * that the segmented, size-binned rounds are measured against; it has no
+ * reference counterpart (the reference always sorts per group,
+ * src/composer.cpp:1280-1335). */
+FMCS_API int fmcs_sort_round_plain(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits,
+                                   uint32_t *order, const uint32_t *in_group, uint32_t *out_group,
+                                   void *sorted_bank, uint64_t n, uint32_t *ngroups);
+
 /* (e) One hash-grouping round (Composer::hashByGroup_reordered<T>,
  * src/composer.cpp:814-976; Hashing::subgroup_range, src/hashing.h:289-385;
  * Partition::histogram_based_reordering, src/partition.h:44-161).
@@ -159,6 +181,16 @@ FMCS_API int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_
                   const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
                   const uint32_t *split, uint32_t nbanks, uint64_t n, int hash,
                   uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
+
+/* The cost-model plan search alone (StitchComposer::optimizeAndRun without
+ * the run, src/stitch_composer.cpp:3839-3984): given each column's declared
+ * width, number of distinct values and storage bytes, returns the estimated
+ * cheapest split (split_out, *nbanks_out <= max_banks) and, for GROUP BY
+ * (ordered == 0, columns may be permuted), the column order.  Costs come from
+ * the GPU tables (tuning/b200.json next to the library, or FMCS_TUNING). */
+FMCS_API int fmcs_optimize_plan(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes,
+                                uint32_t ncols, uint64_t n, int ordered, uint32_t *split_out, uint32_t max_banks,
+                                uint32_t *nbanks_out, uint32_t *col_order_out, double *est_ms);
 
 /* Allocation-free group ids (no counterpart in the reference, which mallocs
  * on every call).  For callers that cannot let a library allocate device

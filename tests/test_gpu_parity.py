@@ -63,8 +63,8 @@ def _segments(rng, n, kind):
         sizes = rng.integers(1, 300, size=n)
     elif kind == "tiers":
         # straddle every tier threshold
-        base = np.array([1, 2, 31, 32, 33, 127, 128, 129, 1023, 1024, 1025, 4095, 4096, 4097,
-                         9000, 70000])
+        base = np.array([1, 2, 3, 15, 16, 17, 31, 32, 33, 127, 128, 129, 511, 512, 513, 1023, 1024, 1025,
+                         2047, 2048, 2049, 4095, 4096, 4097, 9000, 70000])
         sizes = rng.permutation(np.repeat(base, 3))
     else:  # zipf-like
         sizes = np.maximum(1, (20000 / np.arange(1, 2000)).astype(np.int64))
@@ -218,3 +218,43 @@ def C_hash_unordered(ctx, bank, in_group, out):
                                      bank.shape[0], ctypes.byref(ng))
     assert rc == 0
     return ng.value
+
+
+@pytest.mark.parametrize("segmented", [False, True])
+@pytest.mark.parametrize("dtype,bits", [(np.uint32, 24), (np.uint64, 40)])
+def test_sort_round_plain(ctx, segmented, dtype, bits):
+    rng = np.random.default_rng(bits + segmented)
+    n = 250001
+    bank = rng.integers(0, (1 << bits) - 1, size=n, dtype=np.uint64, endpoint=True).astype(dtype)
+    bank[::7] = bank[3]   # ties
+    if segmented:
+        in_group = _segments(rng, n, "zipf")
+        order_in = rng.permutation(n).astype(np.uint32)
+    else:
+        in_group, order_in = None, None
+    order = np.zeros(n, np.uint32) if order_in is None else order_in.copy()
+    group = np.zeros(n, np.uint32)
+    keys = np.zeros(n, dtype)
+    ng = ctx.sort_round_plain(bank, bits, order, in_group=in_group, out_group=group, sorted_bank=keys)
+    o_ref, g_ref, k_ref, ng_ref = O.sort_round(bank, order=order_in, in_group=in_group)
+    assert np.array_equal(order, o_ref) and np.array_equal(group, g_ref) and np.array_equal(keys, k_ref)
+    assert ng == ng_ref
+
+
+@pytest.mark.parametrize("knobs", [dict(rank_mode=1), dict(local_max=1024), dict(local_max=2048, msd_items=16),
+                                   dict(msd_items=16, rank_mode=1)])
+def test_tuning_knobs_same_results(knobs):
+    from fastmulticolsort_b200 import capi
+    cols, bw = W.cols_zipf(400000, seed_index=77)
+    with capi.Context(0) as c:
+        for k, v in knobs.items():
+            c.set_tuning(k, v)
+            assert c.get_tuning(k) == v
+        for split in ([20, 24, 40], [44, 40]):
+            order = np.zeros(400000, np.uint32)
+            group = np.zeros(400000, np.uint32)
+            ng = c.run_plan(cols, bw, split, order, group)
+            o, g, n_ref = O.run_plan_sort(cols, bw, split)
+            assert ng == n_ref and np.array_equal(order, o) and np.array_equal(group, g)
+        with pytest.raises(capi.FmcsError):
+            c.set_tuning("local_max", 5000)
