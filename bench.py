@@ -454,6 +454,20 @@ def run_fmcs(args):
     return 0
 
 
+def run_serving(args):
+    """Serving-loop workload: one JSON line of its own."""
+    from fastmulticolsort_b200 import serving
+    res = serving.benchmark(rate=args.rate, duration=args.duration)
+    line = {"metric": METRIC, "workload": "serving", "value": res["served"]["rows_per_s_M"], "unit": "M rows/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded; generated on the device)",
+            "latency_ms": {"p50": res["served"]["p50_ms"], "p99": res["served"]["p99_ms"]},
+            "config": {"workload": "Poisson 200 req/s, rows log-uniform [65536, 67108864], 2-6 columns of 1-64 "
+                                   "bits, uniform or Zipf(0.8) codes, columns resident, 150 GB admission budget"},
+            **res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,6 +478,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-zipf", action="store_true", help="skip the Zipf segmented comparison")
     ap.add_argument("--zipf-rows", type=int, default=67_108_864)
+    ap.add_argument("--workload", default="massaged", choices=["massaged", "serving"])
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--duration", type=float, default=5.0)
     ap.add_argument("--only-steps", action="store_true",
                     help="warm-up and timed steps only (no comparators, e2e or CPU baseline): "
                          "the command the ncu captures profile")
@@ -472,6 +489,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_fmcs(args)
 
 

@@ -30,7 +30,8 @@ EXPORTS = (
     "fmcs_workspace_bytes", "fmcs_stitch", "fmcs_gather", "fmcs_sort_round", "fmcs_hash_round",
     "fmcs_run_plan", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
     "fmcs_group_ids_noalloc", "fmcs_shift_left", "fmcs_assemble", "fmcs_hash_round_unordered",
-    "fmcs_sort_round_plain", "fmcs_optimize_plan", "fmcs_set_tuning", "fmcs_get_tuning",
+    "fmcs_sort_round_plain", "fmcs_optimize_plan", "fmcs_set_tuning", "fmcs_get_tuning", "fmcs_run_batch",
+    "fmcs_server_create", "fmcs_server_submit", "fmcs_server_wait", "fmcs_server_load", "fmcs_server_destroy",
 )
 
 
@@ -38,6 +39,22 @@ class FmcsError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"fmcs error {code}: {msg}")
         self.code = code
+
+
+class Instance(C.Structure):
+    _fields_ = [("row_off", C.c_uint64), ("n", C.c_uint64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("cols", C.POINTER(C.c_void_p)), ("col_bytes", C.POINTER(C.c_uint32)),
+                ("bw", C.POINTER(C.c_uint32)), ("ncols", C.c_uint32), ("split", C.POINTER(C.c_uint32)),
+                ("nbanks", C.c_uint32), ("cardinality", C.POINTER(C.c_uint64)), ("n", C.c_uint64),
+                ("hash", C.c_int), ("order_out", C.c_void_p), ("group_out", C.c_void_p)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("ngroups", C.c_uint32), ("batched_with", C.c_uint32),
+                ("queue_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double)]
 
 
 class Slice(C.Structure):
@@ -83,6 +100,14 @@ def load(path: str = LIB_PATH):
     L.fmcs_assemble.argtypes = [vp, vp, u32, u64, C.POINTER(Slice)]
     L.fmcs_hash_round_unordered.argtypes = [vp, vp, u32, vp, vp, u64, u32p]
     L.fmcs_sort_round_plain.argtypes = [vp, vp, u32, u32, vp, vp, vp, vp, u64, u32p]
+    L.fmcs_run_batch.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32, C.POINTER(Instance), u32, u64,
+                                 vp, vp, u32p]
+    L.fmcs_server_create.argtypes = [C.POINTER(vp), i32, C.c_size_t, u32, u64]
+    L.fmcs_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
+    L.fmcs_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(Result)]
+    L.fmcs_server_load.argtypes = [vp, C.POINTER(C.c_size_t), u32p, u32p]
+    L.fmcs_server_destroy.argtypes = [vp]
+    L.fmcs_server_destroy.restype = None
     L.fmcs_set_tuning.argtypes = [vp, C.c_char_p, C.c_longlong]
     L.fmcs_get_tuning.argtypes = [vp, C.c_char_p]
     L.fmcs_get_tuning.restype = C.c_longlong
@@ -273,6 +298,23 @@ class Context:
                                             1 if last_round else 0, C.byref(ng)))
         return ng.value
 
+    # -- many instances ----------------------------------------------------
+    def run_batch(self, cols, bw, split, sizes, order_out, group_out=None):
+        """sizes[k] rows per instance, concatenated in the column arrays; returns
+        the per-instance group counts."""
+        k = len(sizes)
+        inst = (Instance * k)()
+        off = 0
+        for i, s in enumerate(sizes):
+            inst[i] = Instance(off, int(s))
+            off += int(s)
+        ptrs = (C.c_void_p * len(cols))(*[_addr(c) for c in cols])
+        counts = np.zeros(k, np.uint32)
+        self._check(self._L.fmcs_run_batch(self._h, ptrs, _u32arr([_itemsize(c) for c in cols]), _u32arr(bw),
+                                           len(cols), _u32arr(split), len(split), inst, k, off, _addr(order_out),
+                                           _addr(group_out), counts.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return counts
+
     # -- whole plan ---------------------------------------------------------
     def run_plan(self, cols, bw, split, order_out, group_out=None, col_order=None,
                  hash: bool = False) -> int:
@@ -285,3 +327,66 @@ class Context:
                                           1 if hash else 0, _addr(order_out), _addr(group_out),
                                           C.byref(ng)))
         return ng.value
+
+
+class Server:
+    """fmcs_server (include/fmcs_server.h): execution slots with their own
+    streams, admission against an HBM budget, continuous batching of small
+    compatible requests."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 150 << 30, slots: int = 4,
+                 batch_rows_max: int = 1 << 20):
+        self._L = load()
+        h = C.c_void_p()
+        rc = self._L.fmcs_server_create(C.byref(h), device, hbm_budget_bytes, slots, batch_rows_max)
+        if rc != FMCS_OK:
+            raise FmcsError(rc, "fmcs_server_create failed")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, cols, bw, order_out, group_out=None, split=None, cardinality=None, hash=False) -> int:
+        n = _len(cols[0])
+        ptrs = (C.c_void_p * len(cols))(*[_addr(c) for c in cols])
+        cb = _u32arr([_itemsize(c) for c in cols])
+        bwa = _u32arr(bw)
+        spl = _u32arr(split) if split else None
+        card = (C.c_uint64 * len(cols))(*[int(x) for x in cardinality]) if cardinality else None
+        req = Request(ptrs, cb, bwa, len(cols), spl, len(split) if split else 0, card, n, 1 if hash else 0,
+                      _addr(order_out), _addr(group_out))
+        t = C.c_uint64(0)
+        rc = self._L.fmcs_server_submit(self._h, C.byref(req), C.byref(t))
+        if rc != FMCS_OK:
+            raise FmcsError(rc, "fmcs_server_submit failed")
+        self._keep[t.value] = (ptrs, cb, bwa, spl, card, cols, order_out, group_out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = -1.0) -> dict:
+        r = Result()
+        rc = self._L.fmcs_server_wait(self._h, ticket, timeout_s, C.byref(r))
+        if rc != FMCS_OK:
+            raise FmcsError(rc, "fmcs_server_wait failed")
+        self._keep.pop(ticket, None)
+        return {"status": r.status, "ngroups": r.ngroups, "batched_with": r.batched_with,
+                "queue_ms": r.queue_ms, "run_ms": r.run_ms, "total_ms": r.total_ms}
+
+    def load(self):
+        a, q, r = C.c_size_t(0), C.c_uint32(0), C.c_uint32(0)
+        self._L.fmcs_server_load(self._h, C.byref(a), C.byref(q), C.byref(r))
+        return a.value, q.value, r.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fmcs_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

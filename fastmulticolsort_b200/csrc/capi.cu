@@ -89,7 +89,7 @@ int counters(fmcs_ctx *ctx, uint32_t **w)
 int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits, uint32_t *order,
                    const uint32_t *in_group, const uint32_t *seg_start, const uint32_t *d_nseg,
                    uint32_t *out_group, void *keys_out, uint32_t *next_seg_start, uint32_t *d_next_nseg,
-                   uint64_t n, uint32_t *d_ngroups)
+                   uint64_t n, uint32_t *d_ngroups, bool identity_order = false)
 {
     int rc;
     void *p;
@@ -110,7 +110,7 @@ int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_
     a.bank = bank;
     a.bank_bytes = bank_bytes;
     a.key_bits = key_bits;
-    a.order_in = in_group ? order : nullptr;
+    a.order_in = (in_group && !identity_order) ? order : nullptr;
     a.seg_start = in_group ? seg_start : nullptr;
     a.nseg_host = 0;
     a.d_nseg = in_group ? d_nseg : nullptr;
@@ -521,4 +521,187 @@ extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint3
     if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
     if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
     return finish(ctx, "fmcs_run_plan", ngroups, d_ng);
+}
+
+// ---------------------------------------------------------------------------
+// Many independent instances in one batch
+// ---------------------------------------------------------------------------
+namespace fmcs {
+namespace {
+
+__global__ void instance_ids_kernel(const uint32_t *starts, uint32_t ninst, uint32_t *inst_id, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = ninst;   // starts[lo] <= i < starts[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (starts[mid] <= i) lo = mid; else hi = mid;
+        }
+        inst_id[i] = lo;
+    }
+}
+
+__global__ void instance_bases_kernel(const uint32_t *starts, uint32_t ninst, const uint32_t *group, uint32_t *base,
+                                      uint32_t *count)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ninst; k += gridDim.x * blockDim.x) {
+        const uint32_t s = starts[k], e = starts[k + 1];
+        base[k] = e > s ? group[s] : 0u;
+        count[k] = e > s ? group[e - 1] - group[s] + 1 : 0u;
+    }
+}
+
+__global__ void localize_kernel(const uint32_t *starts, const uint32_t *inst_id, const uint32_t *base,
+                                uint32_t *order, uint32_t *group, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = inst_id[i];
+        order[i] -= starts[k];
+        if (group) group[i] -= base[k];
+    }
+}
+
+}  // namespace
+}  // namespace fmcs
+
+extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
+                              uint32_t ncols, const uint32_t *split, uint32_t nbanks, const fmcs_instance *inst,
+                              uint32_t ninst, uint64_t total_rows, uint32_t *order_out, uint32_t *group_out,
+                              uint32_t *ngroups_out)
+{
+    if (!ctx) return FMCS_E_INVAL;
+    cudaSetDevice(ctx->device);
+    if (!cols || !col_bytes || !bw || !split || !inst || ncols == 0 || nbanks == 0 || ninst == 0 ||
+        ncols > kMaxPlanCols || nbanks > kMaxPlanBanks)
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: invalid arguments");
+    if (total_rows >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: total_rows must be < 2^32");
+    std::vector<uint32_t> starts(ninst + 1);
+    uint64_t off = 0;
+    for (uint32_t k = 0; k < ninst; ++k) {
+        if (inst[k].row_off != off)
+            return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: instances must be contiguous and in row order");
+        starts[k] = (uint32_t)off;
+        off += inst[k].n;
+    }
+    if (off != total_rows) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: instance rows do not add up");
+    starts[ninst] = (uint32_t)off;
+    for (uint32_t c = 0; c < ncols; ++c) {
+        if (!valid_bank(col_bytes[c]) || col_bytes[c] == 1 || bw[c] == 0 || bw[c] > 8 * col_bytes[c] ||
+            (total_rows && !cols[c]))
+            return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: invalid column");
+    }
+    std::vector<uint32_t> corder(ncols);
+    for (uint32_t c = 0; c < ncols; ++c) corder[c] = c;
+    Plan plan;
+    std::string perr;
+    if (!build_plan(bw, ncols, corder.data(), split, nbanks, false, plan, perr))
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: " + perr);
+    const uint64_t n = total_rows;
+    if (n == 0) {
+        if (ngroups_out)
+            for (uint32_t k = 0; k < ninst; ++k) ngroups_out[k] = 0;
+        return FMCS_OK;
+    }
+    if (!order_out) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_batch: order_out is required");
+    int rc;
+    void *p;
+    cudaStream_t st = ctx->stream;
+    // instance starts, ids per row, bases and counts
+    if ((rc = ws_get(ctx, kSlotMisc, (2 * (size_t)ninst + 2) * sizeof(uint32_t) + n * sizeof(uint32_t) + 1024, &p)))
+        return rc;
+    uint32_t *d_starts = (uint32_t *)p;
+    uint32_t *d_base = d_starts + ninst + 1;
+    uint32_t *d_count = d_base + ninst;
+    uint32_t *inst_id = d_count + ninst + 1;
+    cudaError_t e = cudaMemcpyAsync(d_starts, starts.data(), (ninst + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch upload");
+    {
+        LaunchScope ls_(ctx, "instance_ids");
+        instance_ids_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(d_starts, ninst, inst_id, n);
+    }
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    uint32_t *d_ninst = w + kCtrNgroups + 4;
+    e = cudaMemcpyAsync(d_ninst, &ninst, sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch upload");
+    // columns
+    std::vector<const void *> dcols(ncols);
+    size_t stage_bytes = 0;
+    for (uint32_t c = 0; c < ncols; ++c)
+        if (!is_device_ptr(cols[c])) stage_bytes += ((n * col_bytes[c] + 255) & ~uint64_t(255));
+    char *stage = nullptr;
+    if (stage_bytes) {
+        if ((rc = ws_get(ctx, kSlotColStage, stage_bytes, &p))) return rc;
+        stage = (char *)p;
+    }
+    for (uint32_t c = 0; c < ncols; ++c) {
+        if (is_device_ptr(cols[c])) {
+            dcols[c] = cols[c];
+        } else {
+            e = cudaMemcpyAsync(stage, cols[c], n * col_bytes[c], cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch stage");
+            dcols[c] = stage;
+            stage += ((n * col_bytes[c] + 255) & ~uint64_t(255));
+        }
+    }
+    void *dorder, *dgroup_out;
+    bool h_order, h_group;
+    if ((rc = stage_out(ctx, order_out, n * 4, kSlotStageOut0, &dorder, &h_order))) return rc;
+    if ((rc = stage_out(ctx, group_out, n * 4, kSlotStageOut1, &dgroup_out, &h_group))) return rc;
+    uint32_t *g[2];
+    if ((rc = ws_get(ctx, kSlotGroupA, n * 4, &p))) return rc;
+    g[0] = (uint32_t *)p;
+    if ((rc = ws_get(ctx, kSlotGroupB, n * 4, &p))) return rc;
+    g[1] = (uint32_t *)p;
+    uint32_t *segs[2];
+    if ((rc = ws_get(ctx, kSlotSegStart, 2 * (n + 2) * sizeof(uint32_t), &p))) return rc;
+    segs[0] = (uint32_t *)p;
+    segs[1] = segs[0] + (n + 2);
+    uint32_t *d_nseg[2] = {w + kCtrNgroups + 2, w + kCtrNgroups + 3};
+    // round 0 is segmented by instance: instance ids are the incoming groups
+    const uint32_t *in_group = inst_id;
+    const uint32_t *seg_in = d_starts;
+    const uint32_t *d_nseg_in = d_ninst;
+    for (uint32_t b = 0; b < nbanks; ++b) {
+        const BankPlan &bp = plan.banks[b];
+        const bool last = (b + 1 == nbanks);
+        ctx->prof_round = (int)b;
+        void *bank;
+        if ((rc = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, &bank))) return rc;
+        std::vector<StitchSlice> sl(bp.slices.size());
+        for (size_t k = 0; k < bp.slices.size(); ++k) {
+            const SliceRec &r = bp.slices[k];
+            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
+        }
+        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n))) return rc;
+        uint32_t *og = (last && dgroup_out) ? (uint32_t *)dgroup_out : g[b & 1];
+        uint32_t *ns = last ? nullptr : segs[b & 1];
+        if ((rc = sort_round_dev(ctx, bank, bp.bytes, bp.bits, (uint32_t *)dorder, in_group, seg_in, d_nseg_in, og,
+                                 nullptr, ns, d_nseg[b & 1], n, d_ng, b == 0)))
+            return rc;
+        seg_in = ns;
+        d_nseg_in = d_nseg[b & 1];
+        in_group = og;
+    }
+    ctx->prof_round = -1;
+    // instance-local oids and group ids
+    {
+        LaunchScope ls_(ctx, "instance_bases");
+        instance_bases_kernel<<<(ninst + 255) / 256, 256, 0, st>>>(d_starts, ninst, in_group, d_base, d_count);
+    }
+    {
+        LaunchScope ls_(ctx, "localize");
+        localize_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(d_starts, inst_id, d_base, (uint32_t *)dorder,
+                                                           (uint32_t *)in_group, n);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch localize");
+    if (ngroups_out) {
+        e = cudaMemcpyAsync(ngroups_out, d_count, ninst * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch counts");
+    }
+    if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
+    if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
+    return finish(ctx, "fmcs_run_batch", nullptr, nullptr);
 }

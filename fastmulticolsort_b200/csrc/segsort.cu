@@ -52,7 +52,6 @@ constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
 constexpr int kNtC2 = 256, kItC2 = 16, kCapC2 = kNtC2 * kItC2;  // 4096
 constexpr int kCapLocal = kCapC2;   // largest segment a local tier can take; larger: MSD levels
 constexpr int kNtM = 256;           // MSD tile: 256 threads x IT items (IT = 8 or 16, tuned)
-constexpr int kTileMin = kNtM * 8;
 
 // counters slot words
 constexpr int kCtrMsdTile = 1;

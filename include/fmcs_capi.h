@@ -182,6 +182,24 @@ FMCS_API int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_
                   const uint32_t *split, uint32_t nbanks, uint64_t n, int hash,
                   uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 
+/* Many independent sort instances in one batch (no reference counterpart: the
+ * reference sorts one relation per process).  Instance k holds rows
+ * [inst[k].row_off, inst[k].row_off + inst[k].n) of the shared column arrays;
+ * instances are contiguous and in row order and share the plan (bw, split).
+ * Every instance is one segment of the same size-binned launches.  Outputs
+ * are per-instance ranges of order_out / group_out at the same row offsets,
+ * with oids and group ids LOCAL to the instance; ngroups_out[k] (optional,
+ * host) gets instance k's group count. */
+typedef struct {
+    uint64_t row_off;
+    uint64_t n;
+} fmcs_instance;
+
+FMCS_API int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
+                            uint32_t ncols, const uint32_t *split, uint32_t nbanks, const fmcs_instance *inst,
+                            uint32_t ninst, uint64_t total_rows, uint32_t *order_out, uint32_t *group_out,
+                            uint32_t *ngroups_out);
+
 /* The cost-model plan search alone (StitchComposer::optimizeAndRun without
  * the run, src/stitch_composer.cpp:3839-3984): given each column's declared
  * width, number of distinct values and storage bytes, returns the estimated
