@@ -155,6 +155,8 @@ def visible_gpu_index(local_rank: int) -> int:
 # distributed plumbing (replicas only: no collective on the data path)
 # --------------------------------------------------------------------------
 def dist_setup(n_gpus: int):
+    """One process per GPU (torchrun env); NCCL when CUDA is present, gloo
+    otherwise (the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -163,18 +165,23 @@ def dist_setup(n_gpus: int):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
 def dist_max(x: float, world: int) -> float:
+    """Max over ranks (the slowest replica's time)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -338,35 +345,47 @@ def run_fmcs(args):
     def plain_step():
         ctx.run_plan(dcols, bw, PLAIN_SPLIT, dorder, dgroup)
 
+    graph = ctx.plan_graph(dcols, bw, SPLIT, dorder, dgroup)
+    gstream = torch.cuda.ExternalStream(graph.stream)
+
+    def graph_step():
+        graph.launch()
+
     clocks = ClockSampler(visible_gpu_index(local))
     clocks.start()
     t_load = time.perf_counter()
     for _ in range(args.warmup):
+        graph_step()
         step()
     # keep the GPU busy for at least ~1 s before the timed region so that the
     # clock samples describe the loaded state
     while not args.only_steps and time.perf_counter() - t_load < 1.0:
-        step()
+        graph_step()
     dist_barrier(world)
     torch.cuda.synchronize()
-    ctx.profile(True)
-    launches0 = ctx.launch_count()
-    total_ms, per_ms = time_steps(ctx, stream, step, args.steps)
-    launches = ctx.launch_count() - launches0
-    prof = {k: v for k, v in ctx.profile_report().items() if not k.startswith("_")}
-    ctx.profile(False)
+    # timed region: K replays of the captured plan (device-resident columns)
+    total_ms, per_ms = time_steps(ctx, gstream, graph_step, args.steps)
     torch.cuda.synchronize()
     dist_barrier(world)
     clk = clocks.stop()
     total_ms = dist_max(total_ms, world)
     ms_per_step = total_ms / args.steps
     value = world * n / (ms_per_step / 1e3) / 1e6
+    launches = graph.kernels() * args.steps
+    # the same K steps as eager C-ABI calls, with the library's CUDA events
+    # around every kernel: the per-kernel split and the roofline
+    ctx.profile(True)
+    eager_total, _ = time_steps(ctx, stream, step, args.steps)
+    prof = {k: v for k, v in ctx.profile_report().items() if not k.startswith("_")}
+    ctx.profile(False)
+    eager_ms = dist_max(eager_total / args.steps, world)
     if args.only_steps:
+        graph.close()
         ctx.close()
         dist_done(world)
         if rank == 0:
             print(json.dumps({"only_steps": True, "value": value, "ms_per_step": ms_per_step,
-                              "kernels": prof}), flush=True)
+                              "eager_ms_per_step": eager_ms, "kernels": prof}), flush=True)
         return 0
 
     # plain one-sort-per-column comparator on the same data
@@ -425,7 +444,9 @@ def run_fmcs(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded PRNG; 17-bit codes from 8,192 distinct values + uniform 33-bit codes)",
         "config": {"workload": WORKLOAD, "rows": n, "plan": SPLIT, "columns": "u32 (17 bits) + u64 (33 bits)",
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (192 MB of columns)"},
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (192 MB of columns)",
+                   "launch": "CUDA-graph replay of the plan (fmcs_graph_launch); eager C-ABI calls in eager_ms"},
+        "eager_ms_per_step": round(eager_ms, 4),
         "latency_ms": {"p50": round(float(np.percentile(per_ms, 50)), 4),
                        "p99": round(float(np.percentile(per_ms, 99)), 4)},
         "plan_hbm": {"model_bytes_per_row": model_bpr, "achieved_gbs": round(plan_gbs, 1),
@@ -447,6 +468,7 @@ def run_fmcs(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cols, bw, SPLIT, args.cpu_runs)
         line["cpu_baseline"].pop("seconds", None)
+    graph.close()
     ctx.close()
     dist_done(world)
     if rank == 0:

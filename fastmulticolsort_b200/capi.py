@@ -32,6 +32,7 @@ EXPORTS = (
     "fmcs_group_ids_noalloc", "fmcs_shift_left", "fmcs_assemble", "fmcs_hash_round_unordered",
     "fmcs_sort_round_plain", "fmcs_optimize_plan", "fmcs_set_tuning", "fmcs_get_tuning", "fmcs_run_batch",
     "fmcs_server_create", "fmcs_server_submit", "fmcs_server_wait", "fmcs_server_load", "fmcs_server_destroy",
+    "fmcs_graph_create", "fmcs_graph_launch", "fmcs_graph_stream", "fmcs_graph_destroy", "fmcs_graph_kernels",
 )
 
 
@@ -102,6 +103,13 @@ def load(path: str = LIB_PATH):
     L.fmcs_sort_round_plain.argtypes = [vp, vp, u32, u32, vp, vp, vp, vp, u64, u32p]
     L.fmcs_run_batch.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32, C.POINTER(Instance), u32, u64,
                                  vp, vp, u32p]
+    L.fmcs_graph_create.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32p, u32, u64, vp, vp, C.POINTER(vp)]
+    L.fmcs_graph_launch.argtypes = [vp, u32p]
+    L.fmcs_graph_stream.argtypes = [vp]
+    L.fmcs_graph_stream.restype = vp
+    L.fmcs_graph_kernels.argtypes = [vp]
+    L.fmcs_graph_destroy.argtypes = [vp]
+    L.fmcs_graph_destroy.restype = None
     L.fmcs_server_create.argtypes = [C.POINTER(vp), i32, C.c_size_t, u32, u64]
     L.fmcs_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
     L.fmcs_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(Result)]
@@ -298,6 +306,10 @@ class Context:
                                             1 if last_round else 0, C.byref(ng)))
         return ng.value
 
+    # -- CUDA graph of a whole plan -----------------------------------------
+    def plan_graph(self, cols, bw, split, order_out, group_out=None, col_order=None) -> "PlanGraph":
+        return PlanGraph(self, cols, bw, split, order_out, group_out, col_order)
+
     # -- many instances ----------------------------------------------------
     def run_batch(self, cols, bw, split, sizes, order_out, group_out=None):
         """sizes[k] rows per instance, concatenated in the column arrays; returns
@@ -327,6 +339,50 @@ class Context:
                                           1 if hash else 0, _addr(order_out), _addr(group_out),
                                           C.byref(ng)))
         return ng.value
+
+
+class PlanGraph:
+    """fmcs_graph: a sort plan captured once, replayed with launch()."""
+
+    def __init__(self, ctx: "Context", cols, bw, split, order_out, group_out=None, col_order=None):
+        self._L = load()
+        self._ctx = ctx
+        n = _len(cols[0])
+        self._keep = (cols, order_out, group_out)
+        ptrs = (C.c_void_p * len(cols))(*[_addr(c) for c in cols])
+        co = None if col_order is None else _u32arr(col_order)
+        h = C.c_void_p()
+        rc = self._L.fmcs_graph_create(ctx.handle, ptrs, _u32arr([_itemsize(c) for c in cols]), _u32arr(bw),
+                                       len(cols), co, _u32arr(split), len(split), n, _addr(order_out),
+                                       _addr(group_out), C.byref(h))
+        ctx._check(rc)
+        self._h = h
+
+    def launch(self) -> int:
+        ng = C.c_uint32(0)
+        rc = self._L.fmcs_graph_launch(self._h, C.byref(ng))
+        if rc != FMCS_OK:
+            raise FmcsError(rc, "fmcs_graph_launch failed")
+        return ng.value
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.fmcs_graph_stream(self._h) or 0)
+
+    def kernels(self) -> int:
+        """Kernel launches one replay performs."""
+        return int(self._L.fmcs_graph_kernels(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fmcs_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

@@ -89,7 +89,7 @@ int counters(fmcs_ctx *ctx, uint32_t **w)
 int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits, uint32_t *order,
                    const uint32_t *in_group, const uint32_t *seg_start, const uint32_t *d_nseg,
                    uint32_t *out_group, void *keys_out, uint32_t *next_seg_start, uint32_t *d_next_nseg,
-                   uint64_t n, uint32_t *d_ngroups, bool identity_order = false)
+                   uint64_t n, uint32_t *d_ngroups, bool identity_order = false, bool fixed_launches = false)
 {
     int rc;
     void *p;
@@ -117,10 +117,78 @@ int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_
     a.order_out = order;
     a.keys_out = keys_out;
     a.n = n;
+    a.fixed_launches = fixed_launches;
     if ((rc = sort_segments(ctx, a))) return rc;
     if (out_group || next_seg_start)
         return launch_group_ids_segments(ctx, keys_out, bank_bytes, in_group, out_group, next_seg_start, n,
                                          next_seg_start ? d_next_nseg : d_ngroups);
+    return FMCS_OK;
+}
+
+// The device work of one plan (stitch + rounds), enqueued on the context's
+// stream with no host synchronization when `fixed` (every radix level is
+// launched and exits on the device when it has nothing to do): the form a
+// CUDA graph captures.  *d_ng_out receives the device word of the group count.
+int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, const uint32_t *col_bytes,
+                  const uint32_t *bw, uint64_t n, bool hash, uint32_t *dorder, uint32_t *dgroup_out, bool fixed,
+                  uint32_t **d_ng_out)
+{
+    int rc;
+    void *p;
+    const uint32_t nbanks = (uint32_t)plan.banks.size();
+    uint32_t *w;
+    if ((rc = counters(ctx, &w))) return rc;
+    uint32_t *d_ng = w + kCtrNgroups;
+    // group ping-pong and segment starts
+    uint32_t *g[2];
+    if ((rc = ws_get(ctx, kSlotGroupA, n * 4, &p))) return rc;
+    g[0] = (uint32_t *)p;
+    if ((rc = ws_get(ctx, kSlotGroupB, n * 4, &p))) return rc;
+    g[1] = (uint32_t *)p;
+    uint32_t *segs[2];
+    if ((rc = ws_get(ctx, kSlotSegStart, 2 * (n + 2) * sizeof(uint32_t), &p))) return rc;
+    segs[0] = (uint32_t *)p;
+    segs[1] = segs[0] + (n + 2);
+    uint32_t *d_nseg[2] = {w + kCtrNgroups + 2, w + kCtrNgroups + 3};
+    const uint32_t *in_group = nullptr;
+    const uint32_t *seg_in = nullptr;
+    const uint32_t *d_nseg_in = nullptr;
+    for (uint32_t b = 0; b < nbanks; ++b) {
+        const BankPlan &bp = plan.banks[b];
+        const bool last = (b + 1 == nbanks);
+        ctx->prof_round = (int)b;
+        // (a) stitch the bank
+        void *bank;
+        if ((rc = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, &bank))) return rc;
+        std::vector<StitchSlice> sl(bp.slices.size());
+        for (size_t k = 0; k < bp.slices.size(); ++k) {
+            const SliceRec &r = bp.slices[k];
+            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
+        }
+        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n))) return rc;
+        uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
+        if (!hash) {
+            // (b)+(d): sort, then group ids (+ the next round's segments)
+            uint32_t *ns = last ? nullptr : segs[b & 1];
+            if ((rc = sort_round_dev(ctx, bank, bp.bytes, bp.bits, dorder, in_group, seg_in, d_nseg_in, og, nullptr,
+                                     ns, d_nseg[b & 1], n, d_ng, false, fixed)))
+                return rc;
+            seg_in = ns;
+            d_nseg_in = d_nseg[b & 1];
+        } else {
+            // (e): hash grouping rounds; the last round leaves the order alone
+            uint32_t *oin = in_group ? dorder : nullptr;
+            if (!in_group && last) {
+                if ((rc = launch_iota(ctx, dorder, n))) return rc;
+                oin = dorder;
+            }
+            if ((rc = hash_round(ctx, bank, bp.bytes, oin, dorder, in_group, og, n, last, d_ng)))
+                return rc;
+        }
+        in_group = og;
+    }
+    ctx->prof_round = -1;
+    *d_ng_out = d_ng;
     return FMCS_OK;
 }
 
@@ -466,57 +534,10 @@ extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint3
     bool h_order, h_group;
     if ((rc = stage_out(ctx, order_out, n * 4, kSlotStageOut0, &dorder, &h_order))) return rc;
     if ((rc = stage_out(ctx, group_out, n * 4, kSlotStageOut1, &dgroup_out, &h_group))) return rc;
-    uint32_t *w;
-    if ((rc = counters(ctx, &w))) return rc;
-    uint32_t *d_ng = w + kCtrNgroups;
-    // group ping-pong and segment starts
-    uint32_t *g[2];
-    if ((rc = ws_get(ctx, kSlotGroupA, n * 4, &p))) return rc;
-    g[0] = (uint32_t *)p;
-    if ((rc = ws_get(ctx, kSlotGroupB, n * 4, &p))) return rc;
-    g[1] = (uint32_t *)p;
-    uint32_t *segs[2];
-    if ((rc = ws_get(ctx, kSlotSegStart, 2 * (n + 2) * sizeof(uint32_t), &p))) return rc;
-    segs[0] = (uint32_t *)p;
-    segs[1] = segs[0] + (n + 2);
-    uint32_t *d_nseg[2] = {w + kCtrNgroups + 2, w + kCtrNgroups + 3};
-    const uint32_t *in_group = nullptr;
-    const uint32_t *seg_in = nullptr;
-    const uint32_t *d_nseg_in = nullptr;
-    for (uint32_t b = 0; b < nbanks; ++b) {
-        const BankPlan &bp = plan.banks[b];
-        const bool last = (b + 1 == nbanks);
-        ctx->prof_round = (int)b;
-        // (a) stitch the bank
-        void *bank;
-        if ((rc = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, &bank))) return rc;
-        std::vector<StitchSlice> sl(bp.slices.size());
-        for (size_t k = 0; k < bp.slices.size(); ++k) {
-            const SliceRec &r = bp.slices[k];
-            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
-        }
-        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n))) return rc;
-        uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
-        if (!hash) {
-            // (b)+(d): sort, then group ids (+ the next round's segments)
-            uint32_t *ns = last ? nullptr : segs[b & 1];
-            if ((rc = sort_round_dev(ctx, bank, bp.bytes, bp.bits, (uint32_t *)dorder, in_group, seg_in, d_nseg_in,
-                                     og, nullptr, ns, d_nseg[b & 1], n, d_ng)))
-                return rc;
-            seg_in = ns;
-            d_nseg_in = d_nseg[b & 1];
-        } else {
-            // (e): hash grouping rounds; the last round leaves the order alone
-            uint32_t *oin = in_group ? (uint32_t *)dorder : nullptr;
-            if (!in_group && last) {
-                if ((rc = launch_iota(ctx, (uint32_t *)dorder, n))) return rc;
-                oin = (uint32_t *)dorder;
-            }
-            if ((rc = hash_round(ctx, bank, bp.bytes, oin, (uint32_t *)dorder, in_group, og, n, last, d_ng)))
-                return rc;
-        }
-        in_group = og;
-    }
+    uint32_t *d_ng = nullptr;
+    if ((rc = plan_pipeline(ctx, plan, dcols.data(), col_bytes, bw, n, hash != 0, (uint32_t *)dorder,
+                            (uint32_t *)dgroup_out, false, &d_ng)))
+        return rc;
     ctx->prof_round = -1;
     if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
     if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
@@ -704,4 +725,111 @@ extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint
     if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
     if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
     return finish(ctx, "fmcs_run_batch", nullptr, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// A whole sort plan captured once as a CUDA graph and replayed
+// ---------------------------------------------------------------------------
+struct fmcs_graph {
+    fmcs_ctx *ctx = nullptr;   // private context: its workspace stays as captured
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t *d_ng = nullptr;
+};
+
+extern "C" void fmcs_graph_destroy(fmcs_graph *g)
+{
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->ctx) fmcs_destroy(g->ctx);
+    delete g;
+}
+
+extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, const uint32_t *col_bytes,
+                                 const uint32_t *bw, uint32_t ncols, const uint32_t *col_order, const uint32_t *split,
+                                 uint32_t nbanks, uint64_t n, uint32_t *order_out, uint32_t *group_out,
+                                 fmcs_graph **out)
+{
+    if (!parent || !out) return FMCS_E_INVAL;
+    *out = nullptr;
+    cudaSetDevice(parent->device);
+    if (!cols || !col_bytes || !bw || !split || ncols == 0 || nbanks == 0 || ncols > kMaxPlanCols ||
+        nbanks > kMaxPlanBanks || n == 0 || n >= (1ull << 32) || !order_out)
+        return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: invalid arguments");
+    for (uint32_t c = 0; c < ncols; ++c) {
+        if (!(col_bytes[c] == 2 || col_bytes[c] == 4 || col_bytes[c] == 8) || bw[c] == 0 || bw[c] > 8 * col_bytes[c])
+            return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: invalid column");
+        if (!is_device_ptr(cols[c]))
+            return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: columns must be device memory");
+    }
+    if (!is_device_ptr(order_out) || (group_out && !is_device_ptr(group_out)))
+        return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: outputs must be device memory");
+    std::vector<uint32_t> corder(ncols);
+    for (uint32_t c = 0; c < ncols; ++c) corder[c] = col_order ? col_order[c] : c;
+    Plan plan;
+    std::string perr;
+    if (!build_plan(bw, ncols, corder.data(), split, nbanks, false, plan, perr))
+        return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: " + perr);
+    fmcs_graph *g = new fmcs_graph();
+    int rc = fmcs_create(&g->ctx, parent->device, 0);
+    if (rc) {
+        delete g;
+        return set_error(parent, rc, "fmcs_graph_create: context");
+    }
+    fmcs_ctx *ctx = g->ctx;
+    ctx->rank_mode = parent->rank_mode;
+    ctx->local_max = parent->local_max;
+    ctx->msd_items = parent->msd_items;
+    // 1) one eager run of the fixed launch sequence sizes every workspace slot
+    rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, false, order_out, group_out, true, &g->d_ng);
+    if (!rc) rc = check_status(ctx, "fmcs_graph_create warm-up");
+    // 2) capture: reset the look-back words (their epochs repeat on every
+    //    replay), then the same launches
+    if (!rc) {
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (int slot : {kSlotLookback, kSlotScanTiles})
+                if (ctx->ws.ptr[slot]) cudaMemsetAsync(ctx->ws.ptr[slot], 0, ctx->ws.cap[slot], ctx->stream);
+            rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, false, order_out, group_out, true, &g->d_ng);
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamEndCapture(ctx->stream, &graph);
+            g->graph = graph;
+            if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, graph, 0);
+        }
+        if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "fmcs_graph_create capture");
+    }
+    if (rc) {
+        set_error(parent, rc, std::string("fmcs_graph_create: ") + ctx->err);
+        fmcs_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return FMCS_OK;
+}
+
+extern "C" int fmcs_graph_launch(fmcs_graph *g, uint32_t *ngroups)
+{
+    if (!g || !g->exec) return FMCS_E_INVAL;
+    cudaSetDevice(g->ctx->device);
+    cudaError_t e = cudaGraphLaunch(g->exec, g->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(g->ctx, e, "fmcs_graph_launch");
+    return finish(g->ctx, "fmcs_graph_launch", ngroups, g->d_ng);
+}
+
+extern "C" void *fmcs_graph_stream(fmcs_graph *g) { return g && g->ctx ? (void *)g->ctx->stream : nullptr; }
+
+extern "C" int fmcs_graph_kernels(fmcs_graph *g)
+{
+    if (!g || !g->graph) return -1;
+    size_t count = 0;
+    if (cudaGraphGetNodes(g->graph, nullptr, &count) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(count);
+    if (count && cudaGraphGetNodes(g->graph, nodes.data(), &count) != cudaSuccess) return -1;
+    int kernels = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kernels++;
+    }
+    return kernels;
 }

@@ -44,6 +44,7 @@ constexpr uint32_t kSkipBit = 0x100;
 // Local tiers: a segment goes to the smallest tier whose capacity holds it, so
 // that each kernel's unrolled item steps match the segment (few idle steps).
 constexpr int kCapT = 16;    // thread per segment: registers, odd-even transposition network
+constexpr int kCapT32 = 32;  // the same up to 32 rows, for 2- and 4-byte keys (own kernel: more registers)
 constexpr int kCapA = 128;   // warp per segment: 32 lanes x 4 items
 constexpr int kItemsA = 4;
 constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
@@ -64,6 +65,7 @@ constexpr int kCtrMoved = 8;    // rows the current level's scatter moves
 constexpr int kCtrLocalC1 = 9;
 constexpr int kCtrLocalC2 = 10;
 constexpr int kCtrLocalT = 11;
+constexpr int kCtrLocalT32 = 14;
 constexpr int kCtrCopyLarge = 12;   // copy entries larger than kCopySplit rows
 constexpr int kCtrCopyTile = 13;
 constexpr uint32_t kCopySplit = 4096;
@@ -114,7 +116,8 @@ __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32
 }
 
 struct Lists {
-    uint2 *t, *a, *b1, *b2, *c1, *c2;
+    uint2 *t, *t32, *a, *b1, *b2, *c1, *c2;
+    uint32_t cap_t32;      // kCapT32 for keys of <= 4 bytes, else 0 (17..32 rows go to the warp tier)
     LargeSeg *copy;        // segments that only need to reach BUF0, <= kCopySplit rows (warp each)
     LargeSeg *copy_large;  // the same, larger: copied by tiles across the grid
     uint32_t local_max;   // segments above this size take the MSD levels (tuned, <= kCapLocal)
@@ -151,6 +154,7 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
         return;
     }
     if (len <= (uint32_t)kCapT) L.t[atomicAdd(&ctr[kCtrLocalT], 1u)] = e;
+    else if (len <= L.cap_t32) L.t32[atomicAdd(&ctr[kCtrLocalT32], 1u)] = e;
     else if (len <= (uint32_t)kCapA) L.a[atomicAdd(&ctr[kCtrLocalA], 1u)] = e;
     else if (len <= (uint32_t)kCapB1) L.b1[atomicAdd(&ctr[kCtrLocalB1], 1u)] = e;
     else if (len <= (uint32_t)kCapB2) L.b2[atomicAdd(&ctr[kCtrLocalB2], 1u)] = e;
@@ -252,31 +256,49 @@ __device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, ui
     return lo;
 }
 
+// Top-digit histogram of every large segment.  A block takes one tile at a
+// time; each thread issues all of its tile's loads before counting (up to 16
+// in flight), and each warp counts into its own shared sub-histogram so that
+// skewed digits do not serialize the whole block on one counter.
 template <typename K>
 __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
                                                         const uint32_t *tile_prefix, uint32_t *hist, uint32_t tile_rows)
 {
-    __shared__ uint32_t sh[kRadix];
+    constexpr int NW = kNtM / 32;
+    constexpr int MAXJ = 16;   // tile_rows <= 16 * kNtM
+    __shared__ uint32_t sh[NW][kRadix];
     const uint32_t nseg = *d_nseg;
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
+    const int warp = threadIdx.x >> 5;
     for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
         const uint32_t s = find_segment(tile_prefix, nseg, t);
         const LargeSeg sg = segs[s];
         const uint32_t k = t - tile_prefix[s];
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
         const uint32_t lo = sg.shift - width;
-        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) sh[d] = 0;
+        for (int d = threadIdx.x; d < NW * kRadix; d += blockDim.x) (&sh[0][0])[d] = 0;
         __syncthreads();
         const uint64_t beg = (uint64_t)sg.start + (uint64_t)k * tile_rows;
         const uint64_t end = min((uint64_t)sg.start + sg.len, beg + tile_rows);
-        for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-            const K key = load_k(b, sg.src, i);
-            atomicAdd(&sh[digit_of(key, lo, width)], 1u);
+        K key[MAXJ];
+#pragma unroll
+        for (int j = 0; j < MAXJ; ++j) {
+            const uint64_t i = beg + threadIdx.x + (uint64_t)j * kNtM;
+            if (i < end) key[j] = load_k(b, sg.src, i);
+        }
+#pragma unroll
+        for (int j = 0; j < MAXJ; ++j) {
+            const uint64_t i = beg + threadIdx.x + (uint64_t)j * kNtM;
+            if (i < end) atomicAdd(&sh[warp][digit_of(key[j], lo, width)], 1u);
         }
         __syncthreads();
-        for (int d = threadIdx.x; d < kRadix; d += blockDim.x)
-            if (sh[d]) atomicAdd(&hist[(uint64_t)s * kRadix + d], sh[d]);
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+            uint32_t c = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) c += sh[w][d];
+            if (c) atomicAdd(&hist[(uint64_t)s * kRadix + d], c);
+        }
         __syncthreads();
     }
 }
@@ -663,7 +685,7 @@ __device__ __forceinline__ void sort_tiny(const Bufs<K> &b, uint32_t start, uint
     }
 }
 
-template <typename K>
+template <typename K, int NMAX>
 __global__ void __launch_bounds__(256) thread_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
     const uint32_t count = *d_count;
@@ -672,10 +694,14 @@ __global__ void __launch_bounds__(256) thread_sort_kernel(Bufs<K> b, const uint2
         const uint32_t start = ent.x;
         const uint32_t len = ent.y & 0xFFFFu;
         const uint32_t src = (ent.y >> 24) & 3u;
-        if (len <= 2) sort_tiny<K, 2>(b, start, len, src);
-        else if (len <= 4) sort_tiny<K, 4>(b, start, len, src);
-        else if (len <= 8) sort_tiny<K, 8>(b, start, len, src);
-        else sort_tiny<K, 16>(b, start, len, src);
+        if constexpr (NMAX > 16) {
+            sort_tiny<K, NMAX>(b, start, len, src);
+        } else {
+            if (len <= 2) sort_tiny<K, 2>(b, start, len, src);
+            else if (len <= 4) sort_tiny<K, 4>(b, start, len, src);
+            else if (len <= 8) sort_tiny<K, 8>(b, start, len, src);
+            else sort_tiny<K, 16>(b, start, len, src);
+        }
     }
 }
 
@@ -861,7 +887,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const uint32_t local_max = std::max<uint32_t>(kCapA, std::min<uint32_t>(ctx->local_max, kCapLocal));
     const uint32_t tile_rows = kNtM * IT;
     const uint64_t cap_large = n / (local_max + 1) + 2;
-    const uint64_t cap_t = n / 2 + 2, cap_a = n / (kCapT + 1) + 2, cap_b1 = n / (kCapA + 1) + 2;
+    const uint64_t cap_t = n / 2 + 2, cap_t32 = n / (kCapT + 1) + 2, cap_a = n / (kCapT + 1) + 2;
+    const uint64_t cap_b1 = n / (kCapA + 1) + 2;
     const uint64_t cap_b2 = n / (kCapB1 + 1) + 2;
     const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2;
     // copy entries: disjoint ranges; at most 256 children per large segment per
@@ -875,10 +902,12 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     large[1] = (LargeSeg *)p;
     Lists lists;
     {
-        const uint64_t tot = cap_t + cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2;
+        const uint64_t tot = cap_t + cap_t32 + cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2;
         if ((rc = ws_get(ctx, kSlotLocalA, tot * sizeof(uint2), &p))) return rc;
         lists.t = (uint2 *)p;
-        lists.a = lists.t + cap_t;
+        lists.t32 = lists.t + cap_t;
+        lists.a = lists.t32 + cap_t32;
+        lists.cap_t32 = sizeof(K) <= 4 ? kCapT32 : 0;
         lists.b1 = lists.a + cap_a;
         lists.b2 = lists.b1 + cap_b1;
         lists.c1 = lists.b2 + cap_b2;
@@ -980,7 +1009,11 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1, kItC1, RANK>, smem_c1))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
     { LaunchScope ls_(ctx, "thread_sort");
-        thread_sort_kernel<K><<<sms * 8, 256, 0, st>>>(b, lists.t, &ctr[kCtrLocalT]);
+        thread_sort_kernel<K, 16><<<sms * 8, 256, 0, st>>>(b, lists.t, &ctr[kCtrLocalT]);
+    }
+    if constexpr (sizeof(K) <= 4) {
+        LaunchScope ls_(ctx, "thread_sort_32");
+        thread_sort_kernel<K, 32><<<sms * 8, 256, 0, st>>>(b, lists.t32, &ctr[kCtrLocalT32]);
     }
     { LaunchScope ls_(ctx, "warp_sort");
         warp_sort_kernel<K, RANK><<<sms * 16, 256, 0, st>>>(b, lists.a, &ctr[kCtrLocalA]);

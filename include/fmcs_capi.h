@@ -182,6 +182,26 @@ FMCS_API int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_
                   const uint32_t *split, uint32_t nbanks, uint64_t n, int hash,
                   uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 
+/* A whole sort plan captured once as a CUDA graph and replayed (no reference
+ * counterpart).  The graph is bound to the DEVICE buffers given here (columns,
+ * order_out, group_out): refill the columns between launches and replay.
+ * It runs in a private context (own stream and workspace, sized by one eager
+ * run at creation); every radix level is part of the graph and exits on the
+ * device when it has no work, so a replay needs no host round trip until its
+ * final status check.  Sort plans only (hash rounds read a count back).
+ * fmcs_graph_launch returns when the results are complete; fmcs_graph_stream
+ * is the graph's stream. */
+typedef struct fmcs_graph fmcs_graph;
+FMCS_API int fmcs_graph_create(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes,
+                               const uint32_t *bw, uint32_t ncols, const uint32_t *col_order, const uint32_t *split,
+                               uint32_t nbanks, uint64_t n, uint32_t *order_out, uint32_t *group_out,
+                               fmcs_graph **graph);
+FMCS_API int fmcs_graph_launch(fmcs_graph *graph, uint32_t *ngroups);
+FMCS_API void *fmcs_graph_stream(fmcs_graph *graph);
+/* Kernel launches one replay performs (kernel nodes of the graph). */
+FMCS_API int fmcs_graph_kernels(fmcs_graph *graph);
+FMCS_API void fmcs_graph_destroy(fmcs_graph *graph);
+
 /* Many independent sort instances in one batch (no reference counterpart: the
  * reference sorts one relation per process).  Instance k holds rows
  * [inst[k].row_off, inst[k].row_off + inst[k].n) of the shared column arrays;
