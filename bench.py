@@ -371,11 +371,15 @@ def run_fmcs(args):
     total_ms = dist_max(total_ms, world)
     ms_per_step = total_ms / args.steps
     value = world * n / (ms_per_step / 1e3) / 1e6
-    launches = graph.kernels() * args.steps
     # the same K steps as eager C-ABI calls, with the library's CUDA events
-    # around every kernel: the per-kernel split and the roofline
+    # around every kernel: the per-kernel split and the roofline.  An eager
+    # step launches the same kernels as a replay (the replay's level loop runs
+    # as many levels as the eager host loop), so its launch count per step is
+    # the replay's.
     ctx.profile(True)
+    lc0 = ctx.launch_count()
     eager_total, _ = time_steps(ctx, stream, step, args.steps)
+    launches = (ctx.launch_count() - lc0) // max(1, args.steps) * args.steps
     prof = {k: v for k, v in ctx.profile_report().items() if not k.startswith("_")}
     ctx.profile(False)
     eager_ms = dist_max(eager_total / args.steps, world)

@@ -370,7 +370,7 @@ class PlanGraph:
         return int(self._L.fmcs_graph_stream(self._h) or 0)
 
     def kernels(self) -> int:
-        """Kernel launches one replay performs."""
+        """Kernel nodes of the graph (each loop body counted once)."""
         return int(self._L.fmcs_graph_kernels(self._h))
 
     def close(self):

@@ -735,6 +735,7 @@ struct fmcs_graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t *d_ng = nullptr;
+    unsigned long long kernels = 0;   // kernel nodes captured (a loop body once)
 };
 
 extern "C" void fmcs_graph_destroy(fmcs_graph *g)
@@ -791,7 +792,9 @@ extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, cons
         if (e == cudaSuccess) {
             for (int slot : {kSlotLookback, kSlotScanTiles})
                 if (ctx->ws.ptr[slot]) cudaMemsetAsync(ctx->ws.ptr[slot], 0, ctx->ws.cap[slot], ctx->stream);
+            const unsigned long long l0 = ctx->launches;   // every launch site counts itself
             rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, false, order_out, group_out, true, &g->d_ng);
+            g->kernels = ctx->launches - l0;
             cudaGraph_t graph = nullptr;
             e = cudaStreamEndCapture(ctx->stream, &graph);
             g->graph = graph;
@@ -822,14 +825,5 @@ extern "C" void *fmcs_graph_stream(fmcs_graph *g) { return g && g->ctx ? (void *
 extern "C" int fmcs_graph_kernels(fmcs_graph *g)
 {
     if (!g || !g->graph) return -1;
-    size_t count = 0;
-    if (cudaGraphGetNodes(g->graph, nullptr, &count) != cudaSuccess) return -1;
-    std::vector<cudaGraphNode_t> nodes(count);
-    if (count && cudaGraphGetNodes(g->graph, nodes.data(), &count) != cudaSuccess) return -1;
-    int kernels = 0;
-    for (auto nd : nodes) {
-        cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kernels++;
-    }
-    return kernels;
+    return (int)g->kernels;
 }

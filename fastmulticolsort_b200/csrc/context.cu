@@ -76,6 +76,47 @@ int ws_get(fmcs_ctx *ctx, int slot, size_t bytes, void **out, bool zero_new)
     return FMCS_OK;
 }
 
+int capture_while(fmcs_ctx *ctx, cudaStream_t st,
+                  const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: capture info");
+    if (cs != cudaStreamCaptureStatusActive) return set_error(ctx, FMCS_E_INVAL, "capture_while: stream not capturing");
+    if (!ctx->side) {
+        e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: stream");
+    }
+    cudaGraphConditionalHandle h;
+    e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: handle");
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, deps, ndeps, &np);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: node");
+    cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: dependencies");
+    e = cudaStreamBeginCaptureToGraph(ctx->side, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: body capture");
+    cudaStream_t saved = ctx->stream;
+    ctx->stream = ctx->side;
+    int rc = body(ctx->side, h);
+    ctx->stream = saved;
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(ctx->side, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_while: body end");
+    return FMCS_OK;
+}
+
 int check_status(fmcs_ctx *ctx, const char *what)
 {
     cudaError_t e = cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost,
@@ -180,7 +221,7 @@ static void load_tuning(fmcs_ctx *ctx)
     const std::string txt = ss.str();
     double v;
     if (json_number(txt, "rank_mode", &v)) ctx->rank_mode = v != 0.0 ? 1 : 0;
-    if (json_number(txt, "local_max", &v) && v >= 128 && v <= 4096) ctx->local_max = (uint32_t)v;
+    if (json_number(txt, "local_max", &v) && v >= 128 && v <= 8192) ctx->local_max = (uint32_t)v;
     if (json_number(txt, "msd_items", &v)) ctx->msd_items = v >= 16 ? 16 : 8;
 }
 
@@ -238,6 +279,7 @@ extern "C" void fmcs_destroy(fmcs_ctx *ctx)
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
     if (ctx->ev_level) cudaEventDestroy(ctx->ev_level);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -331,7 +373,7 @@ extern "C" int fmcs_set_tuning(fmcs_ctx *ctx, const char *key, long long value)
     if (k == "rank_mode") {
         ctx->rank_mode = value ? 1 : 0;
     } else if (k == "local_max") {
-        if (value < 128 || value > 4096) return set_error(ctx, FMCS_E_INVAL, "local_max must be in 128..4096");
+        if (value < 128 || value > 8192) return set_error(ctx, FMCS_E_INVAL, "local_max must be in 128..8192");
         ctx->local_max = (uint32_t)value;
     } else if (k == "msd_items") {
         if (value != 8 && value != 16) return set_error(ctx, FMCS_E_INVAL, "msd_items must be 8 or 16");

@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -68,6 +69,7 @@ struct fmcs_ctx {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;     // capture stream of conditional-node bodies (created on first use)
     size_t budget = 0;   // 0 = unlimited
     size_t held = 0;     // bytes held by the workspace
     fmcs::Workspace ws;
@@ -84,7 +86,7 @@ struct fmcs_ctx {
     cudaEvent_t ev_level = nullptr;    // host-side read-back point of the sort levels
     // tuned knobs (the autotuner's tuning/b200.json, FMCS_TUNING, or fmcs_set_tuning)
     int rank_mode = 0;                 // 0: match.any multi-split, 1: ballot multi-split
-    uint32_t local_max = 4096;         // segments above this many rows take the MSD levels
+    uint32_t local_max = 8192;         // segments above this many rows take the MSD levels
     uint32_t msd_items = 8;            // items per thread of an MSD tile (8 or 16)
     int prof_round = -1;               // round tag of the launches being profiled
 };
@@ -110,6 +112,13 @@ class LaunchScope {
     fmcs_ctx *ctx_;
     int rec_ = -1;
 };
+
+// Appends a WHILE conditional node to the graph being captured on `st` and
+// captures body(stream, handle) as the loop body.  The handle is 1 at the
+// start of every graph launch; a kernel of the body sets it to 0 (with
+// cudaGraphSetConditional) to end the loop.
+int capture_while(fmcs_ctx *ctx, cudaStream_t st,
+                  const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body);
 
 // True when the device can dereference p directly (device or managed memory).
 bool is_device_ptr(const void *p);

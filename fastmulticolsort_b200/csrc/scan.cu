@@ -22,7 +22,50 @@ constexpr int kScanItems = 16;                  // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kScanWarps = kScanThreads / 32;
 
-template <typename K>
+// kScanItems consecutive values starting at i0 (zero past n); 16-byte vector
+// loads when the run is whole and VEC (the caller checked the alignment).
+template <typename T, bool VEC>
+__device__ __forceinline__ void load_run(const T *__restrict__ p, uint64_t i0, uint64_t n, T (&v)[kScanItems])
+{
+    if (VEC && i0 + kScanItems <= n) {
+        constexpr int W = kScanItems * (int)sizeof(T) / 16;
+        const uint4 *q = reinterpret_cast<const uint4 *>(p + i0);
+        uint4 t[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) t[w] = q[w];
+        memcpy(&v[0], &t[0], sizeof(t));
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v[k] = i0 + k < n ? p[i0 + k] : T(0);
+    }
+}
+
+// Decoupled look-back by one warp: each lane reads one predecessor's word
+// (bounded waits), and the warp adds the aggregates back to the nearest
+// inclusive prefix.  Returns the exclusive prefix of `tile` (every lane).
+__device__ __forceinline__ uint32_t warp_lookback(unsigned long long *lookback, uint32_t tile, uint32_t epoch,
+                                                  int *status)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t excl = 0;
+    int64_t last = (int64_t)tile - 1;   // the window is tiles last - lane
+    for (;;) {
+        const int64_t p = last - lane;
+        const unsigned long long w = p >= 0 ? lb_wait(&lookback[p], epoch, status) : lb_word(epoch, kFlagInclusive, 0);
+        const uint32_t inc = __ballot_sync(0xFFFFFFFFu, ((uint32_t)(w >> 32) & 3u) == kFlagInclusive);
+        const int first = inc ? __ffs(inc) - 1 : 32;   // nearest inclusive predecessor
+        uint32_t v = lane <= first ? (uint32_t)w : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        excl += v;
+        if (inc) return excl;
+        last -= 32;
+    }
+}
+
+// One tile of kScanTile positions per block; thread t owns the kScanItems
+// consecutive positions starting at tile base + t * kScanItems.
+template <typename K, bool VEC>
 __global__ void __launch_bounds__(kScanThreads)
 boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group,
                      const uint8_t *__restrict__ flags, uint32_t *__restrict__ out_group, uint32_t *__restrict__ seg_start,
@@ -39,74 +82,122 @@ boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in
     const uint64_t base = (uint64_t)tile * kScanTile;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const uint64_t wbase = base + (uint64_t)warp * (kScanItems * 32);
+    const uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
 
-    // flags in warp-striped order: item j of lane l sits at wbase + j*32 + l
-    uint32_t ballots[kScanItems];
-    uint32_t wtotal = 0;
+    // boundary flags of the thread's positions, bit k = position i0 + k
+    uint32_t fl = 0;
+    if (i0 < n) {
+        if (flags) {
+            uint8_t f[kScanItems];
+            load_run<uint8_t, VEC>(flags, i0, n, f);
 #pragma unroll
-    for (int j = 0; j < kScanItems; ++j) {
-        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
-        bool f = false;
-        if (i < n) {
-            if (flags) {
-                f = flags[i] != 0;
-            } else if (i == 0) {
-                f = true;
-            } else {
-                if (keys) f = keys[i] != keys[i - 1];
-                if (in_group) f = f || (in_group[i] != in_group[i - 1]);
+            for (int k = 0; k < kScanItems; ++k) fl |= (uint32_t)(f[k] != 0) << k;
+        } else {
+            if (keys) {
+                K v[kScanItems];
+                load_run<K, VEC>(keys, i0, n, v);
+                K prev = i0 > 0 ? keys[i0 - 1] : K(0);
+#pragma unroll
+                for (int k = 0; k < kScanItems; ++k) {
+                    fl |= (uint32_t)(v[k] != prev) << k;
+                    prev = v[k];
+                }
             }
+            if (in_group) {
+                uint32_t g[kScanItems];
+                load_run<uint32_t, VEC>(in_group, i0, n, g);
+                uint32_t prev = i0 > 0 ? in_group[i0 - 1] : 0u;
+#pragma unroll
+                for (int k = 0; k < kScanItems; ++k) {
+                    fl |= (uint32_t)(g[k] != prev) << k;
+                    prev = g[k];
+                }
+            }
+            if (i0 == 0) fl |= 1u;
         }
-        ballots[j] = __ballot_sync(0xFFFFFFFFu, f);
-        wtotal += __popc(ballots[j]);
+        if (n - i0 < (uint64_t)kScanItems) fl &= (1u << (uint32_t)(n - i0)) - 1u;   // positions past n
     }
-    if (lane == 0) s_warp[warp] = wtotal;
+    const uint32_t cnt = __popc(fl);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int w = 0; w < kScanWarps; ++w) {
-            uint32_t c = s_warp[w];
-            s_warp[w] = run;
-            run += c;
+    if (warp == 0) {
+        uint32_t wv = lane < kScanWarps ? s_warp[lane] : 0u;
+        uint32_t wi = wv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= o) wi += y;
         }
-        s_warp[kScanWarps] = run;
-        // decoupled look-back over previous tiles
-        const uint32_t agg = run;
+        const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, kScanWarps - 1);
+        if (lane < kScanWarps) s_warp[lane] = wi - wv;
         uint32_t excl = 0;
         if (tile == 0) {
-            st_volatile_u64(&lookback[0], lb_word(epoch, kFlagInclusive, agg));
+            if (lane == 0) st_volatile_u64(&lookback[0], lb_word(epoch, kFlagInclusive, agg));
         } else {
-            st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagAggregate, agg));
-            int64_t p = (int64_t)tile - 1;
-            while (p >= 0) {
-                unsigned long long w = lb_wait(&lookback[p], epoch, status);
-                excl += (uint32_t)w;
-                if (((uint32_t)(w >> 32) & 3u) == kFlagInclusive) break;
-                --p;
-            }
-            st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
+            if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagAggregate, agg));
+            excl = warp_lookback(lookback, tile, epoch, status);
+            if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
         }
-        s_excl = excl;
-        if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
+        if (lane == 0) {
+            s_excl = excl;
+            s_warp[kScanWarps] = agg;
+            if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
+        }
     }
     __syncthreads();
-    uint32_t run = s_excl + s_warp[warp];
+    if (i0 < n) {
+        // 1-based id of the group holding position i0 + k, for every k
+        uint32_t id = s_excl + s_warp[warp] + incl - cnt;
+        if (out_group) {
+            uint32_t o[kScanItems];
 #pragma unroll
-    for (int j = 0; j < kScanItems; ++j) {
-        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
-        const uint32_t b = ballots[j];
-        const uint32_t incl = run + __popc(b & (lanemask_lt() | (1u << lane)));
-        if (i < n) {
-            if (out_group) out_group[i] = incl - 1;
-            if (seg_start && ((b >> lane) & 1u)) seg_start[incl - 1] = (uint32_t)i;
+            for (int k = 0; k < kScanItems; ++k) {
+                id += (fl >> k) & 1u;
+                o[k] = id - 1u;
+            }
+            if (VEC && i0 + kScanItems <= n) {
+                uint4 *q = reinterpret_cast<uint4 *>(out_group + i0);
+#pragma unroll
+                for (int w = 0; w < kScanItems / 4; ++w) q[w] = make_uint4(o[4 * w], o[4 * w + 1], o[4 * w + 2], o[4 * w + 3]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kScanItems; ++k)
+                    if (i0 + k < n) out_group[i0 + k] = o[k];
+            }
         }
-        run += __popc(b);
+        if (seg_start) {
+            uint32_t sid = s_excl + s_warp[warp] + incl - cnt;
+            for (uint32_t m = fl; m; m &= m - 1) {
+                const uint32_t k = __ffs(m) - 1;
+                seg_start[sid++] = (uint32_t)(i0 + k);
+            }
+        }
     }
     if (seg_start && base + kScanTile >= n && threadIdx.x == 0) {
-        // total written by thread 0 above into *d_count; the end sentinel
+        // the end sentinel after the last segment
         seg_start[s_excl + s_warp[kScanWarps]] = (uint32_t)n;
     }
+}
+
+// Launches the scan, with 16-byte vector accesses when every array allows.
+template <typename K>
+void launch_scan(unsigned grid, cudaStream_t st, const K *keys, const uint32_t *in_group, const uint8_t *flags,
+                 uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_counter,
+                 unsigned long long *lookback, uint32_t epoch, uint32_t *d_count, int *status)
+{
+    const bool vec = (((uintptr_t)keys | (uintptr_t)in_group | (uintptr_t)flags | (uintptr_t)out_group) & 15u) == 0;
+    if (vec)
+        boundary_scan_kernel<K, true><<<grid, kScanThreads, 0, st>>>(keys, in_group, flags, out_group, seg_start, n,
+                                                                      tile_counter, lookback, epoch, d_count, status);
+    else
+        boundary_scan_kernel<K, false><<<grid, kScanThreads, 0, st>>>(keys, in_group, flags, out_group, seg_start, n,
+                                                                       tile_counter, lookback, epoch, d_count, status);
 }
 
 int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
@@ -127,41 +218,28 @@ int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const
     cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), ctx->stream);
     const uint32_t epoch = ctx->epoch++;
     const unsigned grid = (unsigned)tiles;
+    unsigned long long *lbw = (unsigned long long *)lb;
+    LaunchScope ls_(ctx, "boundary_scan");
     switch (keys ? key_bytes : 0) {
     case 0:
-        { LaunchScope ls_(ctx, "boundary_scan");
-            boundary_scan_kernel<uint32_t><<<grid, kScanThreads, 0, ctx->stream>>>(
-                nullptr, in_group, flags, out_group, seg_start, n, tile_counter, (unsigned long long *)lb, epoch,
-                d_count, ctx->d_status);
-        }
+        launch_scan<uint32_t>(grid, ctx->stream, nullptr, in_group, flags, out_group, seg_start, n, tile_counter, lbw,
+                              epoch, d_count, ctx->d_status);
         break;
     case 1:
-        { LaunchScope ls_(ctx, "boundary_scan");
-            boundary_scan_kernel<uint8_t><<<grid, kScanThreads, 0, ctx->stream>>>(
-                (const uint8_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
-                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
-        }
+        launch_scan<uint8_t>(grid, ctx->stream, (const uint8_t *)keys, in_group, flags, out_group, seg_start, n,
+                             tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     case 2:
-        { LaunchScope ls_(ctx, "boundary_scan");
-            boundary_scan_kernel<uint16_t><<<grid, kScanThreads, 0, ctx->stream>>>(
-                (const uint16_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
-                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
-        }
+        launch_scan<uint16_t>(grid, ctx->stream, (const uint16_t *)keys, in_group, flags, out_group, seg_start, n,
+                              tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     case 4:
-        { LaunchScope ls_(ctx, "boundary_scan");
-            boundary_scan_kernel<uint32_t><<<grid, kScanThreads, 0, ctx->stream>>>(
-                (const uint32_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
-                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
-        }
+        launch_scan<uint32_t>(grid, ctx->stream, (const uint32_t *)keys, in_group, flags, out_group, seg_start, n,
+                              tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     case 8:
-        { LaunchScope ls_(ctx, "boundary_scan");
-            boundary_scan_kernel<uint64_t><<<grid, kScanThreads, 0, ctx->stream>>>(
-                (const uint64_t *)keys, in_group, flags, out_group, seg_start, n, tile_counter,
-                (unsigned long long *)lb, epoch, d_count, ctx->d_status);
-        }
+        launch_scan<uint64_t>(grid, ctx->stream, (const uint64_t *)keys, in_group, flags, out_group, seg_start, n,
+                              tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     default:
         return set_error(ctx, FMCS_E_INVAL, "boundary scan: bad key width");
@@ -304,24 +382,20 @@ extern "C" int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t k
     const unsigned grid = (unsigned)tiles;
     switch (key_bytes) {
     case 1:
-        boundary_scan_kernel<uint8_t><<<grid, kScanThreads, 0, st>>>((const uint8_t *)keys, in_group, nullptr,
-                                                                      out_group, nullptr, n, tile_counter, lookback,
-                                                                      epoch, d_count, status);
+        launch_scan<uint8_t>(grid, st, (const uint8_t *)keys, in_group, nullptr, out_group, nullptr, n,
+                             tile_counter, lookback, epoch, d_count, status);
         break;
     case 2:
-        boundary_scan_kernel<uint16_t><<<grid, kScanThreads, 0, st>>>((const uint16_t *)keys, in_group, nullptr,
-                                                                       out_group, nullptr, n, tile_counter, lookback,
-                                                                       epoch, d_count, status);
+        launch_scan<uint16_t>(grid, st, (const uint16_t *)keys, in_group, nullptr, out_group, nullptr, n,
+                              tile_counter, lookback, epoch, d_count, status);
         break;
     case 4:
-        boundary_scan_kernel<uint32_t><<<grid, kScanThreads, 0, st>>>((const uint32_t *)keys, in_group, nullptr,
-                                                                       out_group, nullptr, n, tile_counter, lookback,
-                                                                       epoch, d_count, status);
+        launch_scan<uint32_t>(grid, st, (const uint32_t *)keys, in_group, nullptr, out_group, nullptr, n,
+                              tile_counter, lookback, epoch, d_count, status);
         break;
     default:
-        boundary_scan_kernel<uint64_t><<<grid, kScanThreads, 0, st>>>((const uint64_t *)keys, in_group, nullptr,
-                                                                       out_group, nullptr, n, tile_counter, lookback,
-                                                                       epoch, d_count, status);
+        launch_scan<uint64_t>(grid, st, (const uint64_t *)keys, in_group, nullptr, out_group, nullptr, n,
+                              tile_counter, lookback, epoch, d_count, status);
         break;
     }
     e = cudaGetLastError();

@@ -50,8 +50,9 @@ constexpr int kItemsA = 4;
 constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
 constexpr int kNtB2 = 128, kItB2 = 8, kCapB2 = kNtB2 * kItB2;   // 1024
 constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
-constexpr int kNtC2 = 256, kItC2 = 16, kCapC2 = kNtC2 * kItC2;  // 4096
-constexpr int kCapLocal = kCapC2;   // largest segment a local tier can take; larger: MSD levels
+constexpr int kNtC2 = 512, kItC2 = 8, kCapC2 = kNtC2 * kItC2;   // 4096
+constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
+constexpr int kCapLocal = kCapC3;   // largest segment a local tier can take; larger: MSD levels
 constexpr int kNtM = 256;           // MSD tile: 256 threads x IT items (IT = 8 or 16, tuned)
 
 // counters slot words
@@ -69,11 +70,34 @@ constexpr int kCtrLocalT32 = 14;
 constexpr int kCtrCopyLarge = 12;   // copy entries larger than kCopySplit rows
 constexpr int kCtrCopyTile = 13;
 constexpr uint32_t kCopySplit = 4096;
-constexpr int kCtrWords = 16;
+constexpr int kCtrLevel = 15;      // MSD levels started so far (device-side level index)
+constexpr int kCtrLocalC3 = 16;
+constexpr int kCtrWords = 32;
 
 struct LargeSeg {
     uint32_t start, len, shift, src;
 };
+
+// The two alternating sets of an MSD level's buffers (large-segment list and
+// digit histogram rows; level L reads set L & 1 and fills set (L + 1) & 1).
+// With dev_level the level index is read on the device (ctr[kCtrLevel]), so a
+// level's launches are the same for every level (one graph body that loops);
+// otherwise every launch works on set 0.
+// (Kernels select a set with a conditional, not by indexing with the level
+// parity: a parameter array indexed at run time is copied to local memory.)
+struct LevelRefs {
+    LargeSeg *large[2];
+    uint32_t *hist[2];
+    uint32_t *ctr;
+    int dev_level;
+};
+
+// Index of the level whose launches are running (level_prefix_kernel has
+// already advanced the counter for it).
+__device__ __forceinline__ uint32_t running_level(const LevelRefs &r)
+{
+    return r.dev_level ? *(volatile const uint32_t *)&r.ctr[kCtrLevel] - 1u : 0u;
+}
 
 template <typename K>
 struct Bufs {
@@ -116,7 +140,7 @@ __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32
 }
 
 struct Lists {
-    uint2 *t, *t32, *a, *b1, *b2, *c1, *c2;
+    uint2 *t, *t32, *a, *b1, *b2, *c1, *c2, *c3;
     uint32_t cap_t32;      // kCapT32 for keys of <= 4 bytes, else 0 (17..32 rows go to the warp tier)
     LargeSeg *copy;        // segments that only need to reach BUF0, <= kCopySplit rows (warp each)
     LargeSeg *copy_large;  // the same, larger: copied by tiles across the grid
@@ -160,6 +184,7 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
     else if (len <= (uint32_t)kCapB2) L.b2[atomicAdd(&ctr[kCtrLocalB2], 1u)] = e;
     else if (len <= (uint32_t)kCapC1) L.c1[atomicAdd(&ctr[kCtrLocalC1], 1u)] = e;
     else if (len <= (uint32_t)kCapC2) L.c2[atomicAdd(&ctr[kCtrLocalC2], 1u)] = e;
+    else if (len <= (uint32_t)kCapC3) L.c3[atomicAdd(&ctr[kCtrLocalC3], 1u)] = e;
     else {
         // a large segment: its digit histogram row starts at zero
         const uint32_t slot = atomicAdd(&ctr[large_ctr], 1u);
@@ -202,18 +227,11 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
 // Exclusive prefix of the tile counts of the level's large segments (one CTA).
 // Also resets the level's counters (tile counter, rows moved, next-level
 // count) so that no separate memsets are needed.
-__global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs, const uint32_t *d_nseg,
-                                                           uint32_t *tile_prefix, uint32_t *reset0,
-                                                           uint32_t *reset1, uint32_t *reset2, uint32_t tile_rows)
+__device__ __forceinline__ void tile_prefix_body(const LargeSeg *segs, uint32_t nseg, uint32_t *tile_prefix,
+                                                 uint32_t tile_rows)
 {
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry;
-    const uint32_t nseg = *d_nseg;
-    if (threadIdx.x == 0) {
-        *reset0 = 0;
-        *reset1 = 0;
-        *reset2 = 0;
-    }
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (uint32_t base = 0; base < nseg; base += blockDim.x) {
@@ -245,6 +263,31 @@ __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs,
     if (threadIdx.x == 0) tile_prefix[nseg] = carry;
 }
 
+__global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs, const uint32_t *d_nseg,
+                                                           uint32_t *tile_prefix, uint32_t *reset, uint32_t tile_rows)
+{
+    if (threadIdx.x == 0) *reset = 0;
+    tile_prefix_body(segs, *d_nseg, tile_prefix, tile_rows);
+}
+
+// First launch of an MSD level: tile prefix of the level's large segments,
+// resets of the level's counters, and (device-side levels) the level index
+// advanced for the level's other launches.
+__global__ void __launch_bounds__(1024) level_prefix_kernel(LevelRefs r, uint32_t *tile_prefix, uint32_t tile_rows)
+{
+    const uint32_t lvl = r.dev_level ? r.ctr[kCtrLevel] : 0u;
+    const uint32_t cur = lvl & 1u, nxt = cur ^ 1u;
+    const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
+    __syncthreads();   // every thread has read the level index before it advances
+    if (threadIdx.x == 0) {
+        r.ctr[kCtrLarge0 + nxt] = 0;
+        r.ctr[kCtrMsdTile] = 0;
+        r.ctr[kCtrMoved] = 0;
+        if (r.dev_level) r.ctr[kCtrLevel] = lvl + 1;
+    }
+    tile_prefix_body((cur ? r.large[1] : r.large[0]), nseg, tile_prefix, tile_rows);
+}
+
 
 __device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
 {
@@ -261,13 +304,16 @@ __device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, ui
 // in flight), and each warp counts into its own shared sub-histogram so that
 // skewed digits do not serialize the whole block on one counter.
 template <typename K>
-__global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
-                                                        const uint32_t *tile_prefix, uint32_t *hist, uint32_t tile_rows)
+__global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, const uint32_t *tile_prefix,
+                                                        uint32_t tile_rows)
 {
     constexpr int NW = kNtM / 32;
     constexpr int MAXJ = 16;   // tile_rows <= 16 * kNtM
     __shared__ uint32_t sh[NW][kRadix];
-    const uint32_t nseg = *d_nseg;
+    const uint32_t cur = running_level(r) & 1u;
+    const LargeSeg *segs = (cur ? r.large[1] : r.large[0]);
+    uint32_t *hist = (cur ? r.hist[1] : r.hist[0]);
+    const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
     const int warp = threadIdx.x >> 5;
@@ -304,15 +350,19 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, const LargeSe
 }
 
 // Per large segment: exclusive digit offsets, skip detection, children.
-__global__ void __launch_bounds__(kRadix) msd_plan_kernel(LargeSeg *segs, const uint32_t *d_nseg,
-                                                          uint32_t *hist, uint32_t *ctr, int next_large_ctr,
-                                                          LargeSeg *large_next, Lists lists, uint32_t *hist_next,
-                                                          bool emit_children = true)
+__global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lists, bool emit_children = true)
 {
     __shared__ uint32_t cnt[kRadix];
     __shared__ uint32_t tmp[kRadix / 32 + 1];
     __shared__ uint32_t s_skip;
-    const uint32_t nseg = *d_nseg;
+    const uint32_t cur = running_level(r) & 1u, nxt = cur ^ 1u;
+    LargeSeg *segs = (cur ? r.large[1] : r.large[0]);
+    uint32_t *hist = (cur ? r.hist[1] : r.hist[0]);
+    uint32_t *ctr = r.ctr;
+    const int next_large_ctr = kCtrLarge0 + (int)nxt;
+    LargeSeg *large_next = (nxt ? r.large[1] : r.large[0]);
+    uint32_t *hist_next = (nxt ? r.hist[1] : r.hist[0]);
+    const uint32_t nseg = ctr[kCtrLarge0 + cur];
     for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
         const LargeSeg sg = segs[s];
         const uint32_t d = threadIdx.x;
@@ -351,15 +401,25 @@ struct MsdSmem {
 };
 
 template <typename K, int RANK, int IT>
-__global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(Bufs<K> b, const LargeSeg *segs, const uint32_t *d_nseg,
-                                                           const uint32_t *tile_prefix, const uint32_t *offs,
-                                                           uint32_t *tile_counter, unsigned long long *lookback,
-                                                           uint32_t epoch, int *status)
+__global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(Bufs<K> b, LevelRefs r,
+                                                           const uint32_t *tile_prefix, unsigned long long *lookback,
+                                                           uint32_t epoch_base, int *status,
+                                                           cudaGraphConditionalHandle more, uint32_t levels)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MsdSmem<K, IT> &sm = *reinterpret_cast<MsdSmem<K, IT> *>(smem_raw);
     constexpr uint32_t kTileM = kNtM * IT;
-    const uint32_t nseg = *d_nseg;
+    const uint32_t lvl = running_level(r);
+    const uint32_t cur = lvl & 1u;
+    const LargeSeg *segs = (cur ? r.large[1] : r.large[0]);
+    const uint32_t *offs = (cur ? r.hist[1] : r.hist[0]);
+    uint32_t *tile_counter = &r.ctr[kCtrMsdTile];
+    const uint32_t epoch = epoch_base + lvl;
+    const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
+    // Inside a graph, the level loop goes on while the next level has large
+    // segments (msd_plan has counted them before this launch).
+    if (more && blockIdx.x == 0 && threadIdx.x == 0)
+        cudaGraphSetConditional(more, (r.ctr[kCtrLarge0 + (cur ^ 1u)] > 0 && lvl + 1 < levels) ? 1u : 0u);
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
     const int warp = threadIdx.x >> 5;
@@ -462,9 +522,19 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
 // ---------------------------------------------------------------------------
 // local tiers
 // ---------------------------------------------------------------------------
-// Block-per-segment stable sort over key bits [0, shift).
+// Block-per-segment stable sort over key bits [0, shift).  One HBM read and
+// one HBM write per row; everything else in shared memory.
 //
-// Strategy (all in shared memory, one HBM read and one HBM write per row):
+// Fast path (bucket_rank_sort): the bits in which the segment's keys differ
+// are found by an OR/AND reduction; rows are bucketed by the top
+// ceil(log2(len)) of those bits (about one row per bucket) with shared-memory
+// atomics, in no particular order inside a bucket; each row's final place is
+// then its bucket's start plus the number of rows of the bucket that sort
+// before it by (key, position in the segment).  Ties are decided by the
+// position, so the result is the stable order although the bucketing is not.
+//
+// Fallback, when some bucket holds more than kBucketMax rows (heavily
+// repeated keys):
 //   1. one stable split on the top digit (bits [shift-8, shift)), ranked by
 //      warp-level multi-split: rows land in 256 buckets in key order;
 //   2. if every bucket holds <= kCountRankMax rows, each row's final place is
@@ -475,6 +545,207 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
 //      pass on the top digit finish the sort from the split order.
 // Every step is stable, so ties keep their input order.
 constexpr uint32_t kCountRankMax = 64;
+constexpr uint32_t kBucketMax = 64;
+
+template <typename K, int NT, int IT>
+struct BucketSmem {
+    unsigned long long cs[NT * IT];   // compound keys, bucketed
+    uint32_t vals[NT * IT];
+    uint32_t off[NT * IT + 1];        // per bucket: count -> start; then (as u16) final place -> slot
+    uint16_t orig[NT * IT];           // position in the segment, when the compound key has no room for it
+    uint32_t tmp[NT / 32 + 1];
+    unsigned long long any, all;      // OR and AND of the segment's keys
+    uint32_t maxb;
+};
+
+// Exclusive scan of off[0, nb) by the block (nb a power of two >= NT or any
+// nb <= NT), also leaving the largest count in *maxb.
+template <int NT>
+__device__ __forceinline__ void block_scan_bins(uint32_t *off, uint32_t nb, uint32_t *tmp, uint32_t *maxb)
+{
+    const uint32_t per = nb >= (uint32_t)NT ? nb / NT : 1u;
+    const uint32_t base = threadIdx.x * per;
+    uint32_t sum = 0, mx = 0;
+    if (base < nb) {
+        for (uint32_t i = 0; i < per; ++i) {
+            const uint32_t c = off[base + i];
+            sum += c;
+            mx = max(mx, c);
+        }
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if ((int)lane_id() >= o) incl += y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 31) tmp[w] = incl;
+    if (lane_id() == 0) atomicMax(maxb, mx);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t v = threadIdx.x < NT / 32 ? tmp[threadIdx.x] : 0u;
+        uint32_t vi = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, vi, o);
+            if ((int)threadIdx.x >= o) vi += y;
+        }
+        if (threadIdx.x < NT / 32) tmp[threadIdx.x] = vi - v;
+    }
+    __syncthreads();
+    uint32_t run = tmp[w] + incl - sum;
+    if (base < nb) {
+        for (uint32_t i = 0; i < per; ++i) {
+            const uint32_t c = off[base + i];
+            off[base + i] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+}
+
+// The fast path above.  Rows are in registers (warp w holds positions
+// wbase + j*32 + lane, j < steps).  Returns false, with nothing written,
+// when a bucket is too large; the caller then runs the stable fallback.
+// Ends with a block barrier either way.
+//
+// Compound key: the key bits below `top` (the bits above are the same in
+// every row), shifted left by nbits with the row's position in the low
+// nbits when they fit in 64 bits, so that compound keys are all distinct and
+// compare like (key, position).  Otherwise the position is kept beside it.
+// A row's bucket is the top `width` bits of its compound key; its final place
+// is its bucket's start plus the rows of the bucket with a smaller compound
+// key, found by scanning the neighbouring slots while they hold the same
+// bucket (buckets hold about one row).
+template <typename K, int NT, int IT>
+__device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, const K (&key)[IT],
+                                                 const uint32_t (&val)[IT], uint32_t steps, uint32_t wbase,
+                                                 uint32_t len, const Bufs<K> &b, uint32_t start)
+{
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        sm.any = 0ull;
+        sm.all = ~0ull;
+        sm.maxb = 0;
+    }
+    __syncthreads();
+    unsigned long long any = 0ull, all = ~0ull;
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t p = wbase + j * 32 + lane;
+        if (j < (int)steps && p < len) {
+            any |= (unsigned long long)key[j];
+            all &= (unsigned long long)key[j];
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        any |= __shfl_xor_sync(0xFFFFFFFFu, any, o);
+        all &= __shfl_xor_sync(0xFFFFFFFFu, all, o);
+    }
+    if (lane == 0) {
+        atomicOr(&sm.any, any);
+        atomicAnd(&sm.all, all);
+    }
+    __syncthreads();
+    const unsigned long long diff = sm.any & ~sm.all;
+    if (diff == 0ull) {
+        // every key is the same: the segment is in order already
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (j < (int)steps && p < len) {
+                b.k0[(uint64_t)start + p] = key[j];
+                b.v0[(uint64_t)start + p] = val[j];
+            }
+        }
+        __syncthreads();
+        return true;
+    }
+    const uint32_t top = 64u - (uint32_t)__clzll((long long)diff);   // bits [0, top) differ somewhere
+    const unsigned long long low = top >= 64u ? ~0ull : ((1ull << top) - 1ull);
+    const unsigned long long prefix = sm.all & ~low;                 // the bits every row shares
+    const uint32_t nbits = 32u - (uint32_t)__clz(len - 1u);          // ceil(log2(len)), len >= 2
+    const bool packed = top + nbits <= 64u;
+    const uint32_t sh = packed ? nbits : 0u;
+    const uint32_t lo = top > nbits ? top - nbits : 0u;
+    const uint32_t width = top - lo;
+    const uint32_t dshift = lo + sh;                                 // bucket = compound >> dshift
+    const uint32_t nb = 1u << width;
+    for (uint32_t i = threadIdx.x; i <= nb; i += NT) sm.off[i] = 0;
+    __syncthreads();
+    uint32_t slot[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t p = wbase + j * 32 + lane;
+        if (j < (int)steps && p < len)
+            slot[j] = atomicAdd(&sm.off[(uint32_t)((((unsigned long long)key[j] & low) << sh) >> dshift)], 1u);
+    }
+    __syncthreads();
+    block_scan_bins<NT>(sm.off, nb, sm.tmp, &sm.maxb);
+    if (sm.maxb > kBucketMax) {
+        __syncthreads();
+        return false;   // uniform across the block
+    }
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t p = wbase + j * 32 + lane;
+        if (j < (int)steps && p < len) {
+            const unsigned long long c = ((((unsigned long long)key[j] & low) << sh)) | (packed ? p : 0u);
+            const uint32_t pos = sm.off[(uint32_t)(c >> dshift)] + slot[j];
+            sm.cs[pos] = c;
+            sm.vals[pos] = val[j];
+            if (!packed) sm.orig[pos] = (uint16_t)p;
+        }
+    }
+    __syncthreads();
+    uint16_t *perm = reinterpret_cast<uint16_t *>(sm.off);   // off is not needed any more
+    for (uint32_t p = threadIdx.x; p < len; p += NT) {
+        const unsigned long long c = sm.cs[p];
+        const unsigned long long d = c >> dshift;
+        uint32_t r = 0, before = 0;
+        if (packed) {
+            for (int q = (int)p - 1; q >= 0; --q) {
+                const unsigned long long cq = sm.cs[q];
+                if ((cq >> dshift) != d) break;
+                ++before;
+                r += cq < c;
+            }
+            for (uint32_t q = p + 1; q < len; ++q) {
+                const unsigned long long cq = sm.cs[q];
+                if ((cq >> dshift) != d) break;
+                r += cq < c;
+            }
+        } else {
+            const uint32_t o = sm.orig[p];
+            for (int q = (int)p - 1; q >= 0; --q) {
+                const unsigned long long cq = sm.cs[q];
+                if ((cq >> dshift) != d) break;
+                ++before;
+                r += (cq < c) | ((cq == c) & ((uint32_t)sm.orig[q] < o));
+            }
+            for (uint32_t q = p + 1; q < len; ++q) {
+                const unsigned long long cq = sm.cs[q];
+                if ((cq >> dshift) != d) break;
+                r += (cq < c) | ((cq == c) & ((uint32_t)sm.orig[q] < o));
+            }
+        }
+        perm[p - before + r] = (uint16_t)p;
+    }
+    __syncthreads();
+    // every load of this segment is done (barriers above) before the first
+    // store into BUF0, which may alias the EXT oids of the range
+    for (uint32_t p = threadIdx.x; p < len; p += NT) {
+        const uint32_t q = perm[p];
+        b.k0[(uint64_t)start + p] = (K)(prefix | (sm.cs[q] >> sh));
+        b.v0[(uint64_t)start + p] = sm.vals[q];
+    }
+    __syncthreads();
+    return true;
+}
 
 template <typename K, int NT, int IT>
 struct BlockSmem {
@@ -558,12 +829,91 @@ __device__ __forceinline__ bool block_pass(BlockSmem<K, NT, IT> &sm, K (&key)[IT
     return true;
 }
 
+// The stable fallback of the block sort (see above) for one segment; rows
+// are loaded again from HBM.  Kept out of line so that its register demand
+// does not weigh on the fast path.
 template <typename K, int NT, int IT, int RANK>
-__global__ void __launch_bounds__(NT, (NT * IT >= 4096 ? 2 : (NT * IT >= 2048 ? 3 : 4)))
+__device__ __noinline__ void block_sort_fallback(BlockSmem<K, NT, IT> &sm, Bufs<K> b, uint32_t start, uint32_t len,
+                                                 uint32_t shift, uint32_t src)
+{
+    constexpr int NW = NT / 32;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t steps = (len + NW * 32 - 1) / (NW * 32);
+    const uint32_t wbase = warp * steps * 32;
+    K key[IT];
+    uint32_t val[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t p = wbase + j * 32 + lane;
+        key[j] = 0;
+        val[j] = 0;
+        if (j < (int)steps && p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
+    }
+    bool written = false;
+    uint32_t lsd_top = shift;   // LSD passes cover [0, lsd_top)
+    if (shift > (uint32_t)kRadixBits) {
+        const uint32_t top = shift - kRadixBits;
+        const bool moved = block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, top, kRadixBits, true);
+        if (!moved) {
+            lsd_top = top;   // the top digit is constant: sort the bits below it
+        } else if (sm.maxb <= kCountRankMax) {
+            // rows are in smem in top-digit order; rank each row inside its bucket
+            for (uint32_t p = threadIdx.x; p < len; p += NT) {
+                const K k = sm.keys[p];
+                const uint32_t v = sm.vals[p];
+                const uint32_t d = digit_of(k, top, kRadixBits);
+                const uint32_t b0 = sm.doff[d];
+                const uint32_t b1 = b0 + sm.cnt[d];
+                uint32_t r = 0;
+                for (uint32_t q = b0; q < b1; ++q) {
+                    const K kq = sm.keys[q];
+                    r += (kq < k) || (kq == k && q < p);
+                }
+                b.k0[(uint64_t)start + b0 + r] = k;
+                b.v0[(uint64_t)start + b0 + r] = v;
+            }
+            written = true;
+        } else {
+            // skewed: continue from the split order with LSD passes below the
+            // top digit, then the top digit again
+#pragma unroll
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t p = wbase + j * 32 + lane;
+                if (j < (int)steps && p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
+            }
+            __syncthreads();
+            for (uint32_t lo = 0; lo < top; lo += kRadixBits)
+                block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, lo, min((uint32_t)kRadixBits, top - lo),
+                                            false);
+            block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, top, kRadixBits, false);
+            lsd_top = 0;
+        }
+    }
+    if (!written) {
+        for (uint32_t lo = 0; lo < lsd_top; lo += kRadixBits)
+            block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, lo, min((uint32_t)kRadixBits, lsd_top - lo),
+                                        false);
+        // every load of this segment is done (barriers above) before the
+        // first store into BUF0, which may alias the EXT oids of the range
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (j < (int)steps && p < len) {
+                b.k0[(uint64_t)start + p] = key[j];
+                b.v0[(uint64_t)start + p] = val[j];
+            }
+        }
+    }
+}
+
+// 1024 threads per SM for every tier (64 registers a thread).
+template <typename K, int NT, int IT, int RANK>
+__global__ void __launch_bounds__(NT, 1024 / NT)
 block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockSmem<K, NT, IT> &sm = *reinterpret_cast<BlockSmem<K, NT, IT> *>(smem_raw);
     constexpr int NW = NT / 32;
     const uint32_t count = *d_count;
     const int warp = threadIdx.x >> 5;
@@ -587,63 +937,12 @@ block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
             val[j] = 0;
             if (j < (int)steps && p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
         }
-        bool written = false;
-        uint32_t lsd_top = shift;   // LSD passes cover [0, lsd_top)
-        if (shift > (uint32_t)kRadixBits) {
-            const uint32_t top = shift - kRadixBits;
-            const bool moved = block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, top, kRadixBits, true);
-            if (!moved) {
-                lsd_top = top;   // the top digit is constant: sort the bits below it
-            } else if (sm.maxb <= kCountRankMax) {
-                // rows are in smem in top-digit order; rank each row inside its bucket
-                for (uint32_t p = threadIdx.x; p < len; p += NT) {
-                    const K k = sm.keys[p];
-                    const uint32_t v = sm.vals[p];
-                    const uint32_t d = digit_of(k, top, kRadixBits);
-                    const uint32_t b0 = sm.doff[d];
-                    const uint32_t b1 = b0 + sm.cnt[d];
-                    uint32_t r = 0;
-                    for (uint32_t q = b0; q < b1; ++q) {
-                        const K kq = sm.keys[q];
-                        r += (kq < k) || (kq == k && q < p);
-                    }
-                    b.k0[(uint64_t)start + b0 + r] = k;
-                    b.v0[(uint64_t)start + b0 + r] = v;
-                }
-                written = true;
-            } else {
-                // skewed: continue from the split order with LSD passes below the
-                // top digit, then the top digit again
-#pragma unroll
-                for (int j = 0; j < IT; ++j) {
-                    const uint32_t p = wbase + j * 32 + lane;
-                    if (j < (int)steps && p < len) { key[j] = sm.keys[p]; val[j] = sm.vals[p]; }
-                }
-                __syncthreads();
-                for (uint32_t lo = 0; lo < top; lo += kRadixBits)
-                    block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, lo, min((uint32_t)kRadixBits, top - lo),
-                                                false);
-                block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, top, kRadixBits, false);
-                lsd_top = 0;
-            }
-        }
-        if (!written) {
-            for (uint32_t lo = 0; lo < lsd_top; lo += kRadixBits)
-                block_pass<K, NT, IT, RANK>(sm, key, val, steps, wbase, len, lo, min((uint32_t)kRadixBits, lsd_top - lo),
-                                            false);
-            // every load of this segment is done (barriers above) before the
-            // first store into BUF0, which may alias the EXT oids of the range
+        if (!bucket_rank_sort<K, NT, IT>(*reinterpret_cast<BucketSmem<K, NT, IT> *>(smem_raw), key, val, steps, wbase,
+                                         len, b, start)) {
+            block_sort_fallback<K, NT, IT, RANK>(*reinterpret_cast<BlockSmem<K, NT, IT> *>(smem_raw), b, start, len,
+                                                 shift, src);
             __syncthreads();
-#pragma unroll
-            for (int j = 0; j < IT; ++j) {
-                const uint32_t p = wbase + j * 32 + lane;
-                if (j < (int)steps && p < len) {
-                    b.k0[(uint64_t)start + p] = key[j];
-                    b.v0[(uint64_t)start + p] = val[j];
-                }
-            }
         }
-        __syncthreads();
     }
 }
 
@@ -890,7 +1189,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const uint64_t cap_t = n / 2 + 2, cap_t32 = n / (kCapT + 1) + 2, cap_a = n / (kCapT + 1) + 2;
     const uint64_t cap_b1 = n / (kCapA + 1) + 2;
     const uint64_t cap_b2 = n / (kCapB1 + 1) + 2;
-    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2;
+    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2, cap_c3 = n / (kCapC2 + 1) + 2;
     // copy entries: disjoint ranges; at most 256 children per large segment per
     // level, so bounded by both n and (levels + 1) * 256 * cap_large
     const uint64_t levels_max = (a.key_bits + kRadixBits - 1) / kRadixBits;
@@ -902,7 +1201,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     large[1] = (LargeSeg *)p;
     Lists lists;
     {
-        const uint64_t tot = cap_t + cap_t32 + cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2;
+        const uint64_t tot = cap_t + cap_t32 + cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2 + cap_c3;
         if ((rc = ws_get(ctx, kSlotLocalA, tot * sizeof(uint2), &p))) return rc;
         lists.t = (uint2 *)p;
         lists.t32 = lists.t + cap_t;
@@ -912,6 +1211,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         lists.b2 = lists.b1 + cap_b1;
         lists.c1 = lists.b2 + cap_b2;
         lists.c2 = lists.c1 + cap_c1;
+        lists.c3 = lists.c2 + cap_c2;
         if ((rc = ws_get(ctx, kSlotLocalC, (cap_copy + cap_large) * sizeof(LargeSeg), &p))) return rc;
         lists.copy = (LargeSeg *)p;
         lists.copy_large = lists.copy + cap_copy;
@@ -962,52 +1262,71 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level count");
             nlarge = ctx->h_small[8];
         }
-        for (int lvl = 0; lvl < levels && nlarge > 0; ++lvl) {
-            const int cur = lvl & 1, nxt = cur ^ 1;
-            const uint32_t *d_cnt = &ctr[kCtrLarge0 + cur];
+        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1};
+        const uint32_t epoch_base = ctx->epoch;
+        ctx->epoch += (uint32_t)levels;
+        const unsigned scatter_grid = sms * (IT >= 16 ? 2 : 4);
+        int host_lvl = 0;   // the level being launched, for the eager read-back
+        // one level: the same four launches for every level (the level index
+        // lives on the device)
+        auto level = [&](cudaStream_t s, cudaGraphConditionalHandle more, bool read_back) -> int {
             { LaunchScope ls_(ctx, "tile_prefix");
-                tile_prefix_kernel<<<1, 1024, 0, st>>>(large[cur], d_cnt, tile_prefix, &ctr[kCtrLarge0 + nxt],
-                                                       &ctr[kCtrMsdTile], &ctr[kCtrMoved], tile_rows);
+                level_prefix_kernel<<<1, 1024, 0, s>>>(lr, tile_prefix, tile_rows);
             }
-            uint32_t *hist = hists[cur];
             { LaunchScope ls_(ctx, "msd_hist");
-                msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, large[cur], d_cnt, tile_prefix, hist, tile_rows);
+                msd_hist_kernel<K><<<sms * 8, kNtM, 0, s>>>(b, lr, tile_prefix, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
-                msd_plan_kernel<<<sms * 8, kRadix, 0, st>>>(large[cur], d_cnt, hist, ctr, kCtrLarge0 + nxt, large[nxt],
-                                                             lists, hists[nxt]);
+                msd_plan_kernel<<<sms * 8, kRadix, 0, s>>>(lr, lists);
             }
-            if (!a.fixed_launches) {
+            if (read_back) {
                 // read the next level's count while the scatter runs
-                cudaMemcpyAsync(ctx->h_small + 8, &ctr[kCtrLarge0 + nxt], sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-                cudaMemcpyAsync(ctx->h_small + 9, &ctr[kCtrMoved], sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-                cudaEventRecord(ctx->ev_level, st);
+                const uint32_t nxt = (uint32_t)(host_lvl + 1) & 1u;
+                cudaMemcpyAsync(ctx->h_small + 8, &ctr[kCtrLarge0 + nxt], sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+                cudaMemcpyAsync(ctx->h_small + 9, &ctr[kCtrMoved], sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+                cudaEventRecord(ctx->ev_level, s);
             }
             {
                 LaunchScope ls_(ctx, "msd_scatter");
-                msd_scatter_kernel<K, RANK, IT><<<sms * (IT >= 16 ? 2 : 4), kNtM, msd_smem, st>>>(b, large[cur], d_cnt,
-                                                                         tile_prefix, hist,
-                                                                         &ctr[kCtrMsdTile], lookback, ctx->epoch++,
-                                                                         ctx->d_status);
-                if (!a.fixed_launches) {
+                msd_scatter_kernel<K, RANK, IT><<<scatter_grid, kNtM, msd_smem, s>>>(b, lr, tile_prefix, lookback,
+                                                                                   epoch_base, ctx->d_status, more,
+                                                                                   (uint32_t)levels);
+                if (read_back) {
                     cudaError_t e = cudaEventSynchronize(ctx->ev_level);
                     if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level event");
-                    nlarge = ctx->h_small[8];
                     ls_.set_units((double)ctx->h_small[9]);
                 }
             }
             FMCS_LAUNCH_CHECK("msd level");
+            return FMCS_OK;
+        };
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (a.fixed_launches && cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusActive) {
+            // graph capture: the levels are one WHILE node whose body is one
+            // level; each level's scatter decides whether another follows
+            if ((rc = capture_while(ctx, st, [&](cudaStream_t s, cudaGraphConditionalHandle h) {
+                     return level(s, h, false);
+                 })))
+                return rc;
+        } else {
+            for (int lvl = 0; lvl < levels && nlarge > 0; ++lvl) {
+                host_lvl = lvl;
+                if ((rc = level(st, 0, !a.fixed_launches))) return rc;
+                if (!a.fixed_launches) nlarge = ctx->h_small[8];
+            }
         }
     }
     // local tiers
-    const size_t smem_b1 = sizeof(BlockSmem<K, kNtB1, kItB1>);
-    const size_t smem_b2 = sizeof(BlockSmem<K, kNtB2, kItB2>);
-    const size_t smem_c1 = sizeof(BlockSmem<K, kNtC1, kItC1>);
-    const size_t smem_c2 = sizeof(BlockSmem<K, kNtC2, kItC2>);
+    const size_t smem_b1 = std::max(sizeof(BlockSmem<K, kNtB1, kItB1>), sizeof(BucketSmem<K, kNtB1, kItB1>));
+    const size_t smem_b2 = std::max(sizeof(BlockSmem<K, kNtB2, kItB2>), sizeof(BucketSmem<K, kNtB2, kItB2>));
+    const size_t smem_c1 = std::max(sizeof(BlockSmem<K, kNtC1, kItC1>), sizeof(BucketSmem<K, kNtC1, kItC1>));
+    const size_t smem_c2 = std::max(sizeof(BlockSmem<K, kNtC2, kItC2>), sizeof(BucketSmem<K, kNtC2, kItC2>));
+    const size_t smem_c3 = std::max(sizeof(BlockSmem<K, kNtC3, kItC3>), sizeof(BucketSmem<K, kNtC3, kItC3>));
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB1, kItB1, RANK>, smem_b1))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB2, kItB2, RANK>, smem_b2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1, kItC1, RANK>, smem_c1))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC3, kItC3, RANK>, smem_c3))) return rc;
     { LaunchScope ls_(ctx, "thread_sort");
         thread_sort_kernel<K, 16><<<sms * 8, 256, 0, st>>>(b, lists.t, &ctr[kCtrLocalT]);
     }
@@ -1019,23 +1338,31 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         warp_sort_kernel<K, RANK><<<sms * 16, 256, 0, st>>>(b, lists.a, &ctr[kCtrLocalA]);
     }
     { LaunchScope ls_(ctx, "block_sort_512");
-        block_sort_kernel<K, kNtB1, kItB1, RANK><<<sms * 12, kNtB1, smem_b1, st>>>(b, lists.b1, &ctr[kCtrLocalB1]);
+        block_sort_kernel<K, kNtB1, kItB1, RANK><<<sms * (1024 / kNtB1), kNtB1, smem_b1, st>>>(b, lists.b1,
+                                                                                           &ctr[kCtrLocalB1]);
     }
     { LaunchScope ls_(ctx, "block_sort_1024");
-        block_sort_kernel<K, kNtB2, kItB2, RANK><<<sms * 8, kNtB2, smem_b2, st>>>(b, lists.b2, &ctr[kCtrLocalB2]);
+        block_sort_kernel<K, kNtB2, kItB2, RANK><<<sms * (1024 / kNtB2), kNtB2, smem_b2, st>>>(b, lists.b2,
+                                                                                           &ctr[kCtrLocalB2]);
     }
     { LaunchScope ls_(ctx, "block_sort_2048");
-        block_sort_kernel<K, kNtC1, kItC1, RANK><<<sms * 5, kNtC1, smem_c1, st>>>(b, lists.c1, &ctr[kCtrLocalC1]);
+        block_sort_kernel<K, kNtC1, kItC1, RANK><<<sms * (1024 / kNtC1), kNtC1, smem_c1, st>>>(b, lists.c1,
+                                                                                           &ctr[kCtrLocalC1]);
     }
     { LaunchScope ls_(ctx, "block_sort_4096");
-        block_sort_kernel<K, kNtC2, kItC2, RANK><<<sms * 3, kNtC2, smem_c2, st>>>(b, lists.c2, &ctr[kCtrLocalC2]);
+        block_sort_kernel<K, kNtC2, kItC2, RANK><<<sms * (1024 / kNtC2), kNtC2, smem_c2, st>>>(b, lists.c2,
+                                                                                           &ctr[kCtrLocalC2]);
+    }
+    { LaunchScope ls_(ctx, "block_sort_8192");
+        block_sort_kernel<K, kNtC3, kItC3, RANK><<<sms * (1024 / kNtC3), kNtC3, smem_c3, st>>>(b, lists.c3,
+                                                                                           &ctr[kCtrLocalC3]);
     }
     { LaunchScope ls_(ctx, "copy");
         copy_kernel<K><<<sms * 4, 256, 0, st>>>(b, lists.copy, &ctr[kCtrCopy]);
     }
     { LaunchScope ls_(ctx, "tile_prefix");
         tile_prefix_kernel<<<1, 1024, 0, st>>>(lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix, &ctr[kCtrCopyTile],
-                                               &ctr[kCtrCopyTile], &ctr[kCtrCopyTile], kCopySplit);
+                                               kCopySplit);
     }
     { LaunchScope ls_(ctx, "copy_tiles");
         copy_tiles_kernel<K><<<sms * 8, 256, 0, st>>>(b, lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix);
@@ -1114,6 +1441,8 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
     if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK, IT>, msd_smem))) return rc;
     const int sms = ctx->num_sms;
     Lists none{};
+    // one segment [0, n), re-set before every pass; level buffers of set 0
+    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0};
     int pass = 0;
     for (uint32_t lo = 0; lo < bits; lo += kRadixBits, ++pass) {
         const uint32_t shift = std::min(bits, lo + kRadixBits);
@@ -1121,21 +1450,17 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
             lsd_set_pass_kernel<<<1, 256, 0, st>>>(seg, hist, &ctr[kCtrLarge0], (uint32_t)n, shift, pass == 0);
         }
         { LaunchScope ls_(ctx, "tile_prefix");
-            tile_prefix_kernel<<<1, 1024, 0, st>>>(seg, &ctr[kCtrLarge0], tile_prefix, &ctr[kCtrLarge0 + 1],
-                                                   &ctr[kCtrMsdTile], &ctr[kCtrMoved], tile_rows);
+            level_prefix_kernel<<<1, 1024, 0, st>>>(lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_hist");
-            msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, seg, &ctr[kCtrLarge0], tile_prefix, hist, tile_rows);
+            msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_plan");
-            msd_plan_kernel<<<1, kRadix, 0, st>>>(seg, &ctr[kCtrLarge0], hist, ctr, kCtrLarge0 + 1, seg + 1, none,
-                                                  hist + kRadix, false);
+            msd_plan_kernel<<<1, kRadix, 0, st>>>(lr, none, false);
         }
         { LaunchScope ls_(ctx, "msd_scatter");
-            msd_scatter_kernel<K, RANK, IT><<<sms * (IT >= 16 ? 2 : 4), kNtM, msd_smem, st>>>(b, seg, &ctr[kCtrLarge0],
-                                                                                           tile_prefix, hist,
-                                                                       &ctr[kCtrMsdTile], lookback, ctx->epoch++,
-                                                                       ctx->d_status);
+            msd_scatter_kernel<K, RANK, IT><<<sms * (IT >= 16 ? 2 : 4), kNtM, msd_smem, st>>>(
+                b, lr, tile_prefix, lookback, ctx->epoch++, ctx->d_status, 0, 1u);
         }
         FMCS_LAUNCH_CHECK("lsd pass");
     }

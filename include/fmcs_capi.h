@@ -79,7 +79,7 @@ FMCS_API unsigned long long fmcs_launch_count(const fmcs_ctx *ctx);
  * starts from the autotuner's file (tuning/b200.json next to the library, or
  * the file FMCS_TUNING names), else the built-in defaults.  Keys:
  *   "rank_mode"  0: match.any multi-split ranking, 1: ballot multi-split;
- *   "local_max"  128..4096: segments with more rows take the HBM radix levels;
+ *   "local_max"  128..8192: segments with more rows take the HBM radix levels;
  *   "msd_items"  8 or 16: items per thread of an HBM radix tile.
  * fmcs_get_tuning returns -1 for an unknown key. */
 FMCS_API int fmcs_set_tuning(fmcs_ctx *ctx, const char *key, long long value);
@@ -198,7 +198,8 @@ FMCS_API int fmcs_graph_create(fmcs_ctx *ctx, const void *const *cols, const uin
                                fmcs_graph **graph);
 FMCS_API int fmcs_graph_launch(fmcs_graph *graph, uint32_t *ngroups);
 FMCS_API void *fmcs_graph_stream(fmcs_graph *graph);
-/* Kernel launches one replay performs (kernel nodes of the graph). */
+/* Kernel nodes of the graph, each loop body (the radix levels of a sort round,
+ * a conditional WHILE node that runs as many times as the data needs) counted once. */
 FMCS_API int fmcs_graph_kernels(fmcs_graph *graph);
 FMCS_API void fmcs_graph_destroy(fmcs_graph *graph);
 

@@ -39,3 +39,37 @@ def test_graph_replays_match_oracle(ctx, kind, split):
             assert np.array_equal(group.cpu().numpy().view(np.uint32), gr)
     finally:
         g.close()
+
+
+def test_graph_level_loop_follows_the_data(ctx):
+    """The radix levels of a captured plan run as a loop on the device: a
+    replay on data that needs more levels than the captured run (constant
+    and low-cardinality keys keep whole-array segments large level after
+    level) or fewer (all keys distinct) still matches the oracle."""
+    torch = pytest.importorskip("torch")
+    n = 1 << 20
+    widths, split = [20, 30], [50]
+    datasets = [
+        W.cols_uniform(n, widths, seed_index=310)[0],                       # captured on this
+        [np.zeros(n, np.uint32), np.zeros(n, np.uint32)],                   # every level skips
+        W.cols_uniform(n, widths, seed_index=311, distinct=[3, 5])[0],      # few distinct keys
+        W.cols_uniform(n, widths, seed_index=312)[0],
+        [np.full(n, 7, np.uint32), np.arange(n, dtype=np.uint32)[::-1].copy()],  # reverse order
+    ]
+    dcols = [_dev(torch, c) for c in datasets[0]]
+    order = torch.zeros(n, dtype=torch.int32, device="cuda")
+    group = torch.zeros(n, dtype=torch.int32, device="cuda")
+    g = ctx.plan_graph(dcols, widths, split, order, group)
+    try:
+        assert g.kernels() > 0
+        for cols in datasets:
+            for d, c in zip(dcols, cols):
+                d.copy_(_dev(torch, c))
+            torch.cuda.synchronize()
+            ng = g.launch()
+            o, gr, ng_ref = O.run_plan_sort(cols, widths, split)
+            assert ng == ng_ref
+            assert np.array_equal(order.cpu().numpy().view(np.uint32), o)
+            assert np.array_equal(group.cpu().numpy().view(np.uint32), gr)
+    finally:
+        g.close()

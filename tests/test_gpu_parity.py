@@ -242,7 +242,7 @@ def test_sort_round_plain(ctx, segmented, dtype, bits):
 
 
 @pytest.mark.parametrize("knobs", [dict(rank_mode=1), dict(local_max=1024), dict(local_max=2048, msd_items=16),
-                                   dict(msd_items=16, rank_mode=1)])
+                                   dict(msd_items=16, rank_mode=1), dict(local_max=8192)])
 def test_tuning_knobs_same_results(knobs):
     from fastmulticolsort_b200 import capi
     cols, bw = W.cols_zipf(400000, seed_index=77)
@@ -257,4 +257,48 @@ def test_tuning_knobs_same_results(knobs):
             o, g, n_ref = O.run_plan_sort(cols, bw, split)
             assert ng == n_ref and np.array_equal(order, o) and np.array_equal(group, g)
         with pytest.raises(capi.FmcsError):
-            c.set_tuning("local_max", 5000)
+            c.set_tuning("local_max", 9000)
+
+
+@pytest.mark.parametrize("local_max", [4096, 8192])
+@pytest.mark.parametrize("dtype,bits", [(np.uint32, 32), (np.uint64, 64)])
+def test_sort_round_block_tier_key_shapes(dtype, bits, local_max):
+    """Segments of every block tier (129..8192 rows) whose keys are distinct,
+    repeated up to exactly 64 and 65 times (the largest bucket the rank-by-
+    counting path takes, and one more), constant, differing only in the top
+    or only in the lowest bit, and in reverse order: the stable order of the
+    oracle in every case."""
+    rng = np.random.default_rng(bits)
+    segs = []
+    for length in (129, 512, 513, 1024, 1025, 2048, 2049, 4096, 4097, 8192):
+        top = (1 << (bits - 1))
+        shapes = [
+            rng.integers(0, (1 << bits) - 1, size=length, dtype=np.uint64, endpoint=True),
+            np.repeat(rng.integers(0, 1 << 20, size=length // 64 + 1, dtype=np.uint64), 64)[:length],
+            np.repeat(rng.integers(0, 1 << 20, size=length // 65 + 1, dtype=np.uint64), 65)[:length],
+            np.full(length, 12345, np.uint64),
+            (rng.integers(0, 2, size=length, dtype=np.uint64) * top) | 5,
+            rng.integers(0, 2, size=length, dtype=np.uint64) | (top - 2),
+            np.arange(length, dtype=np.uint64)[::-1] * 977,
+        ]
+        for sh in shapes:
+            segs.append(rng.permutation(sh).astype(dtype))
+    by_position = np.concatenate(segs)
+    n = by_position.shape[0]
+    sizes = [s.shape[0] for s in segs]
+    in_group = np.repeat(np.arange(len(sizes), dtype=np.uint32), sizes)
+    order_in = rng.permutation(n).astype(np.uint32)
+    bank = np.empty_like(by_position)
+    bank[order_in] = by_position          # position i of the round holds by_position[i]
+    order = order_in.copy()
+    group = np.zeros(n, np.uint32)
+    keys = np.zeros(n, dtype)
+    from fastmulticolsort_b200 import capi
+    with capi.Context(0) as c:
+        c.set_tuning("local_max", local_max)
+        ng = c.sort_round(bank, bits, order, in_group=in_group, out_group=group, sorted_bank=keys)
+    o_ref, g_ref, k_ref, ng_ref = O.sort_round(bank, order=order_in, in_group=in_group)
+    assert np.array_equal(order, o_ref)
+    assert np.array_equal(group, g_ref)
+    assert np.array_equal(keys, k_ref)
+    assert ng == ng_ref
