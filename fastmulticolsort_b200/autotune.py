@@ -131,7 +131,7 @@ def calibrate(ctx, quick: bool) -> dict:
         msd.append(lvl_ms / (rows / 1e6))
         # on-chip sorts of groups of 2^k rows
         row = [0.0]
-        for k in range(1, 13):
+        for k in range(1, 14):
             size = 1 << k
             ig = torch.arange(n, dtype=torch.int32, device="cuda") // size
             oo = torch.arange(n, dtype=torch.int32, device="cuda")

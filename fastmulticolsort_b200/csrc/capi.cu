@@ -89,7 +89,8 @@ int counters(fmcs_ctx *ctx, uint32_t **w)
 int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_t key_bits, uint32_t *order,
                    const uint32_t *in_group, const uint32_t *seg_start, const uint32_t *d_nseg,
                    uint32_t *out_group, void *keys_out, uint32_t *next_seg_start, uint32_t *d_next_nseg,
-                   uint64_t n, uint32_t *d_ngroups, bool identity_order = false, bool fixed_launches = false)
+                   uint64_t n, uint32_t *d_ngroups, bool identity_order = false, bool fixed_launches = false,
+                   const uint32_t *top_hist = nullptr)
 {
     int rc;
     void *p;
@@ -118,6 +119,7 @@ int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_
     a.keys_out = keys_out;
     a.n = n;
     a.fixed_launches = fixed_launches;
+    a.top_hist = in_group ? nullptr : top_hist;
     if ((rc = sort_segments(ctx, a))) return rc;
     if (out_group || next_seg_start)
         return launch_group_ids_segments(ctx, keys_out, bank_bytes, in_group, out_group, next_seg_start, n,
@@ -165,13 +167,20 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
             const SliceRec &r = bp.slices[k];
             sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
         }
-        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n))) return rc;
+        // round 0 of a sort plan over more rows than one block sorts: the
+        // stitch also counts the first radix level's histogram
+        uint32_t *top_hist = nullptr;
+        if (!hash && !in_group && n > ctx->local_max) {
+            if ((rc = ws_get(ctx, kSlotTopHist, 256 * sizeof(uint32_t), &p))) return rc;
+            top_hist = (uint32_t *)p;
+        }
+        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits))) return rc;
         uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
         if (!hash) {
             // (b)+(d): sort, then group ids (+ the next round's segments)
             uint32_t *ns = last ? nullptr : segs[b & 1];
             if ((rc = sort_round_dev(ctx, bank, bp.bytes, bp.bits, dorder, in_group, seg_in, d_nseg_in, og, nullptr,
-                                     ns, d_nseg[b & 1], n, d_ng, false, fixed)))
+                                     ns, d_nseg[b & 1], n, d_ng, false, fixed, top_hist)))
                 return rc;
             seg_in = ns;
             d_nseg_in = d_nseg[b & 1];

@@ -47,6 +47,7 @@ enum Slot : int {
     kSlotGroupA,      // run_plan group ping
     kSlotGroupB,      // run_plan group pong
     kSlotColStage,    // run_plan host column staging (several columns)
+    kSlotTopHist,     // level-0 digit histogram of a round-0 bank, counted by the stitch
     kSlotMisc,
     kSlotCount
 };
@@ -131,8 +132,11 @@ struct StitchSlice {
     uint32_t width;    // end - start + 1
 };
 constexpr int kMaxSlices = 32;
+// With top_hist (device, 256 words), the stitch also counts the top digit
+// (bits [key_bits - min(8, key_bits), key_bits)) of every bank value: the
+// first radix level's histogram of a round-0 sort of the bank.
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n);
+                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0);
 
 // bank[i] <<= lshift (src == NULL) or bank[i] |= (src[i] >> rshift) & mask(width)
 int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,
@@ -155,6 +159,7 @@ struct SortArgs {
     void *keys_out;            // device, n keys, or NULL
     uint64_t n;
     bool fixed_launches = false;  // launch every level (no host read-back), e.g. under graph capture
+    const uint32_t *top_hist = nullptr;  // round 0 only: the first level's digit histogram, already counted
 };
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
 // Stable full-array LSD radix sort of (keys, vals) in place by key bits

@@ -88,10 +88,16 @@ bool GpuCostTables::Load(const std::string &path)
     if (json_numbers(txt, "gather", v) && v.size() == 3) std::copy(v.begin(), v.end(), t.gather);
     if (json_numbers(txt, "boundary", v) && v.size() == 3) std::copy(v.begin(), v.end(), t.boundary);
     if (json_numbers(txt, "msd_level", v) && v.size() == 3) std::copy(v.begin(), v.end(), t.msd_level);
-    if (json_numbers(txt, "local", v) && v.size() == 39)
+    if (json_numbers(txt, "local", v) && v.size() % 3 == 0 && v.size() >= 3) {
+        // rows of per-size costs (sizes 2^0 ..); missing larger sizes keep the
+        // last measured per-row cost
+        const int per = (int)(v.size() / 3);
         for (int b = 0; b < 3; ++b)
-            for (int k = 0; k < 13; ++k) t.local[b][k] = v[b * 13 + k];
+            for (int k = 0; k < kLocalSizes; ++k) t.local[b][k] = v[b * per + std::min(k, per - 1)];
+    }
     if (json_numbers(txt, "round_fixed_ms", v) && v.size() == 1) t.round_fixed_ms = v[0];
+    if (json_numbers(txt, "local_max", v) && v.size() == 1 && v[0] >= 128 && v[0] <= 8192)
+        t.local_max = (uint32_t)v[0];
     *this = t;
     return true;
 }
@@ -119,7 +125,7 @@ double GpuCostTables::SortGroupMs(double g, uint32_t bank_bytes, uint32_t key_bi
         per_mrow += msd_level[b];
     }
     int k = (int)std::ceil(std::log2(std::max(1.0, std::min(rest, (double)local_max))));
-    k = std::max(0, std::min(12, k));
+    k = std::max(0, std::min(kLocalSizes - 1, k));
     per_mrow += local[b][k];
     return per_mrow * g / 1e6;
 }

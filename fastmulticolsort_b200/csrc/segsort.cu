@@ -90,6 +90,7 @@ struct LevelRefs {
     uint32_t *hist[2];
     uint32_t *ctr;
     int dev_level;
+    int hist0_ready;   // level 0's histogram was counted before the sort (by the stitch)
 };
 
 // Index of the level whose launches are running (level_prefix_kernel has
@@ -201,8 +202,18 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
 template <typename K>
 __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_start, const uint32_t *d_nseg,
                                 uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, Lists lists,
-                                uint32_t *hist0)
+                                uint32_t *hist0, const uint32_t *top_hist)
 {
+    if (!seg_start && top_hist && n > lists.local_max) {
+        // round 0 over the whole array with its first-level histogram already
+        // counted: the one large segment, histogram row 0 = top_hist
+        if (threadIdx.x == 0) {
+            ctr[kCtrLarge0] = 1;
+            large0[0] = LargeSeg{0, (uint32_t)n, key_bits, kSrcExt};
+        }
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist0[d] = top_hist[d];
+        return;
+    }
     const uint32_t nseg = seg_start ? *d_nseg : 1u;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
         const uint32_t start = seg_start ? seg_start[s] : 0u;
@@ -310,7 +321,9 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, 
     constexpr int NW = kNtM / 32;
     constexpr int MAXJ = 16;   // tile_rows <= 16 * kNtM
     __shared__ uint32_t sh[NW][kRadix];
-    const uint32_t cur = running_level(r) & 1u;
+    const uint32_t lvl = running_level(r);
+    if (lvl == 0 && r.hist0_ready) return;
+    const uint32_t cur = lvl & 1u;
     const LargeSeg *segs = (cur ? r.large[1] : r.large[0]);
     uint32_t *hist = (cur ? r.hist[1] : r.hist[0]);
     const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
@@ -1242,7 +1255,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         if (seg_start && a.nseg_host == 0) grid = (unsigned)sms * 16;
         { LaunchScope ls_(ctx, "classify");
             classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists,
-                                                     hists[0]);
+                                                     hists[0], seg_start ? nullptr : a.top_hist);
         }
         FMCS_LAUNCH_CHECK("classify");
     }
@@ -1262,7 +1275,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level count");
             nlarge = ctx->h_small[8];
         }
-        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1};
+        const int hist0_ready = (a.top_hist && !a.seg_start) ? 1 : 0;
+        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready};
         const uint32_t epoch_base = ctx->epoch;
         ctx->epoch += (uint32_t)levels;
         const unsigned scatter_grid = sms * (IT >= 16 ? 2 : 4);
@@ -1273,7 +1287,9 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             { LaunchScope ls_(ctx, "tile_prefix");
                 level_prefix_kernel<<<1, 1024, 0, s>>>(lr, tile_prefix, tile_rows);
             }
-            { LaunchScope ls_(ctx, "msd_hist");
+            if (!(hist0_ready && host_lvl == 0 && read_back)) {
+                // (inside a graph the launch stays and returns at once on level 0)
+                LaunchScope ls_(ctx, "msd_hist");
                 msd_hist_kernel<K><<<sms * 8, kNtM, 0, s>>>(b, lr, tile_prefix, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
@@ -1442,7 +1458,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
     const int sms = ctx->num_sms;
     Lists none{};
     // one segment [0, n), re-set before every pass; level buffers of set 0
-    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0};
+    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0, 0};
     int pass = 0;
     for (uint32_t lo = 0; lo < bits; lo += kRadixBits, ++pass) {
         const uint32_t shift = std::min(bits, lo + kRadixBits);

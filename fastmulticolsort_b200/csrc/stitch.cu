@@ -92,8 +92,14 @@ __device__ __forceinline__ void store4(B *bank, uint64_t row, bool vec, uint64_t
 
 template <typename B>
 __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ StitchParams p, B *bank,
-                                                     uint64_t n, bool aligned)
+                                                     uint64_t n, bool aligned, uint32_t *top_hist,
+                                                     uint32_t hist_lo, uint32_t hist_mask)
 {
+    __shared__ uint32_t sh[256];
+    if (top_hist) {
+        for (int d = threadIdx.x; d < 256; d += blockDim.x) sh[d] = 0;
+        __syncthreads();
+    }
     const uint64_t groups = (n + 3) / 4;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
          g += (uint64_t)gridDim.x * blockDim.x) {
@@ -112,6 +118,16 @@ __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ Sti
             }
         }
         store4<B>(bank, row, vec, n, acc);
+        if (top_hist) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (row + k < n) atomicAdd(&sh[(uint32_t)(acc[k] >> hist_lo) & hist_mask], 1u);
+        }
+    }
+    if (top_hist) {
+        __syncthreads();
+        for (int d = threadIdx.x; d < 256; d += blockDim.x)
+            if (sh[d]) atomicAdd(&top_hist[d], sh[d]);
     }
 }
 
@@ -157,9 +173,11 @@ int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t 
 }
 
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n)
+                  uint64_t n, uint32_t *top_hist, uint32_t key_bits)
 {
     if (ns < 1 || ns > kMaxSlices) return set_error(ctx, FMCS_E_INVAL, "stitch: 1..32 slices");
+    if (!(bank_bytes == 1 || bank_bytes == 2 || bank_bytes == 4 || bank_bytes == 8))
+        return set_error(ctx, FMCS_E_INVAL, "stitch: bank_bytes must be 1, 2, 4 or 8");
     if (n == 0) return FMCS_OK;
     StitchParams p;
     bool aligned = ((uintptr_t)bank % 16) == 0;
@@ -172,19 +190,29 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
     uint64_t blocks = (groups + 255) / 256;
     const uint64_t cap = (uint64_t)ctx->num_sms * 8;
     if (blocks > cap) blocks = cap;
+    uint32_t hist_lo = 0, hist_mask = 0;
+    if (top_hist) {
+        const uint32_t width = key_bits < 8u ? key_bits : 8u;
+        hist_lo = key_bits - width;
+        hist_mask = (1u << width) - 1u;
+        cudaMemsetAsync(top_hist, 0, 256 * sizeof(uint32_t), ctx->stream);
+    }
+    const unsigned grid = (unsigned)blocks;
+    cudaStream_t st = ctx->stream;
+    LaunchScope ls_(ctx, "stitch");
     switch (bank_bytes) {
-    case 1: { LaunchScope ls_(ctx, "stitch");
-        stitch_kernel<uint8_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint8_t *)bank, n, aligned);
-    } break;
-    case 2: { LaunchScope ls_(ctx, "stitch");
-        stitch_kernel<uint16_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint16_t *)bank, n, aligned);
-    } break;
-    case 4: { LaunchScope ls_(ctx, "stitch");
-        stitch_kernel<uint32_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint32_t *)bank, n, aligned);
-    } break;
-    case 8: { LaunchScope ls_(ctx, "stitch");
-        stitch_kernel<uint64_t><<<(unsigned)blocks, 256, 0, ctx->stream>>>(p, (uint64_t *)bank, n, aligned);
-    } break;
+    case 1:
+        stitch_kernel<uint8_t><<<grid, 256, 0, st>>>(p, (uint8_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        break;
+    case 2:
+        stitch_kernel<uint16_t><<<grid, 256, 0, st>>>(p, (uint16_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        break;
+    case 4:
+        stitch_kernel<uint32_t><<<grid, 256, 0, st>>>(p, (uint32_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        break;
+    case 8:
+        stitch_kernel<uint64_t><<<grid, 256, 0, st>>>(p, (uint64_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        break;
     default: return set_error(ctx, FMCS_E_INVAL, "stitch: bank_bytes must be 1, 2, 4 or 8");
     }
     cudaError_t e = cudaGetLastError();

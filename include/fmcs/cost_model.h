@@ -9,8 +9,8 @@
 // the round's AVERAGE group size, which comes from per-column cardinalities --
 // but every table is in milliseconds per million rows measured on the GPU, per
 // bank width (2, 4, 8 bytes), and the sort cost follows the GPU engine: a
-// group of g rows is sorted on chip if g <= 4096 (cost by log2 g), else after
-// ceil(log256(g / 4096)) HBM radix levels.  The autotuner
+// group of g rows is sorted on chip if g <= local_max (8192 unless tuned;
+// cost by log2 g), else after ceil(log256(g / local_max)) HBM radix levels.  The autotuner
 // (fastmulticolsort_b200/autotune.py) re-measures the tables and writes them
 // as JSON; GpuCostTables::Load reads them back.
 #pragma once
@@ -29,13 +29,14 @@ struct FMCS_CXX_API GpuCostTables {
     double gather[3] = {0.0035, 0.0040, 0.0055};
     double boundary[3] = {0.0030, 0.0040, 0.0060};
     double msd_level[3] = {0.010, 0.013, 0.018};   // one HBM radix level over the rows of large groups
-    // on-chip sort of groups of ~2^k rows, k = 0..12
-    double local[3][13] = {
-        {0.0, 0.004, 0.004, 0.004, 0.005, 0.006, 0.007, 0.008, 0.009, 0.011, 0.013, 0.015, 0.018},
-        {0.0, 0.004, 0.004, 0.005, 0.006, 0.007, 0.008, 0.010, 0.011, 0.013, 0.015, 0.018, 0.021},
-        {0.0, 0.005, 0.005, 0.006, 0.007, 0.008, 0.010, 0.012, 0.014, 0.016, 0.019, 0.023, 0.028}};
+    // on-chip sort of groups of ~2^k rows, k = 0..13
+    static constexpr int kLocalSizes = 14;
+    double local[3][kLocalSizes] = {
+        {0.0, 0.004, 0.004, 0.004, 0.005, 0.006, 0.007, 0.008, 0.009, 0.011, 0.013, 0.015, 0.018, 0.020},
+        {0.0, 0.004, 0.004, 0.005, 0.006, 0.007, 0.008, 0.010, 0.011, 0.013, 0.015, 0.018, 0.021, 0.024},
+        {0.0, 0.005, 0.005, 0.006, 0.007, 0.008, 0.010, 0.012, 0.014, 0.016, 0.019, 0.023, 0.028, 0.032}};
     double round_fixed_ms = 0.03;   // per-round launch and synchronization overhead
-    uint32_t local_max = 4096;      // largest group sorted on chip
+    uint32_t local_max = 8192;      // largest group sorted on chip (the engine's knob)
 
     static int BankIndex(uint32_t bank_bytes) { return bank_bytes <= 2 ? 0 : (bank_bytes <= 4 ? 1 : 2); }
     /** Read a table written by the autotuner (JSON); false if absent/invalid. */
