@@ -560,6 +560,47 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
 constexpr uint32_t kCountRankMax = 64;
 constexpr uint32_t kBucketMax = 64;
 
+// A segment's rows into registers: warp-striped positions wbase + j*32 + lane
+// (j < steps, position < len); the source switch is taken once per segment.
+template <typename K, int IT>
+__device__ __forceinline__ void load_rows(const Bufs<K> &b, uint32_t src, uint32_t start, uint32_t len, uint32_t steps,
+                                          uint32_t wbase, K (&key)[IT], uint32_t (&val)[IT])
+{
+    const uint32_t lane = threadIdx.x & 31;
+    if (src == kSrcExt && b.ext_order) {
+        const uint32_t *os = b.ext_order + start;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            val[j] = (j < (int)steps && p < len) ? os[p] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            key[j] = (j < (int)steps && p < len) ? b.ext_bank[val[j]] : K(0);
+        }
+    } else if (src == kSrcExt) {
+        const K *ks = b.ext_bank + start;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            const bool ok = j < (int)steps && p < len;
+            key[j] = ok ? ks[p] : K(0);
+            val[j] = start + p;
+        }
+    } else {
+        const K *ks = (src == kSrcBuf1 ? b.k1 : b.k0) + start;
+        const uint32_t *vs = (src == kSrcBuf1 ? b.v1 : b.v0) + start;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            const bool ok = j < (int)steps && p < len;
+            key[j] = ok ? ks[p] : K(0);
+            val[j] = ok ? vs[p] : 0u;
+        }
+    }
+}
+
 template <typename K, int NT, int IT>
 struct BucketSmem {
     unsigned long long cs[NT * IT];   // compound keys, bucketed
@@ -639,11 +680,14 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
                                                  uint32_t len, const Bufs<K> &b, uint32_t start)
 {
     const int lane = threadIdx.x & 31;
+    const uint32_t nbits = 32u - (uint32_t)__clz(len - 1u);          // ceil(log2(len)), len >= 2
     if (threadIdx.x == 0) {
         sm.any = 0ull;
         sm.all = ~0ull;
         sm.maxb = 0;
     }
+    // bucket counters for any digit width up to nbits
+    for (uint32_t i = threadIdx.x; i <= (1u << nbits); i += NT) sm.off[i] = 0;
     __syncthreads();
     unsigned long long any = 0ull, all = ~0ull;
 #pragma unroll
@@ -664,6 +708,8 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
         atomicAnd(&sm.all, all);
     }
     __syncthreads();
+    K *ko = b.k0 + start;
+    uint32_t *vo = b.v0 + start;
     const unsigned long long diff = sm.any & ~sm.all;
     if (diff == 0ull) {
         // every key is the same: the segment is in order already
@@ -671,8 +717,8 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
         for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             if (j < (int)steps && p < len) {
-                b.k0[(uint64_t)start + p] = key[j];
-                b.v0[(uint64_t)start + p] = val[j];
+                ko[p] = key[j];
+                vo[p] = val[j];
             }
         }
         __syncthreads();
@@ -681,21 +727,21 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
     const uint32_t top = 64u - (uint32_t)__clzll((long long)diff);   // bits [0, top) differ somewhere
     const unsigned long long low = top >= 64u ? ~0ull : ((1ull << top) - 1ull);
     const unsigned long long prefix = sm.all & ~low;                 // the bits every row shares
-    const uint32_t nbits = 32u - (uint32_t)__clz(len - 1u);          // ceil(log2(len)), len >= 2
     const bool packed = top + nbits <= 64u;
     const uint32_t sh = packed ? nbits : 0u;
     const uint32_t lo = top > nbits ? top - nbits : 0u;
     const uint32_t width = top - lo;
     const uint32_t dshift = lo + sh;                                 // bucket = compound >> dshift
     const uint32_t nb = 1u << width;
-    for (uint32_t i = threadIdx.x; i <= nb; i += NT) sm.off[i] = 0;
-    __syncthreads();
+    unsigned long long c[IT];
     uint32_t slot[IT];
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         const uint32_t p = wbase + j * 32 + lane;
-        if (j < (int)steps && p < len)
-            slot[j] = atomicAdd(&sm.off[(uint32_t)((((unsigned long long)key[j] & low) << sh) >> dshift)], 1u);
+        if (j < (int)steps && p < len) {
+            c[j] = (((unsigned long long)key[j] & low) << sh) | (packed ? p : 0u);
+            slot[j] = atomicAdd(&sm.off[(uint32_t)(c[j] >> dshift)], 1u);
+        }
     }
     __syncthreads();
     block_scan_bins<NT>(sm.off, nb, sm.tmp, &sm.maxb);
@@ -707,9 +753,8 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
     for (int j = 0; j < IT; ++j) {
         const uint32_t p = wbase + j * 32 + lane;
         if (j < (int)steps && p < len) {
-            const unsigned long long c = ((((unsigned long long)key[j] & low) << sh)) | (packed ? p : 0u);
-            const uint32_t pos = sm.off[(uint32_t)(c >> dshift)] + slot[j];
-            sm.cs[pos] = c;
+            const uint32_t pos = sm.off[(uint32_t)(c[j] >> dshift)] + slot[j];
+            sm.cs[pos] = c[j];
             sm.vals[pos] = val[j];
             if (!packed) sm.orig[pos] = (uint16_t)p;
         }
@@ -753,8 +798,8 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
     // store into BUF0, which may alias the EXT oids of the range
     for (uint32_t p = threadIdx.x; p < len; p += NT) {
         const uint32_t q = perm[p];
-        b.k0[(uint64_t)start + p] = (K)(prefix | (sm.cs[q] >> sh));
-        b.v0[(uint64_t)start + p] = sm.vals[q];
+        ko[p] = (K)(prefix | (sm.cs[q] >> sh));
+        vo[p] = sm.vals[q];
     }
     __syncthreads();
     return true;
@@ -930,7 +975,6 @@ block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
     constexpr int NW = NT / 32;
     const uint32_t count = *d_count;
     const int warp = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
     for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
         const uint2 ent = list[e];
         const uint32_t start = ent.x;
@@ -943,13 +987,7 @@ block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
         const uint32_t wbase = warp * steps * 32;
         K key[IT];
         uint32_t val[IT];
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            key[j] = 0;
-            val[j] = 0;
-            if (j < (int)steps && p < len) load_kv(b, src, (uint64_t)start + p, key[j], val[j]);
-        }
+        load_rows<K, IT>(b, src, start, len, steps, wbase, key, val);
         if (!bucket_rank_sort<K, NT, IT>(*reinterpret_cast<BucketSmem<K, NT, IT> *>(smem_raw), key, val, steps, wbase,
                                          len, b, start)) {
             block_sort_fallback<K, NT, IT, RANK>(*reinterpret_cast<BlockSmem<K, NT, IT> *>(smem_raw), b, start, len,
