@@ -262,11 +262,17 @@ def run_reference(args):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
-def kernel_bytes_per_unit(name: str, bank_bytes: int):
-    """Algorithmic bytes per row for kernels whose launches report rows."""
-    if name == "msd_scatter":
-        return 2 * (bank_bytes + 4)
-    return None
+def profiled_traffic(kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary profiles/<kernel>_17b33_plan50.md (its line
+    'traffic_bytes_per_launch: N'), or None."""
+    import re
+    path = os.path.join(ROOT, "profiles", f"{kernel}_17b33_plan50.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        m = re.search(r"^traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read(), re.M)
+    return float(m.group(1)) if m else None
 
 
 def time_steps(ctx, stream, fn, steps):
@@ -421,18 +427,14 @@ def run_fmcs(args):
     hbm_peak, peak_kind = peaks()
     dom, dom_ms = None, 0.0
     for name, rec in prof.items():
-        if kernel_bytes_per_unit(name, 8) and rec["units"] > 0 and rec["ms"] > dom_ms:
+        if rec.get("bytes", 0) > 0 and rec["ms"] > dom_ms:
             dom, dom_ms = name, rec["ms"]
     roofline = None
     if dom:
         rec = prof[dom]
-        bytes_total = rec["units"] * kernel_bytes_per_unit(dom, 8)
+        bytes_total = rec["bytes"]   # the library's algorithmic bytes of the launches
         achieved = bytes_total / (rec["ms"] / 1e3) / 1e9
-        traffic = None
-        tp = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tp):
-            with open(tp) as f:
-                traffic = json.load(f).get(dom, {}).get("bytes_per_launch_full_size")
+        traffic = profiled_traffic(dom)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                     "traffic": traffic,

@@ -156,7 +156,7 @@ LaunchScope::LaunchScope(fmcs_ctx *ctx, const char *name) : ctx_(ctx)
 {
     ctx->launches++;
     if (!ctx->prof_on) return;
-    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx), 0.0, ctx->prof_round};
+    fmcs_prof_rec r{name, take_event(ctx), take_event(ctx), 0.0, 0.0, ctx->prof_round};
     if (!r.a || !r.b) return;
     cudaEventRecord(r.a, ctx->stream);
     rec_ = (int)ctx->prof.size();
@@ -166,6 +166,11 @@ LaunchScope::LaunchScope(fmcs_ctx *ctx, const char *name) : ctx_(ctx)
 void LaunchScope::set_units(double u)
 {
     if (rec_ >= 0) ctx_->prof[rec_].units = u;
+}
+
+void LaunchScope::set_bytes(double b)
+{
+    if (rec_ >= 0) ctx_->prof[rec_].bytes = b;
 }
 
 LaunchScope::~LaunchScope()
@@ -320,6 +325,7 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         unsigned long long n = 0;
         double ms = 0;
         double units = 0;
+        double bytes = 0;
     };
     std::vector<Agg> agg;
     std::vector<double> round_ms;
@@ -335,6 +341,7 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
         agg[k].n++;
         agg[k].ms += ms;
         agg[k].units += r.units;
+        agg[k].bytes += r.bytes;
         // per-round totals of the sort/hash work (the stitch is reported apart)
         if (r.round >= 0 && strcmp(r.name, "stitch") != 0) {
             if ((int)round_ms.size() <= r.round) round_ms.resize(r.round + 1, 0.0);
@@ -347,8 +354,8 @@ extern "C" int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len)
     std::string out = "{";
     for (size_t k = 0; k < agg.size(); ++k) {
         char tmp[256];
-        snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"units\": %.0f}",
-                 k ? ", " : "", agg[k].name.c_str(), agg[k].n, agg[k].ms, agg[k].units);
+        snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"units\": %.0f, \"bytes\": %.0f}",
+                 k ? ", " : "", agg[k].name.c_str(), agg[k].n, agg[k].ms, agg[k].units, agg[k].bytes);
         out += tmp;
     }
     if (!round_ms.empty()) {

@@ -63,6 +63,7 @@ struct fmcs_prof_rec {
     const char *name;
     cudaEvent_t a, b;
     double units;   // work items of the launch (rows), when the launcher knows them
+    double bytes;   // algorithmic HBM bytes of the launch, when the launcher knows them
     int round;      // sort/hash round of a plan the launch belongs to (-1: none)
 };
 
@@ -108,6 +109,7 @@ class LaunchScope {
     LaunchScope(fmcs_ctx *ctx, const char *name);
     ~LaunchScope();
     void set_units(double u);
+    void set_bytes(double b);
 
   private:
     fmcs_ctx *ctx_;

@@ -1348,7 +1348,14 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                 if (read_back) {
                     cudaError_t e = cudaEventSynchronize(ctx->ev_level);
                     if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level event");
-                    ls_.set_units((double)ctx->h_small[9]);
+                    // algorithmic bytes: every moved row is read from the level's
+                    // source (the round's bank, through the order when there is
+                    // one, at level 0; the work buffers after) and written once
+                    const double moved = (double)ctx->h_small[9];
+                    const double rd = host_lvl == 0 ? (double)sizeof(K) + (b.ext_order ? 4.0 : 0.0)
+                                                    : (double)sizeof(K) + 4.0;
+                    ls_.set_units(moved);
+                    ls_.set_bytes(moved * (rd + (double)sizeof(K) + 4.0));
                 }
             }
             FMCS_LAUNCH_CHECK("msd level");
