@@ -150,49 +150,70 @@ struct Lists {
 
 // Route a segment (child or initial) to its tier.  Segments that need no
 // sorting (one row, or no key bits left) only need to reach BUF0.
+// A slot in the list whose counter is ctr[which]: the active lanes of a warp
+// that go to the same list take their slots with one atomicAdd (children of
+// one segment mostly share a tier, so the counters are hot addresses).
+__device__ __forceinline__ uint32_t alloc_slot(uint32_t *ctr, int which)
+{
+    const uint32_t mask = __activemask();
+    const uint32_t peers = __match_any_sync(mask, which);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(&ctr[which], (uint32_t)__popc(peers));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(peers & lanemask_lt());
+}
+
 __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
                                               uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L,
                                               uint32_t *hist_out)
 {
-    const uint32_t local_max = L.local_max;
     if (len == 0) return;
+    int which;
     if (len == 1 || shift == 0) {
-        if (src != kSrcBuf0) {
-            if (len > kCopySplit) {
-                const uint32_t slot = atomicAdd(&ctr[kCtrCopyLarge], 1u);
-                L.copy_large[slot] = LargeSeg{start, len, 0, src};
-            } else {
-                const uint32_t slot = atomicAdd(&ctr[kCtrCopy], 1u);
-                L.copy[slot] = LargeSeg{start, len, 0, src};
-            }
-        }
-        return;
+        if (src == kSrcBuf0) return;   // already in place
+        which = len > kCopySplit ? kCtrCopyLarge : kCtrCopy;
+    } else if (len > L.local_max) {
+        which = large_ctr;
+    } else if (len <= (uint32_t)kCapT) {
+        which = kCtrLocalT;
+    } else if (len <= L.cap_t32) {
+        which = kCtrLocalT32;
+    } else if (len <= (uint32_t)kCapA) {
+        which = kCtrLocalA;
+    } else if (len <= (uint32_t)kCapB1) {
+        which = kCtrLocalB1;
+    } else if (len <= (uint32_t)kCapB2) {
+        which = kCtrLocalB2;
+    } else if (len <= (uint32_t)kCapC1) {
+        which = kCtrLocalC1;
+    } else if (len <= (uint32_t)kCapC2) {
+        which = kCtrLocalC2;
+    } else if (len <= (uint32_t)kCapC3) {
+        which = kCtrLocalC3;
+    } else {
+        which = large_ctr;
     }
+    const uint32_t slot = alloc_slot(ctr, which);
     const uint2 e = pack_local(start, len, shift, src);
-    if (len > local_max) {
+    switch (which) {
+    case kCtrCopyLarge: L.copy_large[slot] = LargeSeg{start, len, 0, src}; break;
+    case kCtrCopy: L.copy[slot] = LargeSeg{start, len, 0, src}; break;
+    case kCtrLocalT: L.t[slot] = e; break;
+    case kCtrLocalT32: L.t32[slot] = e; break;
+    case kCtrLocalA: L.a[slot] = e; break;
+    case kCtrLocalB1: L.b1[slot] = e; break;
+    case kCtrLocalB2: L.b2[slot] = e; break;
+    case kCtrLocalC1: L.c1[slot] = e; break;
+    case kCtrLocalC2: L.c2[slot] = e; break;
+    case kCtrLocalC3: L.c3[slot] = e; break;
+    default: {
         // a large segment: its digit histogram row starts at zero
-        const uint32_t slot = atomicAdd(&ctr[large_ctr], 1u);
         large_out[slot] = LargeSeg{start, len, shift, src};
         uint4 *row = reinterpret_cast<uint4 *>(hist_out + (uint64_t)slot * kRadix);
 #pragma unroll 4
         for (int i = 0; i < kRadix / 4; ++i) row[i] = make_uint4(0, 0, 0, 0);
-        return;
     }
-    if (len <= (uint32_t)kCapT) L.t[atomicAdd(&ctr[kCtrLocalT], 1u)] = e;
-    else if (len <= L.cap_t32) L.t32[atomicAdd(&ctr[kCtrLocalT32], 1u)] = e;
-    else if (len <= (uint32_t)kCapA) L.a[atomicAdd(&ctr[kCtrLocalA], 1u)] = e;
-    else if (len <= (uint32_t)kCapB1) L.b1[atomicAdd(&ctr[kCtrLocalB1], 1u)] = e;
-    else if (len <= (uint32_t)kCapB2) L.b2[atomicAdd(&ctr[kCtrLocalB2], 1u)] = e;
-    else if (len <= (uint32_t)kCapC1) L.c1[atomicAdd(&ctr[kCtrLocalC1], 1u)] = e;
-    else if (len <= (uint32_t)kCapC2) L.c2[atomicAdd(&ctr[kCtrLocalC2], 1u)] = e;
-    else if (len <= (uint32_t)kCapC3) L.c3[atomicAdd(&ctr[kCtrLocalC3], 1u)] = e;
-    else {
-        // a large segment: its digit histogram row starts at zero
-        const uint32_t slot = atomicAdd(&ctr[large_ctr], 1u);
-        large_out[slot] = LargeSeg{start, len, shift, src};
-        uint4 *row = reinterpret_cast<uint4 *>(hist_out + (uint64_t)slot * kRadix);
-#pragma unroll 4
-        for (int i = 0; i < kRadix / 4; ++i) row[i] = make_uint4(0, 0, 0, 0);
     }
 }
 

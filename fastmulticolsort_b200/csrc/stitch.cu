@@ -100,28 +100,38 @@ __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ Sti
         for (int d = threadIdx.x; d < 256; d += blockDim.x) sh[d] = 0;
         __syncthreads();
     }
+    // Each thread takes two groups of 4 rows per step (a stride apart), so
+    // that the loads of both are in flight together.
     const uint64_t groups = (n + 3) / 4;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t row = g * 4;
-        const bool vec = aligned && row + 4 <= n;
-        uint64_t acc[4] = {0, 0, 0, 0};
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups; g += 2 * stride) {
+        const bool two = g + stride < groups;
+        const uint64_t row0 = g * 4, row1 = (g + stride) * 4;
+        const bool vec0 = aligned && row0 + 4 <= n;
+        const bool vec1 = aligned && row1 + 4 <= n;
+        uint64_t acc0[4] = {0, 0, 0, 0}, acc1[4] = {0, 0, 0, 0};
         for (int s = 0; s < p.ns; ++s) {
             const StitchSlice sl = p.s[s];
-            uint64_t v[4];
-            load4(sl.src, sl.src_bytes, row, vec, n, v);
+            uint64_t v0[4], v1[4] = {0, 0, 0, 0};
+            load4(sl.src, sl.src_bytes, row0, vec0, n, v0);
+            if (two) load4(sl.src, sl.src_bytes, row1, vec1, n, v1);
             const uint64_t mask = sl.width >= 64 ? ~0ull : ((1ull << sl.width) - 1);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const uint64_t x = (v[k] >> sl.rshift) & mask;
-                acc[k] = (s == 0 || sl.width >= 64) ? x : ((acc[k] << sl.width) | x);
+                const uint64_t x0 = (v0[k] >> sl.rshift) & mask;
+                const uint64_t x1 = (v1[k] >> sl.rshift) & mask;
+                acc0[k] = (s == 0 || sl.width >= 64) ? x0 : ((acc0[k] << sl.width) | x0);
+                acc1[k] = (s == 0 || sl.width >= 64) ? x1 : ((acc1[k] << sl.width) | x1);
             }
         }
-        store4<B>(bank, row, vec, n, acc);
+        store4<B>(bank, row0, vec0, n, acc0);
+        if (two) store4<B>(bank, row1, vec1, n, acc1);
         if (top_hist) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (row + k < n) atomicAdd(&sh[(uint32_t)(acc[k] >> hist_lo) & hist_mask], 1u);
+            for (int k = 0; k < 4; ++k) {
+                if (row0 + k < n) atomicAdd(&sh[(uint32_t)(acc0[k] >> hist_lo) & hist_mask], 1u);
+                if (two && row1 + k < n) atomicAdd(&sh[(uint32_t)(acc1[k] >> hist_lo) & hist_mask], 1u);
+            }
         }
     }
     if (top_hist) {
