@@ -157,14 +157,14 @@ __device__ __forceinline__ void block_exclusive_scan_radix(uint32_t *cnt, uint32
 __device__ __forceinline__ unsigned long long lb_wait(const unsigned long long *p, uint32_t epoch,
                                                       int *status)
 {
-    uint32_t ns = 32;
+    uint32_t ns = 16;
     for (uint32_t it = 0; it < kSpinLimit; ++it) {
         unsigned long long w = ld_volatile_u64(p);
         uint32_t hi = (uint32_t)(w >> 32);
         if ((hi >> 2) == epoch && (hi & 3u) != 0) return w;
         if ((it & 255u) == 255u && *(volatile int *)status != kDevOk) break;
         __nanosleep(ns);
-        if (ns < 256) ns <<= 1;
+        if (ns < 128) ns <<= 1;
     }
     atomicCAS(status, kDevOk, kDevTimeout);
     return lb_word(epoch, kFlagInclusive, 0);

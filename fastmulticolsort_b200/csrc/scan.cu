@@ -17,7 +17,7 @@ namespace fmcs {
 
 namespace {
 
-constexpr int kScanThreads = 256;
+constexpr int kScanThreads = 512;              // a tile of 8192 positions: half as many look-back steps
 constexpr int kScanItems = 16;                  // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kScanWarps = kScanThreads / 32;
@@ -307,8 +307,8 @@ int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64
 // caller passes device inputs and outputs; no context is needed.
 //
 // The array is modest (kNoAllocTiles look-back words, 128 KiB) and every GPU
-// that loads the library holds it until the process exits.  It bounds n at
-// kNoAllocTiles * 4096 = 67,108,864 rows.  All calls share it and it keeps the
+// that loads the library holds it until the process exits.  n is bounded at
+// 67,108,864 rows (at most 8,192 scan tiles).  All calls share it and it keeps the
 // last call's contents, so each call clears the words that must start at zero;
 // calls whose work overlaps on the GPU (two streams, or two host threads)
 // race on it and must be serialized by the caller.
@@ -317,7 +317,8 @@ namespace fmcs {
 namespace {
 
 constexpr uint64_t kNoAllocTiles = 16384;
-constexpr uint64_t kNoAllocMaxRows = kNoAllocTiles * kScanTile;
+constexpr uint64_t kNoAllocMaxRows = 67108864;
+static_assert(kNoAllocMaxRows / kScanTile <= kNoAllocTiles, "look-back words for every tile");
 // layout (64-bit words): [0, kNoAllocTiles) look-back; then the tile counter,
 // the group count and the status word, one 64-bit word each
 constexpr uint64_t kNoAllocWords = kNoAllocTiles + 4;
