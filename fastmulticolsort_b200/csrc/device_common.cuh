@@ -106,6 +106,33 @@ __device__ __forceinline__ uint32_t wlms_rank(uint32_t digit, bool valid, uint32
     return base + __popc(peers & lanemask_lt());
 }
 
+// wlms_rank for a full warp of valid items with full-width (8-bit) digits.
+template <int MODE = kRankMatch>
+__device__ __forceinline__ uint32_t wlms_rank_full(uint32_t digit, uint32_t *whist)
+{
+    uint32_t peers;
+    if constexpr (MODE == kRankMatch) {
+        peers = __match_any_sync(0xFFFFFFFFu, digit);
+    } else {
+        peers = 0xFFFFFFFFu;
+#pragma unroll
+        for (uint32_t b = 0; b < (uint32_t)kRadixBits; ++b) {
+            const uint32_t bit = (digit >> b) & 1u;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+            peers &= bit ? bal : ~bal;
+        }
+    }
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) {
+        base = whist[digit];
+        whist[digit] = base + __popc(peers);
+    }
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    __syncwarp();
+    return base + __popc(peers & lanemask_lt());
+}
+
 // Exclusive scan of kRadix counters in shared memory by a block of NT threads.
 // Returns the total through *total (every thread).  `tmp` holds NT/32 words.
 template <int NT>

@@ -135,6 +135,47 @@ __device__ __forceinline__ K load_k(const Bufs<K> &b, uint32_t src, uint64_t i)
     return src == kSrcBuf1 ? b.k1[i] : b.k0[i];
 }
 
+// A segment's rows into registers: warp-striped positions wbase + j*32 + lane
+// (j < steps, position < len); the source switch is taken once per segment.
+template <typename K, int IT>
+__device__ __forceinline__ void load_rows(const Bufs<K> &b, uint32_t src, uint32_t start, uint32_t len, uint32_t steps,
+                                          uint32_t wbase, K (&key)[IT], uint32_t (&val)[IT])
+{
+    const uint32_t lane = threadIdx.x & 31;
+    if (src == kSrcExt && b.ext_order) {
+        const uint32_t *os = b.ext_order + start;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            val[j] = (j < (int)steps && p < len) ? os[p] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            key[j] = (j < (int)steps && p < len) ? b.ext_bank[val[j]] : K(0);
+        }
+    } else if (src == kSrcExt) {
+        const K *ks = b.ext_bank + start;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            const bool ok = j < (int)steps && p < len;
+            key[j] = ok ? ks[p] : K(0);
+            val[j] = start + p;
+        }
+    } else {
+        const K *ks = (src == kSrcBuf1 ? b.k1 : b.k0) + start;
+        const uint32_t *vs = (src == kSrcBuf1 ? b.v1 : b.v0) + start;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            const bool ok = j < (int)steps && p < len;
+            key[j] = ok ? ks[p] : K(0);
+            val[j] = ok ? vs[p] : 0u;
+        }
+    }
+}
+
 __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32_t shift, uint32_t src)
 {
     return make_uint2(start, len | (shift << 16) | (src << 24));
@@ -483,17 +524,21 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
         uint32_t rank[IT];
         uint32_t dig[IT];
         const uint32_t wbase = warp * (IT * 32);
+        load_rows<K, IT>(b, sg.src, (uint32_t)tbeg, cnt, IT, wbase, key, val);
+        if (cnt == kTileM && width == (uint32_t)kRadixBits) {
+            // a whole tile and a whole digit (the common case): no lane checks
 #pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            if (p < cnt) load_kv(b, sg.src, tbeg + p, key[j], val[j]);
-            else { key[j] = 0; val[j] = 0; }
-        }
+            for (int j = 0; j < IT; ++j) {
+                dig[j] = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
+                rank[j] = wlms_rank_full<RANK>(dig[j], sm.whist[warp]);
+            }
+        } else {
 #pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            dig[j] = digit_of(key[j], lo, width);
-            rank[j] = wlms_rank<RANK>(dig[j], p < cnt, sm.whist[warp], width);
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t p = wbase + j * 32 + lane;
+                dig[j] = digit_of(key[j], lo, width);
+                rank[j] = wlms_rank<RANK>(dig[j], p < cnt, sm.whist[warp], width);
+            }
         }
         __syncthreads();
         // per digit: exclusive over warps, tile total
@@ -580,47 +625,6 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
 // Every step is stable, so ties keep their input order.
 constexpr uint32_t kCountRankMax = 64;
 constexpr uint32_t kBucketMax = 64;
-
-// A segment's rows into registers: warp-striped positions wbase + j*32 + lane
-// (j < steps, position < len); the source switch is taken once per segment.
-template <typename K, int IT>
-__device__ __forceinline__ void load_rows(const Bufs<K> &b, uint32_t src, uint32_t start, uint32_t len, uint32_t steps,
-                                          uint32_t wbase, K (&key)[IT], uint32_t (&val)[IT])
-{
-    const uint32_t lane = threadIdx.x & 31;
-    if (src == kSrcExt && b.ext_order) {
-        const uint32_t *os = b.ext_order + start;
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            val[j] = (j < (int)steps && p < len) ? os[p] : 0u;
-        }
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            key[j] = (j < (int)steps && p < len) ? b.ext_bank[val[j]] : K(0);
-        }
-    } else if (src == kSrcExt) {
-        const K *ks = b.ext_bank + start;
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            const bool ok = j < (int)steps && p < len;
-            key[j] = ok ? ks[p] : K(0);
-            val[j] = start + p;
-        }
-    } else {
-        const K *ks = (src == kSrcBuf1 ? b.k1 : b.k0) + start;
-        const uint32_t *vs = (src == kSrcBuf1 ? b.v1 : b.v0) + start;
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t p = wbase + j * 32 + lane;
-            const bool ok = j < (int)steps && p < len;
-            key[j] = ok ? ks[p] : K(0);
-            val[j] = ok ? vs[p] : 0u;
-        }
-    }
-}
 
 template <typename K, int NT, int IT>
 struct BucketSmem {
