@@ -468,7 +468,7 @@ struct MsdSmem {
     uint32_t whist[kNtM / 32][kRadix];
     uint32_t total[kRadix];
     uint32_t doff[kRadix];       // tile-local exclusive digit offsets
-    long long gdst[kRadix];      // global destination base per digit
+    uint32_t gdst[kRadix];       // global destination base per digit (mod 2^32; rows < 2^32)
     uint32_t tmp[kNtM / 32 + 1];
     uint32_t tile, seg;
     K keys[kNtM * IT];
@@ -572,15 +572,18 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
                 st_volatile_u64(&lookback[(uint64_t)t * kRadix + d],
                                 lb_word(epoch, kFlagInclusive, excl + sm.total[d]));
             }
-            sm.gdst[d] = (long long)sg.start + (long long)offs[(uint64_t)s * kRadix + d] + (long long)excl -
-                         (long long)sm.doff[d];
+            const uint32_t dof = sm.doff[d];
+            sm.gdst[d] = sg.start + offs[(uint64_t)s * kRadix + d] + excl - dof;   // wraps; + slot is in range
+            // the warps' exclusive counts become tile positions
+#pragma unroll
+            for (int w = 0; w < kNtM / 32; ++w) sm.whist[w][d] += dof;
         }
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             if (p < cnt) {
-                const uint32_t pos = sm.doff[dig[j]] + sm.whist[warp][dig[j]] + rank[j];
+                const uint32_t pos = sm.whist[warp][dig[j]] + rank[j];
                 sm.keys[pos] = key[j];
                 sm.vals[pos] = val[j];
             }
@@ -590,7 +593,7 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
         uint32_t *dv = (sg.src == kSrcBuf1) ? b.v0 : b.v1;
         for (uint32_t i = threadIdx.x; i < cnt; i += kNtM) {
             const K kk = sm.keys[i];
-            const long long o = sm.gdst[digit_of(kk, lo, width)] + (long long)i;
+            const uint32_t o = sm.gdst[digit_of(kk, lo, width)] + i;
             dk[o] = kk;
             dv[o] = sm.vals[i];
         }
