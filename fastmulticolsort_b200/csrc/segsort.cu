@@ -54,6 +54,7 @@ constexpr int kNtC2 = 512, kItC2 = 8, kCapC2 = kNtC2 * kItC2;   // 4096
 constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
 constexpr int kCapLocal = kCapC3;   // largest segment a local tier can take; larger: MSD levels
 constexpr int kNtM = 256;           // MSD tile: 256 threads x IT items (IT = 8 or 16, tuned)
+constexpr int kMsdCtas16 = 3;       // resident scatter CTAs per SM with 16 rows per thread
 
 // counters slot words
 constexpr int kCtrMsdTile = 1;
@@ -463,6 +464,9 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lis
     }
 }
 
+// Resident CTAs of the scatter per SM (the launch bound and the grid).
+constexpr int msd_ctas_per_sm(int it) { return it >= 16 ? kMsdCtas16 : 4; }
+
 template <typename K, int IT>
 struct MsdSmem {
     uint32_t whist[kNtM / 32][kRadix];
@@ -476,7 +480,7 @@ struct MsdSmem {
 };
 
 template <typename K, int RANK, int IT>
-__global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(Bufs<K> b, LevelRefs r,
+__global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(Bufs<K> b, LevelRefs r,
                                                            const uint32_t *tile_prefix, unsigned long long *lookback,
                                                            uint32_t epoch_base, int *status,
                                                            cudaGraphConditionalHandle more, uint32_t levels)
@@ -521,23 +525,22 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
 
         K key[IT];
         uint32_t val[IT];
-        uint32_t rank[IT];
-        uint32_t dig[IT];
+        uint32_t rd[IT];   // rank in the warp (low 16 bits) | digit << 16
         const uint32_t wbase = warp * (IT * 32);
         load_rows<K, IT>(b, sg.src, (uint32_t)tbeg, cnt, IT, wbase, key, val);
         if (cnt == kTileM && width == (uint32_t)kRadixBits) {
             // a whole tile and a whole digit (the common case): no lane checks
 #pragma unroll
             for (int j = 0; j < IT; ++j) {
-                dig[j] = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
-                rank[j] = wlms_rank_full<RANK>(dig[j], sm.whist[warp]);
+                const uint32_t d = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
+                rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
             }
         } else {
 #pragma unroll
             for (int j = 0; j < IT; ++j) {
                 const uint32_t p = wbase + j * 32 + lane;
-                dig[j] = digit_of(key[j], lo, width);
-                rank[j] = wlms_rank<RANK>(dig[j], p < cnt, sm.whist[warp], width);
+                const uint32_t d = digit_of(key[j], lo, width);
+                rd[j] = wlms_rank<RANK>(d, p < cnt, sm.whist[warp], width) | (d << 16);
             }
         }
         __syncthreads();
@@ -583,7 +586,7 @@ __global__ void __launch_bounds__(kNtM, (IT >= 16 ? 2 : 4)) msd_scatter_kernel(B
         for (int j = 0; j < IT; ++j) {
             const uint32_t p = wbase + j * 32 + lane;
             if (p < cnt) {
-                const uint32_t pos = sm.whist[warp][dig[j]] + rank[j];
+                const uint32_t pos = sm.whist[warp][rd[j] >> 16] + (rd[j] & 0xFFFFu);
                 sm.keys[pos] = key[j];
                 sm.vals[pos] = val[j];
             }
@@ -1345,7 +1348,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready};
         const uint32_t epoch_base = ctx->epoch;
         ctx->epoch += (uint32_t)levels;
-        const unsigned scatter_grid = sms * (IT >= 16 ? 2 : 4);
+        const unsigned scatter_grid = sms * msd_ctas_per_sm(IT);
         int host_lvl = 0;   // the level being launched, for the eager read-back
         // one level: the same four launches for every level (the level index
         // lives on the device)
@@ -1548,7 +1551,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
             msd_plan_kernel<<<1, kRadix, 0, st>>>(lr, none, false);
         }
         { LaunchScope ls_(ctx, "msd_scatter");
-            msd_scatter_kernel<K, RANK, IT><<<sms * (IT >= 16 ? 2 : 4), kNtM, msd_smem, st>>>(
+            msd_scatter_kernel<K, RANK, IT><<<sms * msd_ctas_per_sm(IT), kNtM, msd_smem, st>>>(
                 b, lr, tile_prefix, lookback, ctx->epoch++, ctx->d_status, 0, 1u);
         }
         FMCS_LAUNCH_CHECK("lsd pass");
