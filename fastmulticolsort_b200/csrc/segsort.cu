@@ -643,52 +643,56 @@ struct BucketSmem {
     uint32_t maxb;
 };
 
-// Exclusive scan of off[0, nb) by the block (nb a power of two >= NT or any
-// nb <= NT), also leaving the largest count in *maxb.
+// Exclusive scan of off[0, nb) by the block, also leaving the largest count
+// in *maxb.  Warp w scans its own run of 32-bin rows (lanes read consecutive
+// bins: no bank conflicts), then the warps' totals are scanned and added.
 template <int NT>
 __device__ __forceinline__ void block_scan_bins(uint32_t *off, uint32_t nb, uint32_t *tmp, uint32_t *maxb)
 {
-    const uint32_t per = nb >= (uint32_t)NT ? nb / NT : 1u;
-    const uint32_t base = threadIdx.x * per;
-    uint32_t sum = 0, mx = 0;
-    if (base < nb) {
-        for (uint32_t i = 0; i < per; ++i) {
-            const uint32_t c = off[base + i];
-            sum += c;
-            mx = max(mx, c);
-        }
-    }
-    uint32_t incl = sum;
+    constexpr int NW = NT / 32;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rows = (nb + 31) / 32;
+    const uint32_t rpw = (rows + NW - 1) / NW;
+    const uint32_t r0 = warp * rpw, r1 = min(rows, r0 + rpw);
+    uint32_t carry = 0, mx = 0;
+    for (uint32_t r = r0; r < r1; ++r) {
+        const uint32_t i = r * 32 + lane;
+        const uint32_t v = i < nb ? off[i] : 0u;
+        uint32_t incl = v;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if ((int)lane_id() >= o) incl += y;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (i < nb) off[i] = carry + incl - v;
+        carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+        mx = max(mx, v);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-    const int w = threadIdx.x >> 5;
-    if (lane_id() == 31) tmp[w] = incl;
-    if (lane_id() == 0) atomicMax(maxb, mx);
+    if (lane == 0) {
+        tmp[warp] = carry;
+        atomicMax(maxb, mx);
+    }
     __syncthreads();
-    if (threadIdx.x < 32) {
-        const uint32_t v = threadIdx.x < NT / 32 ? tmp[threadIdx.x] : 0u;
-        uint32_t vi = v;
+    if (warp == 0) {
+        const uint32_t v = lane < NW ? tmp[lane] : 0u;
+        uint32_t incl = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, vi, o);
-            if ((int)threadIdx.x >= o) vi += y;
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
         }
-        if (threadIdx.x < NT / 32) tmp[threadIdx.x] = vi - v;
+        if (lane < NW) tmp[lane] = incl - v;
     }
     __syncthreads();
-    uint32_t run = tmp[w] + incl - sum;
-    if (base < nb) {
-        for (uint32_t i = 0; i < per; ++i) {
-            const uint32_t c = off[base + i];
-            off[base + i] = run;
-            run += c;
+    const uint32_t add = tmp[warp];
+    if (add)
+        for (uint32_t r = r0; r < r1; ++r) {
+            const uint32_t i = r * 32 + lane;
+            if (i < nb) off[i] += add;
         }
-    }
     __syncthreads();
 }
 
