@@ -206,6 +206,9 @@ __device__ __forceinline__ uint32_t alloc_slot(uint32_t *ctr, int which)
     return base + __popc(peers & lanemask_lt());
 }
 
+// A large segment gets its next-level histogram row zeroed here when
+// hist_out is given (the round's initial segments); the children of a radix
+// level get theirs zeroed by that level's scatter grid, coalesced.
 __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
                                               uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L,
                                               uint32_t *hist_out)
@@ -250,11 +253,12 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
     case kCtrLocalC2: L.c2[slot] = e; break;
     case kCtrLocalC3: L.c3[slot] = e; break;
     default: {
-        // a large segment: its digit histogram row starts at zero
         large_out[slot] = LargeSeg{start, len, shift, src};
-        uint4 *row = reinterpret_cast<uint4 *>(hist_out + (uint64_t)slot * kRadix);
+        if (hist_out) {
+            uint4 *row = reinterpret_cast<uint4 *>(hist_out + (uint64_t)slot * kRadix);
 #pragma unroll 4
-        for (int i = 0; i < kRadix / 4; ++i) row[i] = make_uint4(0, 0, 0, 0);
+            for (int i = 0; i < kRadix / 4; ++i) row[i] = make_uint4(0, 0, 0, 0);
+        }
     }
     }
 }
@@ -437,7 +441,6 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lis
     uint32_t *ctr = r.ctr;
     const int next_large_ctr = kCtrLarge0 + (int)nxt;
     LargeSeg *large_next = (nxt ? r.large[1] : r.large[0]);
-    uint32_t *hist_next = (nxt ? r.hist[1] : r.hist[0]);
     const uint32_t nseg = ctr[kCtrLarge0 + cur];
     for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
         const LargeSeg sg = segs[s];
@@ -457,7 +460,7 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lis
         const uint32_t child_src = skip ? sg.src : (sg.src == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
         if (emit_children && c > 0)
             route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, lists,
-                          hist_next);
+                          nullptr);   // the next level's histogram rows are zeroed by the scatter grid
         if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
         if (d == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
         __syncthreads();
@@ -497,8 +500,19 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
     const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
     // Inside a graph, the level loop goes on while the next level has large
     // segments (msd_plan has counted them before this launch).
+    const uint32_t nnext = r.ctr[kCtrLarge0 + (cur ^ 1u)];
     if (more && blockIdx.x == 0 && threadIdx.x == 0)
-        cudaGraphSetConditional(more, (r.ctr[kCtrLarge0 + (cur ^ 1u)] > 0 && lvl + 1 < levels) ? 1u : 0u);
+        cudaGraphSetConditional(more, (nnext > 0 && lvl + 1 < levels) ? 1u : 0u);
+    {
+        // the histogram rows of the next level's large segments start at zero
+        // (this level's plan has placed them; the rows held this level's
+        // predecessor's offsets, which nothing reads any more)
+        uint4 *h = reinterpret_cast<uint4 *>(cur ? r.hist[0] : r.hist[1]);
+        const uint64_t words = (uint64_t)nnext * (kRadix / 4);
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < words;
+             i += (uint64_t)gridDim.x * blockDim.x)
+            h[i] = make_uint4(0, 0, 0, 0);
+    }
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
     const int warp = threadIdx.x >> 5;
