@@ -496,6 +496,20 @@ def run_serving(args):
     return 0
 
 
+def run_batch_workloads(args):
+    """Many independent instances and the wide table: one JSON line of their own."""
+    from fastmulticolsort_b200 import batch_bench
+    res = batch_bench.benchmark(reps=max(1, min(args.steps, 5)))
+    inst = res["instances"]
+    line = {"metric": METRIC, "workload": "batch", "value": inst["batched_mrows_s"], "unit": "M rows/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded; generated on the device)",
+            "config": {"workload": f"{inst['instances']} instances, {inst['rows']:,} rows in all (8/24/40-bit "
+                                   "columns), one fmcs_run_batch call; plus a 60M-row 6-column wide table"},
+            **res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -506,7 +520,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-zipf", action="store_true", help="skip the Zipf segmented comparison")
     ap.add_argument("--zipf-rows", type=int, default=67_108_864)
-    ap.add_argument("--workload", default="massaged", choices=["massaged", "serving"])
+    ap.add_argument("--workload", default="massaged", choices=["massaged", "serving", "batch"])
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--duration", type=float, default=5.0)
     ap.add_argument("--only-steps", action="store_true",
@@ -519,6 +533,8 @@ def main():
         return run_reference(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "batch":
+        return run_batch_workloads(args)
     return run_fmcs(args)
 
 

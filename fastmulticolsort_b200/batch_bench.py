@@ -1,0 +1,183 @@
+"""Many-instances and wide-table workloads (seeded, generated on the device).
+
+Instances: 4,096 independent sort instances with n_i = floor(2^U(10, 20)) rows
+(mean about 151k, about 619M rows in all), three columns of 8 / 24 / 40 bits
+(u16 / u32 / u64 storage); col0 draws from 16 distinct values in [0, 2^8),
+col1 and col2 are uniform.  Compared:
+  batched      ONE fmcs_run_batch call for all instances (the cost model's plan);
+  per_instance the same plan, one fmcs_run_plan call per instance;
+  plain        one full LSD sort per original column per instance
+               (fmcs_sort_round_plain, no massaging, no size binning).
+
+Wide: N = 60,000,000 rows, six columns of 2 / 1 / 12 / 12 / 32 / 7 bits with
+3 / 2 / 2,526 / 2,526 / uniform 32-bit / 100 distinct values (66 bits: at least
+two banks).  ORDER BY runs the cost model's ordered plan; GROUP BY runs its
+column order and plan through the hash-grouping rounds; plain sorts column by
+column.  The reference's TPC-H-derived inputs are not available here; these
+seeded shapes stand in for them.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import capi
+from . import workloads as W
+
+INSTANCE_COUNT = 4096
+WIDE_ROWS = 60_000_000
+WIDE_BITS = [2, 1, 12, 12, 32, 7]
+WIDE_CARD = [3, 2, 2526, 2526, 1 << 32, 100]
+
+
+def _store_dtype(torch, w):
+    return torch.int16 if w <= 16 else (torch.int32 if w <= 32 else torch.int64)
+
+
+def _gen(torch, rng):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(int(rng.integers(1 << 62)))
+    return g
+
+
+def _pool_column(torch, rng, n, w, count):
+    """n codes drawn uniformly from `count` distinct w-bit values, stored in the
+    reference's width (u16 / u32 / u64 as int16 / int32 / int64 bits)."""
+    pool = W.distinct_pool(rng, count, w).astype(np.int64)
+    idx = torch.randint(0, count, (n,), device="cuda", generator=_gen(torch, rng))
+    v = torch.from_numpy(pool).cuda()[idx]
+    return _narrow(torch, v, w)
+
+
+def _uniform_column(torch, rng, n, w):
+    g = _gen(torch, rng)
+    if w >= 63:
+        v = torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64, device="cuda", generator=g)
+    else:
+        v = torch.randint(0, 1 << w, (n,), dtype=torch.int64, device="cuda", generator=g)
+    return _narrow(torch, v, w)
+
+
+def _narrow(torch, v, w):
+    if w > 32:
+        return v.contiguous()
+    bits = 16 if w <= 16 else 32
+    v = torch.where(v >= (1 << (bits - 1)), v - (1 << bits), v)
+    return v.to(_store_dtype(torch, w)).contiguous()
+
+
+def _time_ms(torch, stream, fn, reps):
+    """Mean ms of fn() over reps, CUDA events on the context's stream."""
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def instances(torch, ctx, stream, reps=3, plain=True):
+    rng = W.rng_for(4)
+    sizes = np.floor(2.0 ** rng.uniform(10, 20, size=INSTANCE_COUNT)).astype(np.int64)
+    total = int(sizes.sum())
+    bw = [8, 24, 40]
+    cols = [_pool_column(torch, rng, total, 8, 16), _uniform_column(torch, rng, total, 24),
+            _uniform_column(torch, rng, total, 40)]
+    col_bytes = [c.element_size() for c in cols]
+    mean_n = int(sizes.mean())
+    split, _, est = capi.optimize_plan(bw, [16, min(mean_n, 1 << 24), mean_n], col_bytes, mean_n)
+    order = torch.empty(total, dtype=torch.int32, device="cuda")
+    group = torch.empty(total, dtype=torch.int32, device="cuda")
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+
+    def batched():
+        ctx.run_batch(cols, bw, split, sizes, order, group)
+
+    def per_instance():
+        for i in range(INSTANCE_COUNT):
+            a, b = int(offs[i]), int(offs[i + 1])
+            ctx.run_plan([c[a:b] for c in cols], bw, split, order[a:b], group[a:b])
+
+    g2 = torch.empty_like(group)
+
+    def plain_path():
+        for i in range(INSTANCE_COUNT):
+            a, b = int(offs[i]), int(offs[i + 1])
+            o, g, h = order[a:b], group[a:b], g2[a:b]
+            ctx.sort_round_plain(cols[0][a:b], 8, o, out_group=g)
+            ctx.sort_round_plain(cols[1][a:b], 24, o, in_group=g, out_group=h)
+            ctx.sort_round_plain(cols[2][a:b], 40, o, in_group=h, out_group=g)
+
+    out = {"instances": INSTANCE_COUNT, "rows": total, "rows_min": int(sizes.min()), "rows_max": int(sizes.max()),
+           "rows_mean": round(float(sizes.mean()), 1), "columns": "8-bit (16 distinct values, u16), 24-bit (u32), "
+           "40-bit (u64)", "plan": split, "plan_est_ms": round(est, 3),
+           "column_bytes": int(total * sum(col_bytes))}
+    batched()
+    out["batched_ms"] = round(_time_ms(torch, stream, batched, reps), 3)
+    per_instance()
+    out["per_instance_ms"] = round(_time_ms(torch, stream, per_instance, 1), 3)
+    if plain:
+        plain_path()
+        out["plain_ms"] = round(_time_ms(torch, stream, plain_path, 1), 3)
+    for k in ("batched", "per_instance", "plain"):
+        if f"{k}_ms" in out:
+            out[f"{k}_mrows_s"] = round(total / (out[f"{k}_ms"] / 1e3) / 1e6, 1)
+    out["speedup_batched_vs_per_instance"] = round(out["per_instance_ms"] / out["batched_ms"], 2)
+    if plain:
+        out["speedup_batched_vs_plain"] = round(out["plain_ms"] / out["batched_ms"], 2)
+    del cols, order, group, g2
+    torch.cuda.empty_cache()
+    return out
+
+
+def wide(torch, ctx, stream, reps=3):
+    rng = W.rng_for(4, salt=1)
+    n = WIDE_ROWS
+    cols = []
+    for w, k in zip(WIDE_BITS, WIDE_CARD):
+        cols.append(_uniform_column(torch, rng, n, w) if k >= (1 << w) else _pool_column(torch, rng, n, w, k))
+    col_bytes = [c.element_size() for c in cols]
+    card = [min(k, n) for k in WIDE_CARD]
+    split, _, est_o = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=True)
+    gsplit, gorder, est_g = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=False)
+    order = torch.empty(n, dtype=torch.int32, device="cuda")
+    group = torch.empty(n, dtype=torch.int32, device="cuda")
+    g2 = torch.empty_like(group)
+
+    def order_by():
+        ctx.run_plan(cols, WIDE_BITS, split, order, group)
+
+    def group_by():
+        ctx.run_plan(cols, WIDE_BITS, gsplit, order, group, col_order=gorder, hash=True)
+
+    def plain_path():
+        ig, og = None, group
+        for c, w in zip(cols, WIDE_BITS):
+            ctx.sort_round_plain(c, w, order, in_group=ig, out_group=og)
+            ig, og = og, (g2 if og is group else group)
+
+    out = {"rows": n, "bits": WIDE_BITS, "distinct": WIDE_CARD, "order_by_plan": split,
+           "group_by_plan": gsplit, "group_by_column_order": gorder}
+    for name, fn in (("order_by", order_by), ("group_by", group_by), ("plain", plain_path)):
+        fn()
+        ms = _time_ms(torch, stream, fn, reps)
+        out[f"{name}_ms"] = round(ms, 3)
+        out[f"{name}_mrows_s"] = round(n / (ms / 1e3) / 1e6, 1)
+    out["speedup_order_by_vs_plain"] = round(out["plain_ms"] / out["order_by_ms"], 2)
+    del cols, order, group, g2
+    torch.cuda.empty_cache()
+    return out
+
+
+def benchmark(reps=3, plain=True):
+    import torch
+    with capi.Context(0) as ctx:
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        inst = instances(torch, ctx, stream, reps=reps, plain=plain)
+        wd = wide(torch, ctx, stream, reps=reps)
+    return {"instances": inst, "wide": wd}

@@ -11,10 +11,10 @@
 // B200 design.  First-appearance numbering is order-dependent, so it is made
 // deterministic without a serial walk:
 //   1. one open-addressing table keyed by (parent run, key) over the whole
-//      round; each row claims or finds its slot with a CAS on the slot's
-//      representative row and records the slot, and every row atomicMin's its
-//      position into the slot: the slot's minimum is the key's first
-//      appearance f(i) inside its run;
+//      round, one 64-bit word per slot (a fingerprint of the key and the
+//      smallest row seen); each row claims or finds its slot and records it,
+//      and lowers the slot's row to its own position: the slot's final row is
+//      the key's first appearance f(i) inside its run;
 //   2. first[i] = (f(i) == i); a one-pass flag scan ranks the first
 //      appearances; id(i) = rank(f(i)).  Runs are in position order, so the
 //      ranks continue across runs exactly like startGrpIdx;
@@ -29,8 +29,6 @@
 namespace fmcs {
 
 namespace {
-
-constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 
 __device__ __forceinline__ uint64_t mix64(uint64_t x)
 {
@@ -48,28 +46,54 @@ __device__ __forceinline__ K key_at(const K *bank, const uint32_t *order, uint64
     return order ? bank[order[i]] : bank[i];
 }
 
+// Table slot: (32-bit fingerprint of (run, key)) << 32 | smallest row seen;
+// all ones = empty.  A row claims an empty slot with one CAS (it is then the
+// smallest row so far); a row whose fingerprint matches checks the key of the
+// slot's row (the only extra read, skipped for keys whose fingerprints differ)
+// and lowers the row part with a 64-bit atomicMin (equal fingerprints: only the
+// row part can change).  The slot's final row part is the key's first
+// appearance inside its run.
+constexpr unsigned long long kEmptySlot = ~0ull;
+
+// slot_of of a row alone in its parent run: it is its own first appearance
+// and takes no slot.
+constexpr uint32_t kAlone = 0xFFFFFFFFu;
+
 template <typename K>
 __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ bank, const uint32_t *__restrict__ order,
-                                                          const uint32_t *__restrict__ run, uint64_t n,
-                                                          uint32_t *rep, uint32_t *minpos, uint64_t mask,
+                                                          const uint32_t *__restrict__ run, bool runs_contiguous,
+                                                          uint64_t n, unsigned long long *slots, uint64_t mask,
                                                           uint32_t *slot_of, int *status)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const K k = key_at(bank, order, i);
         const uint32_t r = run ? run[i] : 0u;
-        uint64_t h = mix64((uint64_t)k ^ ((uint64_t)r * 0x9E3779B97F4A7C15ull)) & mask;
+        if (runs_contiguous && (i == 0 || run[i - 1] != r) && (i + 1 == n || run[i + 1] != r)) {
+            slot_of[i] = kAlone;
+            continue;
+        }
+        const K k = key_at(bank, order, i);
+        const uint64_t mixed = mix64((uint64_t)k ^ ((uint64_t)r * 0x9E3779B97F4A7C15ull));
+        uint64_t h = mixed & mask;
+        const uint32_t fp = (uint32_t)(mixed >> 32);
+        const unsigned long long mine = ((unsigned long long)fp << 32) | (uint32_t)i;   // never kEmptySlot: i < 2^32 - 1
         uint64_t probes = 0;
         for (;;) {
-            uint32_t cur = rep[h];
-            if (cur == kEmpty) {
-                const uint32_t prev = atomicCAS(&rep[h], kEmpty, (uint32_t)i);
-                cur = (prev == kEmpty) ? (uint32_t)i : prev;
+            unsigned long long cur = *(volatile unsigned long long *)&slots[h];
+            if (cur == kEmptySlot) {
+                const unsigned long long prev = atomicCAS(&slots[h], kEmptySlot, mine);
+                if (prev == kEmptySlot) {
+                    slot_of[i] = (uint32_t)h;
+                    break;
+                }
+                cur = prev;
             }
-            if (cur == (uint32_t)i ||
-                (key_at(bank, order, cur) == k && (run ? run[cur] : 0u) == r)) {
-                atomicMin(&minpos[h], (uint32_t)i);
-                slot_of[i] = (uint32_t)h;
-                break;
+            if ((uint32_t)(cur >> 32) == fp) {
+                const uint32_t rr = (uint32_t)cur;   // a row of this slot's (run, key)
+                if (key_at(bank, order, rr) == k && (run ? run[rr] : 0u) == r) {
+                    atomicMin(&slots[h], mine);
+                    slot_of[i] = (uint32_t)h;
+                    break;
+                }
             }
             h = (h + 1) & mask;
             if (++probes > mask) {   // table full: cannot happen with >= 2n slots
@@ -81,11 +105,12 @@ __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ 
     }
 }
 
-__global__ void first_flag_kernel(const uint32_t *__restrict__ slot_of, const uint32_t *__restrict__ minpos,
+__global__ void first_flag_kernel(const uint32_t *__restrict__ slot_of, const unsigned long long *__restrict__ slots,
                                   uint8_t *__restrict__ first, uint32_t *__restrict__ fpos, uint64_t n)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t f = minpos[slot_of[i]];
+        const uint32_t so = slot_of[i];
+        const uint32_t f = so == kAlone ? (uint32_t)i : (uint32_t)slots[so];
         fpos[i] = f;
         first[i] = (f == (uint32_t)i) ? 1 : 0;
     }
@@ -105,12 +130,13 @@ __global__ void assign_ids_kernel(const uint32_t *__restrict__ fpos, const uint3
 }
 
 template <typename K>
-int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const uint32_t *run, uint64_t n,
-                uint32_t *rep, uint32_t *minpos, uint64_t mask, uint32_t *slot_of)
+int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const uint32_t *run, bool runs_contiguous,
+                uint64_t n, unsigned long long *slots, uint64_t mask, uint32_t *slot_of)
 {
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     { LaunchScope ls_(ctx, "hash_insert");
-        hash_insert_kernel<K><<<grid, 256, 0, ctx->stream>>>((const K *)bank, order, run, n, rep, minpos, mask, slot_of,
+        hash_insert_kernel<K><<<grid, 256, 0, ctx->stream>>>((const K *)bank, order, run, runs_contiguous, n, slots, mask,
+                                                            slot_of,
                                                             ctx->d_status);
     }
     cudaError_t e = cudaGetLastError();
@@ -129,10 +155,10 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     void *p;
     uint64_t cap = 1024;
     while (cap < 2 * n) cap <<= 1;
-    // table: rep[cap], minpos[cap]
-    if ((rc = ws_get(ctx, kSlotHashTable, cap * 2 * sizeof(uint32_t), &p))) return rc;
-    uint32_t *rep = (uint32_t *)p, *minpos = rep + cap;
-    cudaMemsetAsync(rep, 0xFF, cap * 2 * sizeof(uint32_t), st);
+    // table: cap 64-bit slots, all empty
+    if ((rc = ws_get(ctx, kSlotHashTable, cap * sizeof(unsigned long long), &p))) return rc;
+    unsigned long long *slots = (unsigned long long *)p;
+    cudaMemsetAsync(slots, 0xFF, cap * sizeof(unsigned long long), st);
     // per-row scratch: slot_of / rank (n), fpos (n), run ids (n), first flags (n bytes)
     if ((rc = ws_get(ctx, kSlotHashIdx, n * 3 * sizeof(uint32_t) + n + 64, &p))) return rc;
     uint32_t *slot_of = (uint32_t *)p;
@@ -146,23 +172,25 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     // boundary scan of in_group, or -- when the previous ids are not clustered
     // (group_is_key) -- the previous id itself, over one numbering in row order.
     const uint32_t *keyrun = nullptr;
+    bool contiguous = false;   // runs are position ranges (not the previous ids of unclustered rows)
     if (in_group && group_is_key) {
         keyrun = in_group;
     } else if (in_group) {
         if ((rc = launch_group_ids(ctx, nullptr, 0, in_group, run, n, nullptr))) return rc;
         keyrun = run;
+        contiguous = true;
     }
     switch (bank_bytes) {
-    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
-    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
-    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
-    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, n, rep, minpos, cap - 1, slot_of); break;
+    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
+    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
+    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
+    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
     default: return set_error(ctx, FMCS_E_INVAL, "hash round: bank_bytes must be 1, 2, 4 or 8");
     }
     if (rc) return rc;
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     { LaunchScope ls_(ctx, "first_flag");
-        first_flag_kernel<<<grid, 256, 0, st>>>(slot_of, minpos, first, fpos, n);
+        first_flag_kernel<<<grid, 256, 0, st>>>(slot_of, slots, first, fpos, n);
     }
     uint32_t *rank = slot_of;   // slot_of is dead after the flags
     if ((rc = launch_flag_rank(ctx, first, rank, n, d_ngroups))) return rc;
