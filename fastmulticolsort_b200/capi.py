@@ -28,11 +28,12 @@ FMCS_E_CUDA = -4
 EXPORTS = (
     "fmcs_create", "fmcs_destroy", "fmcs_last_error", "fmcs_synchronize", "fmcs_stream",
     "fmcs_workspace_bytes", "fmcs_stitch", "fmcs_gather", "fmcs_sort_round", "fmcs_hash_round",
-    "fmcs_run_plan", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
+    "fmcs_run_plan", "fmcs_run_plan_desc", "fmcs_profile", "fmcs_profile_report", "fmcs_launch_count",
     "fmcs_group_ids_noalloc", "fmcs_shift_left", "fmcs_assemble", "fmcs_hash_round_unordered",
     "fmcs_sort_round_plain", "fmcs_optimize_plan", "fmcs_set_tuning", "fmcs_get_tuning", "fmcs_run_batch",
     "fmcs_server_create", "fmcs_server_submit", "fmcs_server_wait", "fmcs_server_load", "fmcs_server_destroy",
     "fmcs_graph_create", "fmcs_graph_launch", "fmcs_graph_stream", "fmcs_graph_destroy", "fmcs_graph_kernels",
+    "fmcs_storage_bytes", "fmcs_text_header", "fmcs_read_columns_text", "fmcs_write_columns_text",
 )
 
 
@@ -92,6 +93,13 @@ def load(path: str = LIB_PATH):
     L.fmcs_hash_round.argtypes = [vp, vp, u32, vp, vp, vp, u64, i32, u32p]
     L.fmcs_run_plan.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32p, u32, u64, i32,
                                 vp, vp, u32p]
+    L.fmcs_storage_bytes.argtypes = [u32]
+    L.fmcs_storage_bytes.restype = u32
+    L.fmcs_text_header.argtypes = [C.c_char_p, C.POINTER(u64), C.POINTER(u32)]
+    L.fmcs_read_columns_text.argtypes = [C.c_char_p, i32, u32, u32p, u64, C.POINTER(vp), C.POINTER(u64)]
+    L.fmcs_write_columns_text.argtypes = [C.c_char_p, i32, u32, u64, C.POINTER(vp), u32p]
+    L.fmcs_run_plan_desc.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, C.POINTER(C.c_uint8), u32p, u32,
+                                     u64, i32, vp, vp, u32p]
     L.fmcs_profile.argtypes = [vp, i32]
     L.fmcs_profile_report.argtypes = [vp, C.c_char_p, C.c_size_t]
     L.fmcs_launch_count.argtypes = [vp]
@@ -164,6 +172,52 @@ def group_ids_noalloc(keys, out_group, in_group=None, stream: int = 0) -> int:
     if rc != FMCS_OK:
         raise FmcsError(rc, "fmcs_group_ids_noalloc failed")
     return ng.value
+
+
+def storage_bytes(bw: int) -> int:
+    """Bytes per value of a column of declared width bw (the reference's
+    width -> type mapping: <= 16 bits u16, <= 32 u32, else u64)."""
+    return int(load().fmcs_storage_bytes(int(bw)))
+
+
+def text_header(path: str):
+    """(row count, column count) of a dataset file with the TPC-H header."""
+    n, c = C.c_uint64(0), C.c_uint32(0)
+    rc = load().fmcs_text_header(str(path).encode(), C.byref(n), C.byref(c))
+    if rc != FMCS_OK:
+        raise FmcsError(rc, f"fmcs_text_header failed on {path}")
+    return n.value, c.value
+
+
+def read_columns_text(path: str, bw, nrows: int = None, header: bool = False, cardinality: bool = True):
+    """The reference's text dataset (column after column; header = the TPC-H
+    variant, whose row count is used when nrows is None).  Returns the columns
+    as numpy arrays in their storage widths and, with cardinality, each
+    column's number of distinct values."""
+    if nrows is None:
+        if not header:
+            raise ValueError("nrows is required for a file without a header")
+        nrows, _ = text_header(path)
+    dts = {2: np.uint16, 4: np.uint32, 8: np.uint64}
+    cols = [np.empty(nrows, dts[storage_bytes(w)]) for w in bw]
+    ptrs = (C.c_void_p * len(cols))(*[c.ctypes.data for c in cols])
+    card = (C.c_uint64 * len(cols))()
+    rc = load().fmcs_read_columns_text(str(path).encode(), 1 if header else 0, len(cols), _u32arr(bw), nrows, ptrs,
+                                       card if cardinality else None)
+    if rc != FMCS_OK:
+        raise FmcsError(rc, f"fmcs_read_columns_text failed on {path}")
+    return cols, ([int(x) for x in card] if cardinality else None)
+
+
+def write_columns_text(path: str, cols, header: bool = False):
+    """Writes numpy columns (2, 4 or 8 bytes per value) in the same format."""
+    cols = [np.ascontiguousarray(c) for c in cols]
+    nrows = cols[0].shape[0]
+    ptrs = (C.c_void_p * len(cols))(*[c.ctypes.data for c in cols])
+    rc = load().fmcs_write_columns_text(str(path).encode(), 1 if header else 0, len(cols), nrows, ptrs,
+                                        _u32arr([c.dtype.itemsize for c in cols]))
+    if rc != FMCS_OK:
+        raise FmcsError(rc, f"fmcs_write_columns_text failed on {path}")
 
 
 def optimize_plan(bw, cardinality, col_bytes, n: int, ordered: bool = True):
@@ -329,15 +383,23 @@ class Context:
 
     # -- whole plan ---------------------------------------------------------
     def run_plan(self, cols, bw, split, order_out, group_out=None, col_order=None,
-                 hash: bool = False) -> int:
+                 hash: bool = False, descending=None) -> int:
+        """descending[c] true sorts column c in descending order (fmcs_run_plan_desc)."""
         n = _len(cols[0])
         ptrs = (C.c_void_p * len(cols))(*[_addr(c) for c in cols])
         ng = C.c_uint32(0)
         co = None if col_order is None else _u32arr(col_order)
-        self._check(self._L.fmcs_run_plan(self._h, ptrs, _u32arr([_itemsize(c) for c in cols]),
-                                          _u32arr(bw), len(cols), co, _u32arr(split), len(split), n,
-                                          1 if hash else 0, _addr(order_out), _addr(group_out),
-                                          C.byref(ng)))
+        if descending is None:
+            self._check(self._L.fmcs_run_plan(self._h, ptrs, _u32arr([_itemsize(c) for c in cols]),
+                                              _u32arr(bw), len(cols), co, _u32arr(split), len(split), n,
+                                              1 if hash else 0, _addr(order_out), _addr(group_out),
+                                              C.byref(ng)))
+        else:
+            desc = (C.c_uint8 * len(cols))(*[1 if d else 0 for d in descending])
+            self._check(self._L.fmcs_run_plan_desc(self._h, ptrs, _u32arr([_itemsize(c) for c in cols]),
+                                                   _u32arr(bw), len(cols), co, desc, _u32arr(split), len(split),
+                                                   n, 1 if hash else 0, _addr(order_out), _addr(group_out),
+                                                   C.byref(ng)))
         return ng.value
 
 

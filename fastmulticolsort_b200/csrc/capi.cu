@@ -133,7 +133,7 @@ int sort_round_dev(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, uint32_
 // CUDA graph captures.  *d_ng_out receives the device word of the group count.
 int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, const uint32_t *col_bytes,
                   const uint32_t *bw, uint64_t n, bool hash, uint32_t *dorder, uint32_t *dgroup_out, bool fixed,
-                  uint32_t **d_ng_out)
+                  uint32_t **d_ng_out, const uint8_t *descending = nullptr)
 {
     int rc;
     void *p;
@@ -165,7 +165,8 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
         std::vector<StitchSlice> sl(bp.slices.size());
         for (size_t k = 0; k < bp.slices.size(); ++k) {
             const SliceRec &r = bp.slices[k];
-            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
+            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1,
+                                descending && descending[r.col] ? 1u : 0u};
         }
         // round 0 of a sort plan over more rows than one block sorts: the
         // stitch also counts the first radix level's histogram
@@ -239,7 +240,7 @@ extern "C" int fmcs_stitch(fmcs_ctx *ctx, const fmcs_slice *slices, uint32_t nsl
             src = stage;
             stage += ((n * s.src_bytes + 255) & ~uint64_t(255));
         }
-        sl[i] = StitchSlice{src, s.src_bytes, s.src_bits - s.end, s.end - s.start + 1};
+        sl[i] = StitchSlice{src, s.src_bytes, s.src_bits - s.end, s.end - s.start + 1, 0u};
     }
     void *dbank;
     bool host_out;
@@ -492,9 +493,10 @@ extern "C" int fmcs_hash_round_unordered(fmcs_ctx *ctx, const void *bank, uint32
     return finish(ctx, "fmcs_hash_round_unordered", ngroups, d_ng);
 }
 
-extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
-                             uint32_t ncols, const uint32_t *col_order, const uint32_t *split, uint32_t nbanks,
-                             uint64_t n, int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
+namespace {
+int run_plan_impl(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
+                  uint32_t ncols, const uint32_t *col_order, const uint8_t *descending, const uint32_t *split,
+                  uint32_t nbanks, uint64_t n, int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
 {
     if (!ctx) return FMCS_E_INVAL;
     cudaSetDevice(ctx->device);
@@ -545,12 +547,30 @@ extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint3
     if ((rc = stage_out(ctx, group_out, n * 4, kSlotStageOut1, &dgroup_out, &h_group))) return rc;
     uint32_t *d_ng = nullptr;
     if ((rc = plan_pipeline(ctx, plan, dcols.data(), col_bytes, bw, n, hash != 0, (uint32_t *)dorder,
-                            (uint32_t *)dgroup_out, false, &d_ng)))
+                            (uint32_t *)dgroup_out, false, &d_ng, descending)))
         return rc;
     ctx->prof_round = -1;
     if (h_order && (rc = copy_out(ctx, order_out, dorder, n * 4))) return rc;
     if (h_group && (rc = copy_out(ctx, group_out, dgroup_out, n * 4))) return rc;
     return finish(ctx, "fmcs_run_plan", ngroups, d_ng);
+}
+}  // namespace
+
+extern "C" int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
+                             uint32_t ncols, const uint32_t *col_order, const uint32_t *split, uint32_t nbanks,
+                             uint64_t n, int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
+{
+    return run_plan_impl(ctx, cols, col_bytes, bw, ncols, col_order, nullptr, split, nbanks, n, hash, order_out,
+                         group_out, ngroups);
+}
+
+extern "C" int fmcs_run_plan_desc(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes,
+                                  const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
+                                  const uint8_t *descending, const uint32_t *split, uint32_t nbanks, uint64_t n,
+                                  int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
+{
+    return run_plan_impl(ctx, cols, col_bytes, bw, ncols, col_order, descending, split, nbanks, n, hash, order_out,
+                         group_out, ngroups);
 }
 
 // ---------------------------------------------------------------------------
@@ -702,7 +722,7 @@ extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint
         std::vector<StitchSlice> sl(bp.slices.size());
         for (size_t k = 0; k < bp.slices.size(); ++k) {
             const SliceRec &r = bp.slices[k];
-            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1};
+            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1, 0u};
         }
         if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n))) return rc;
         uint32_t *og = (last && dgroup_out) ? (uint32_t *)dgroup_out : g[b & 1];

@@ -132,6 +132,7 @@ struct StitchSlice {
     uint32_t src_bytes;
     uint32_t rshift;   // src_bits - end
     uint32_t width;    // end - start + 1
+    uint32_t invert;   // 1: the slice's bits are inverted (its column sorts descending)
 };
 constexpr int kMaxSlices = 32;
 // With top_hist (device, 256 words), the stitch also counts the top digit

@@ -116,10 +116,11 @@ __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ Sti
             load4(sl.src, sl.src_bytes, row0, vec0, n, v0);
             if (two) load4(sl.src, sl.src_bytes, row1, vec1, n, v1);
             const uint64_t mask = sl.width >= 64 ? ~0ull : ((1ull << sl.width) - 1);
+            const uint64_t flip = sl.invert ? mask : 0ull;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const uint64_t x0 = (v0[k] >> sl.rshift) & mask;
-                const uint64_t x1 = (v1[k] >> sl.rshift) & mask;
+                const uint64_t x0 = ((v0[k] >> sl.rshift) & mask) ^ flip;
+                const uint64_t x1 = ((v1[k] >> sl.rshift) & mask) ^ flip;
                 acc0[k] = (s == 0 || sl.width >= 64) ? x0 : ((acc0[k] << sl.width) | x0);
                 acc1[k] = (s == 0 || sl.width >= 64) ? x1 : ((acc1[k] << sl.width) | x1);
             }

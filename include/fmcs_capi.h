@@ -182,6 +182,42 @@ FMCS_API int fmcs_run_plan(fmcs_ctx *ctx, const void *const *cols, const uint32_
                   const uint32_t *split, uint32_t nbanks, uint64_t n, int hash,
                   uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 
+/* fmcs_run_plan with a sort direction per column: descending[c] != 0 sorts
+ * column c in descending order (NULL: all ascending).  The reference parses a
+ * per-column direction (compose_params_t::column_asc_desc, --asc-desc in
+ * src/main_tworound_exhaustive.cpp:347-376) but sorts every column
+ * ascending; here the stitch inverts the column's bits inside its declared
+ * width, so a descending column orders by (2^bw - 1 - value) and ties still
+ * keep their input order.  With hash != 0 the groups are the same as with
+ * every column ascending. */
+FMCS_API int fmcs_run_plan_desc(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes,
+                                const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
+                                const uint8_t *descending, const uint32_t *split, uint32_t nbanks, uint64_t n,
+                                int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
+
+/* The reference's text datasets, on the host (DataGenerator::ReadFromFile,
+ * ReadFromFile_tpch, ReadValues and GenAndSaveAsFile, src/generator.h:43-227):
+ * unsigned decimal values separated by white space, all rows of column 0,
+ * then of column 1, ...; the TPC-H variant starts with the row count and the
+ * column count.  Columns are stored in the width their bit width maps to
+ * (src/generator.h:88-94): fmcs_storage_bytes(bw) = 2 (bw <= 16), 4 (<= 32)
+ * or 8.  No GPU is involved.  Return FMCS_E_INVAL for a missing file,
+ * malformed text, a value too large for its column's storage, or a TPC-H
+ * header whose row count differs from nrows. */
+FMCS_API uint32_t fmcs_storage_bytes(uint32_t bw);
+/* Row and column counts of a TPC-H-variant file. */
+FMCS_API int fmcs_text_header(const char *path, uint64_t *nrows, uint32_t *ncols);
+/* Reads nrows values of each of ncols columns into caller-allocated host
+ * arrays cols_out[c] (fmcs_storage_bytes(bw[c]) bytes per value); with
+ * cardinality_out, also each column's number of distinct values (the
+ * reference's Column::GetCardinality). */
+FMCS_API int fmcs_read_columns_text(const char *path, int has_header, uint32_t ncols, const uint32_t *bw,
+                                    uint64_t nrows, void *const *cols_out, uint64_t *cardinality_out);
+/* Writes columns (host, 2/4/8 bytes per value) in the same format, one value
+ * per line, with the TPC-H header when with_header. */
+FMCS_API int fmcs_write_columns_text(const char *path, int with_header, uint32_t ncols, uint64_t nrows,
+                                     const void *const *cols, const uint32_t *col_bytes);
+
 /* A whole sort plan captured once as a CUDA graph and replayed (no reference
  * counterpart).  The graph is bound to the DEVICE buffers given here (columns,
  * order_out, group_out): refill the columns between launches and replay.
