@@ -34,6 +34,7 @@ EXPORTS = (
     "fmcs_server_create", "fmcs_server_submit", "fmcs_server_wait", "fmcs_server_load", "fmcs_server_destroy",
     "fmcs_graph_create", "fmcs_graph_launch", "fmcs_graph_stream", "fmcs_graph_destroy", "fmcs_graph_kernels",
     "fmcs_storage_bytes", "fmcs_text_header", "fmcs_read_columns_text", "fmcs_write_columns_text",
+    "fmcs_group_aggregate",
 )
 
 
@@ -93,6 +94,7 @@ def load(path: str = LIB_PATH):
     L.fmcs_hash_round.argtypes = [vp, vp, u32, vp, vp, vp, u64, i32, u32p]
     L.fmcs_run_plan.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32p, u32, u64, i32,
                                 vp, vp, u32p]
+    L.fmcs_group_aggregate.argtypes = [vp, vp, u32, i32, vp, vp, u64, u32, vp, vp, vp, vp]
     L.fmcs_storage_bytes.argtypes = [u32]
     L.fmcs_storage_bytes.restype = u32
     L.fmcs_text_header.argtypes = [C.c_char_p, C.POINTER(u64), C.POINTER(u32)]
@@ -380,6 +382,15 @@ class Context:
                                            len(cols), _u32arr(split), len(split), inst, k, off, _addr(order_out),
                                            _addr(group_out), counts.ctypes.data_as(C.POINTER(C.c_uint32))))
         return counts
+
+    def group_aggregate(self, payload, order, group, ngroups: int, count=None, sum=None, min=None, max=None,
+                        signed: bool = False):
+        """fmcs_group_aggregate: per-group count / sum / min / max (int64 device
+        tensors of ngroups entries, any may be None) of payload[order[i]] over
+        the sorted positions i of each group."""
+        self._check(self._L.fmcs_group_aggregate(self._h, _addr(payload), _itemsize(payload), 1 if signed else 0,
+                                                 _addr(order), _addr(group), _len(order), int(ngroups), _addr(count),
+                                                 _addr(sum), _addr(min), _addr(max)))
 
     # -- whole plan ---------------------------------------------------------
     def run_plan(self, cols, bw, split, order_out, group_out=None, col_order=None,

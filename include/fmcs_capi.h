@@ -195,6 +195,20 @@ FMCS_API int fmcs_run_plan_desc(fmcs_ctx *ctx, const void *const *cols, const ui
                                 const uint8_t *descending, const uint32_t *split, uint32_t nbanks, uint64_t n,
                                 int hash, uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 
+/* Per-group aggregates of a payload column: the consumer of (order, group)
+ * that GROUP BY queries run next (the reference returns (order, group) only,
+ * Composer::getGroupInfo, src/composer.h:59-68).  For every sorted position i
+ * the payload value of row order[i] joins group group[i] (< ngroups); outputs
+ * of ngroups entries each, any may be NULL: count, sum (64-bit, wrapping; the
+ * signed sum for signed payloads when it does not overflow), min and max
+ * (sign-extended when is_signed).  payload: n values of 4 or 8 bytes in row
+ * order.  All arrays device memory.  Groups need not be runs of positions (a
+ * hash plan's last round is accepted too).  A group id >= ngroups or an order
+ * entry >= n is reported as FMCS_E_INVAL, with nothing read or written there. */
+FMCS_API int fmcs_group_aggregate(fmcs_ctx *ctx, const void *payload, uint32_t payload_bytes, int is_signed,
+                                  const uint32_t *order, const uint32_t *group, uint64_t n, uint32_t ngroups,
+                                  uint64_t *count, uint64_t *sum, uint64_t *min, uint64_t *max);
+
 /* The reference's text datasets, on the host (DataGenerator::ReadFromFile,
  * ReadFromFile_tpch, ReadValues and GenAndSaveAsFile, src/generator.h:43-227):
  * unsigned decimal values separated by white space, all rows of column 0,
