@@ -404,6 +404,23 @@ def run_fmcs(args):
     plain_total, _ = time_steps(ctx, stream, plain_step, max(3, args.steps // 2))
     plain_ms = dist_max(plain_total / max(3, args.steps // 2), world)
 
+    # every bit-borrowing split [17-k, 33+k], k = 0..17 (k = 17 is [50]), the
+    # exhaustive sweep the cost model's choice is checked against
+    sweep = {}
+    for k in range(0, 18):
+        sp = W.split_for_k(k)
+        fn = (lambda sp=sp: ctx.run_plan(dcols, bw, sp, dorder, dgroup))
+        fn()
+        tot, _ = time_steps(ctx, stream, fn, 5)
+        sweep[str(sp)] = round(dist_max(tot / 5, world), 4)
+    card = [8192, n]
+    opt_split, _, opt_est = capi.optimize_plan(bw, card, col_bytes, n)
+    best = min(sweep, key=sweep.get)
+    split_sweep = {"ms_per_plan": sweep, "fastest": best, "cost_model_choice": opt_split,
+                   "cost_model_est_ms": round(opt_est, 4),
+                   "choice_ms": sweep.get(str(opt_split)),
+                   "choice_vs_fastest": round(sweep.get(str(opt_split), float("nan")) / sweep[best], 3)}
+
     # end to end: pinned host buffers, copies inside the timed region
     hcols = []
     for c in cols:
@@ -460,6 +477,7 @@ def run_fmcs(args):
         "plain_gpu": {"plan": PLAIN_SPLIT, "value": round(world * n / (plain_ms / 1e3) / 1e6, 2),
                       "ms_per_step": round(plain_ms, 4),
                       "speedup_of_massaged": round(plain_ms / ms_per_step, 3)},
+        "split_sweep": split_sweep,
         "roofline": roofline,
         "kernels": {k: {"launches_per_step": v["launches"] / args.steps, "ms_per_step": round(v["ms"] / args.steps, 4)}
                     for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
