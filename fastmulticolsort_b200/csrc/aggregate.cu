@@ -26,6 +26,7 @@ constexpr unsigned long long kSignFlip = 1ull << 63;
 __global__ void agg_init_kernel(uint64_t g, unsigned long long *count, unsigned long long *sum,
                                 unsigned long long *mn, unsigned long long *mx)
 {
+    kernel_prologue();
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < g; k += (uint64_t)gridDim.x * blockDim.x) {
         if (count) count[k] = 0;
         if (sum) sum[k] = 0;
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(256) agg_kernel(const P *__restrict__ payload,
                                                   bool vec, unsigned long long *count, unsigned long long *sum,
                                                   unsigned long long *mn, unsigned long long *mx, int *status)
 {
+    kernel_prologue();
     const unsigned long long flip = is_signed ? kSignFlip : 0ull;
     const uint64_t chunks = (n + kAggItems - 1) / kAggItems;
     for (uint64_t ch = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ch < chunks;
@@ -123,6 +125,7 @@ __global__ void __launch_bounds__(256) agg_kernel(const P *__restrict__ payload,
 
 __global__ void agg_unflip_kernel(uint64_t g, unsigned long long *mn, unsigned long long *mx)
 {
+    kernel_prologue();
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < g; k += (uint64_t)gridDim.x * blockDim.x) {
         if (mn) mn[k] ^= kSignFlip;
         if (mx) mx[k] ^= kSignFlip;
@@ -155,7 +158,7 @@ extern "C" int fmcs_group_aggregate(fmcs_ctx *ctx, const void *payload, uint32_t
     const unsigned ig = (unsigned)std::min<uint64_t>((ngroups + 255) / 256, (uint64_t)ctx->num_sms * 8);
     if (ngroups) {
         LaunchScope ls_(ctx, "agg_init");
-        agg_init_kernel<<<ig ? ig : 1, 256, 0, st>>>(ngroups, c, s, lo, hi);
+        launch_k(agg_init_kernel, ig ? ig : 1, 256, 0, st, ngroups, c, s, lo, hi);
     }
     if (n) {
         const uint64_t chunks = (n + kAggItems - 1) / kAggItems;
@@ -163,15 +166,15 @@ extern "C" int fmcs_group_aggregate(fmcs_ctx *ctx, const void *payload, uint32_t
         const bool vec = (((uintptr_t)order | (uintptr_t)group) & 15u) == 0;
         LaunchScope ls_(ctx, "aggregate");
         if (payload_bytes == 4)
-            agg_kernel<uint32_t><<<grid, 256, 0, st>>>((const uint32_t *)payload, is_signed != 0, order, group, n,
+            launch_k(agg_kernel<uint32_t>, grid, 256, 0, st, (const uint32_t *)payload, is_signed != 0, order, group, n,
                                                        ngroups, vec, c, s, lo, hi, ctx->d_status);
         else
-            agg_kernel<uint64_t><<<grid, 256, 0, st>>>((const uint64_t *)payload, is_signed != 0, order, group, n,
+            launch_k(agg_kernel<uint64_t>, grid, 256, 0, st, (const uint64_t *)payload, is_signed != 0, order, group, n,
                                                        ngroups, vec, c, s, lo, hi, ctx->d_status);
     }
     if (is_signed && ngroups && (lo || hi)) {
         LaunchScope ls_(ctx, "agg_unflip");
-        agg_unflip_kernel<<<ig ? ig : 1, 256, 0, st>>>(ngroups, lo, hi);
+        launch_k(agg_unflip_kernel, ig ? ig : 1, 256, 0, st, ngroups, lo, hi);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_group_aggregate launch");

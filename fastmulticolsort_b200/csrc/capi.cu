@@ -6,6 +6,7 @@
 // the round loop of Composer::multiRoundSorting (src/composer.cpp:48-135) and
 // of StitchComposer::run_single_plan (src/stitch_composer.cpp:555-806), and the
 // final status check of the bounded device waits.
+#include "device_common.cuh"
 #include "fmcs_internal.h"
 #include "plan.h"
 
@@ -581,6 +582,7 @@ namespace {
 
 __global__ void instance_ids_kernel(const uint32_t *starts, uint32_t ninst, uint32_t *inst_id, uint64_t n)
 {
+    kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t lo = 0, hi = ninst;   // starts[lo] <= i < starts[hi]
         while (hi - lo > 1) {
@@ -594,6 +596,7 @@ __global__ void instance_ids_kernel(const uint32_t *starts, uint32_t ninst, uint
 __global__ void instance_bases_kernel(const uint32_t *starts, uint32_t ninst, const uint32_t *group, uint32_t *base,
                                       uint32_t *count)
 {
+    kernel_prologue();
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ninst; k += gridDim.x * blockDim.x) {
         const uint32_t s = starts[k], e = starts[k + 1];
         base[k] = e > s ? group[s] : 0u;
@@ -604,6 +607,7 @@ __global__ void instance_bases_kernel(const uint32_t *starts, uint32_t ninst, co
 __global__ void localize_kernel(const uint32_t *starts, const uint32_t *inst_id, const uint32_t *base,
                                 uint32_t *order, uint32_t *group, uint64_t n)
 {
+    kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t k = inst_id[i];
         order[i] -= starts[k];
@@ -667,7 +671,7 @@ extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint
     if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch upload");
     {
         LaunchScope ls_(ctx, "instance_ids");
-        instance_ids_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(d_starts, ninst, inst_id, n);
+        launch_k(instance_ids_kernel, ctx->num_sms * 8, 256, 0, st, d_starts, ninst, inst_id, n);
     }
     uint32_t *w;
     if ((rc = counters(ctx, &w))) return rc;
@@ -738,11 +742,11 @@ extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint
     // instance-local oids and group ids
     {
         LaunchScope ls_(ctx, "instance_bases");
-        instance_bases_kernel<<<(ninst + 255) / 256, 256, 0, st>>>(d_starts, ninst, in_group, d_base, d_count);
+        launch_k(instance_bases_kernel, (ninst + 255) / 256, 256, 0, st, d_starts, ninst, in_group, d_base, d_count);
     }
     {
         LaunchScope ls_(ctx, "localize");
-        localize_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(d_starts, inst_id, d_base, (uint32_t *)dorder,
+        launch_k(localize_kernel, ctx->num_sms * 8, 256, 0, st, d_starts, inst_id, d_base, (uint32_t *)dorder,
                                                            (uint32_t *)in_group, n);
     }
     e = cudaGetLastError();

@@ -29,6 +29,18 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
+// First statement of every kernel of the library (programmatic dependent
+// launch): let the stream's next kernel begin launching now, then wait until
+// the previous kernel has completed and its memory is visible.  Both are
+// no-ops for a kernel launched without the programmatic attribute.  The next
+// kernel is launched only once every block of this one is running, so its
+// waiting blocks never keep this one's blocks from being scheduled.
+__device__ __forceinline__ void kernel_prologue()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt()
 {
     uint32_t m;

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <functional>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/fmcs_capi.h"
@@ -122,6 +123,26 @@ class LaunchScope {
 // cudaGraphSetConditional) to end the loop.
 int capture_while(fmcs_ctx *ctx, cudaStream_t st,
                   const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body);
+
+// Launches a library kernel with programmatic stream serialization: it may
+// begin launching while the stream's previous kernel finishes (its prologue
+// waits for that kernel's completion).  Every kernel launched this way starts
+// with kernel_prologue().
+template <typename... P, typename... A>
+inline cudaError_t launch_k(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A &&...args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 
 // True when the device can dereference p directly (device or managed memory).
 bool is_device_ptr(const void *p);

@@ -3,6 +3,7 @@
 // first read (segsort.cu, the EXT source); this standalone kernel backs the
 // fmcs_gather entry point.  Each thread issues 8 independent gathers before it
 // stores, so enough random reads are in flight to cover HBM latency.
+#include "device_common.cuh"
 #include "fmcs_internal.h"
 
 namespace fmcs {
@@ -15,6 +16,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) gather_kernel(const T *__restrict__ bank, const uint32_t *__restrict__ order,
                                                      T *__restrict__ out, uint64_t n)
 {
+    kernel_prologue();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < n;
          base += stride * kGatherItems) {
@@ -47,16 +49,16 @@ int launch_gather(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const ui
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     switch (bank_bytes) {
     case 1: { LaunchScope ls_(ctx, "gather");
-        gather_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>((const uint8_t *)bank, order, (uint8_t *)out, n);
+        launch_k(gather_kernel<uint8_t>, grid, 256, 0, ctx->stream, (const uint8_t *)bank, order, (uint8_t *)out, n);
     } break;
     case 2: { LaunchScope ls_(ctx, "gather");
-        gather_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>((const uint16_t *)bank, order, (uint16_t *)out, n);
+        launch_k(gather_kernel<uint16_t>, grid, 256, 0, ctx->stream, (const uint16_t *)bank, order, (uint16_t *)out, n);
     } break;
     case 4: { LaunchScope ls_(ctx, "gather");
-        gather_kernel<uint32_t><<<grid, 256, 0, ctx->stream>>>((const uint32_t *)bank, order, (uint32_t *)out, n);
+        launch_k(gather_kernel<uint32_t>, grid, 256, 0, ctx->stream, (const uint32_t *)bank, order, (uint32_t *)out, n);
     } break;
     case 8: { LaunchScope ls_(ctx, "gather");
-        gather_kernel<uint64_t><<<grid, 256, 0, ctx->stream>>>((const uint64_t *)bank, order, (uint64_t *)out, n);
+        launch_k(gather_kernel<uint64_t>, grid, 256, 0, ctx->stream, (const uint64_t *)bank, order, (uint64_t *)out, n);
     } break;
     default: return set_error(ctx, FMCS_E_INVAL, "gather: bank_bytes must be 1, 2, 4 or 8");
     }

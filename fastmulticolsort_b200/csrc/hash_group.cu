@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ 
                                                           uint64_t n, unsigned long long *slots, uint64_t mask,
                                                           uint32_t *slot_of, int *status)
 {
+    kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t r = run ? run[i] : 0u;
         if (runs_contiguous && (i == 0 || run[i - 1] != r) && (i + 1 == n || run[i + 1] != r)) {
@@ -108,6 +109,7 @@ __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ 
 __global__ void first_flag_kernel(const uint32_t *__restrict__ slot_of, const unsigned long long *__restrict__ slots,
                                   uint8_t *__restrict__ first, uint32_t *__restrict__ fpos, uint64_t n)
 {
+    kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t so = slot_of[i];
         const uint32_t f = so == kAlone ? (uint32_t)i : (uint32_t)slots[so];
@@ -122,6 +124,7 @@ __global__ void assign_ids_kernel(const uint32_t *__restrict__ fpos, const uint3
                                   const uint32_t *__restrict__ order, uint32_t *__restrict__ ids,
                                   uint32_t *__restrict__ row_ids, uint64_t n)
 {
+    kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t g = rank[fpos[i]];
         if (ids) ids[i] = g;
@@ -135,7 +138,8 @@ int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const ui
 {
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     { LaunchScope ls_(ctx, "hash_insert");
-        hash_insert_kernel<K><<<grid, 256, 0, ctx->stream>>>((const K *)bank, order, run, runs_contiguous, n, slots, mask,
+        launch_k(hash_insert_kernel<K>, grid, 256, 0, ctx->stream,
+                 (const K *)bank, order, run, runs_contiguous, n, slots, mask,
                                                             slot_of,
                                                             ctx->d_status);
     }
@@ -190,13 +194,13 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     if (rc) return rc;
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     { LaunchScope ls_(ctx, "first_flag");
-        first_flag_kernel<<<grid, 256, 0, st>>>(slot_of, slots, first, fpos, n);
+        launch_k(first_flag_kernel, grid, 256, 0, st, slot_of, slots, first, fpos, n);
     }
     uint32_t *rank = slot_of;   // slot_of is dead after the flags
     if ((rc = launch_flag_rank(ctx, first, rank, n, d_ngroups))) return rc;
     if (last_round) {
         { LaunchScope ls_(ctx, "assign_ids");
-            assign_ids_kernel<<<grid, 256, 0, st>>>(fpos, rank, nullptr, out_group, nullptr, n);
+            launch_k(assign_ids_kernel, grid, 256, 0, st, fpos, rank, nullptr, out_group, nullptr, n);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(ctx, e, "hash ids launch");
@@ -212,7 +216,7 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     // scattered to row order so that the sort's gather through order_in reads them.
     uint32_t *row_ids = run;   // run ids are dead after the insert
     { LaunchScope ls_(ctx, "assign_ids");
-        assign_ids_kernel<<<grid, 256, 0, st>>>(fpos, rank, order_in, nullptr, row_ids, n);
+        launch_k(assign_ids_kernel, grid, 256, 0, st, fpos, rank, order_in, nullptr, row_ids, n);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "hash ids launch");

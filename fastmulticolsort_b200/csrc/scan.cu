@@ -72,6 +72,7 @@ boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in
                      uint64_t n, uint32_t *tile_counter, unsigned long long *lookback,
                      uint32_t epoch, uint32_t *d_count, int *status)
 {
+    kernel_prologue();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[kScanWarps + 1];
     __shared__ uint32_t s_excl;
@@ -193,10 +194,12 @@ void launch_scan(unsigned grid, cudaStream_t st, const K *keys, const uint32_t *
 {
     const bool vec = (((uintptr_t)keys | (uintptr_t)in_group | (uintptr_t)flags | (uintptr_t)out_group) & 15u) == 0;
     if (vec)
-        boundary_scan_kernel<K, true><<<grid, kScanThreads, 0, st>>>(keys, in_group, flags, out_group, seg_start, n,
+        launch_k(boundary_scan_kernel<K, true>, grid, kScanThreads, 0, st,
+                 keys, in_group, flags, out_group, seg_start, n,
                                                                       tile_counter, lookback, epoch, d_count, status);
     else
-        boundary_scan_kernel<K, false><<<grid, kScanThreads, 0, st>>>(keys, in_group, flags, out_group, seg_start, n,
+        launch_k(boundary_scan_kernel<K, false>, grid, kScanThreads, 0, st,
+                 keys, in_group, flags, out_group, seg_start, n,
                                                                        tile_counter, lookback, epoch, d_count, status);
 }
 
@@ -271,6 +274,7 @@ int launch_group_ids_segments(fmcs_ctx *ctx, const void *keys, uint32_t key_byte
 namespace {
 __global__ void iota_kernel(uint32_t *v, uint64_t n)
 {
+    kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         v[i] = (uint32_t)i;
 }
@@ -280,7 +284,7 @@ int launch_iota(fmcs_ctx *ctx, uint32_t *v, uint64_t n)
 {
     if (n == 0) return FMCS_OK;
     { LaunchScope ls_(ctx, "iota");
-        iota_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(v, n);
+        launch_k(iota_kernel, ctx->num_sms * 8, 256, 0, ctx->stream, v, n);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "iota launch");

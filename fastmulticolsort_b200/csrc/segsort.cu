@@ -271,6 +271,7 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
                                 uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, Lists lists,
                                 uint32_t *hist0, const uint32_t *top_hist)
 {
+    kernel_prologue();
     if (!seg_start && top_hist && n > lists.local_max) {
         // round 0 over the whole array with its first-level histogram already
         // counted: the one large segment, histogram row 0 = top_hist
@@ -344,6 +345,7 @@ __device__ __forceinline__ void tile_prefix_body(const LargeSeg *segs, uint32_t 
 __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs, const uint32_t *d_nseg,
                                                            uint32_t *tile_prefix, uint32_t *reset, uint32_t tile_rows)
 {
+    kernel_prologue();
     if (threadIdx.x == 0) *reset = 0;
     tile_prefix_body(segs, *d_nseg, tile_prefix, tile_rows);
 }
@@ -353,6 +355,7 @@ __global__ void __launch_bounds__(1024) tile_prefix_kernel(const LargeSeg *segs,
 // advanced for the level's other launches.
 __global__ void __launch_bounds__(1024) level_prefix_kernel(LevelRefs r, uint32_t *tile_prefix, uint32_t tile_rows)
 {
+    kernel_prologue();
     const uint32_t lvl = r.dev_level ? r.ctr[kCtrLevel] : 0u;
     const uint32_t cur = lvl & 1u, nxt = cur ^ 1u;
     const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
@@ -385,6 +388,7 @@ template <typename K>
 __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, const uint32_t *tile_prefix,
                                                         uint32_t tile_rows)
 {
+    kernel_prologue();
     constexpr int NW = kNtM / 32;
     constexpr int MAXJ = 16;   // tile_rows <= 16 * kNtM
     __shared__ uint32_t sh[NW][kRadix];
@@ -432,6 +436,7 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, 
 // Per large segment: exclusive digit offsets, skip detection, children.
 __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lists, bool emit_children = true)
 {
+    kernel_prologue();
     __shared__ uint32_t cnt[kRadix];
     __shared__ uint32_t tmp[kRadix / 32 + 1];
     __shared__ uint32_t s_skip;
@@ -488,6 +493,7 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
                                                            uint32_t epoch_base, int *status,
                                                            cudaGraphConditionalHandle more, uint32_t levels)
 {
+    kernel_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MsdSmem<K, IT> &sm = *reinterpret_cast<MsdSmem<K, IT> *>(smem_raw);
     constexpr uint32_t kTileM = kNtM * IT;
@@ -1020,6 +1026,7 @@ template <typename K, int NT, int IT, int RANK>
 __global__ void __launch_bounds__(NT, 1024 / NT)
 block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
+    kernel_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NW = NT / 32;
     const uint32_t count = *d_count;
@@ -1087,6 +1094,7 @@ __device__ __forceinline__ void sort_tiny(const Bufs<K> &b, uint32_t start, uint
 template <typename K, int NMAX>
 __global__ void __launch_bounds__(256) thread_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
+    kernel_prologue();
     const uint32_t count = *d_count;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
         const uint2 ent = list[e];
@@ -1115,6 +1123,7 @@ struct WarpSmem {
 template <typename K, int RANK>
 __global__ void __launch_bounds__(256) warp_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
+    kernel_prologue();
     __shared__ WarpSmem<K> all[8];
     WarpSmem<K> &sm = all[threadIdx.x >> 5];
     const uint32_t count = *d_count;
@@ -1206,6 +1215,7 @@ __global__ void __launch_bounds__(256) warp_sort_kernel(Bufs<K> b, const uint2 *
 template <typename K>
 __global__ void __launch_bounds__(256) copy_kernel(Bufs<K> b, const LargeSeg *list, const uint32_t *d_count)
 {
+    kernel_prologue();
     const uint32_t count = *d_count;
     const int lane = threadIdx.x & 31;
     const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
@@ -1228,6 +1238,7 @@ template <typename K>
 __global__ void __launch_bounds__(256) copy_tiles_kernel(Bufs<K> b, const LargeSeg *list, const uint32_t *d_count,
                                                          const uint32_t *tile_prefix)
 {
+    kernel_prologue();
     const uint32_t count = *d_count;
     if (count == 0) return;
     const uint32_t T = tile_prefix[count];
@@ -1341,7 +1352,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                                   : 1u;
         if (seg_start && a.nseg_host == 0) grid = (unsigned)sms * 16;
         { LaunchScope ls_(ctx, "classify");
-            classify_kernel<K><<<grid, 256, 0, st>>>(b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists,
+            launch_k(classify_kernel<K>, grid, 256, 0, st, b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists,
                                                      hists[0], seg_start ? nullptr : a.top_hist);
         }
         FMCS_LAUNCH_CHECK("classify");
@@ -1372,15 +1383,15 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         // lives on the device)
         auto level = [&](cudaStream_t s, cudaGraphConditionalHandle more, bool read_back) -> int {
             { LaunchScope ls_(ctx, "tile_prefix");
-                level_prefix_kernel<<<1, 1024, 0, s>>>(lr, tile_prefix, tile_rows);
+                launch_k(level_prefix_kernel, 1, 1024, 0, s, lr, tile_prefix, tile_rows);
             }
             if (!(hist0_ready && host_lvl == 0 && read_back)) {
                 // (inside a graph the launch stays and returns at once on level 0)
                 LaunchScope ls_(ctx, "msd_hist");
-                msd_hist_kernel<K><<<sms * 8, kNtM, 0, s>>>(b, lr, tile_prefix, tile_rows);
+                launch_k(msd_hist_kernel<K>, sms * 8, kNtM, 0, s, b, lr, tile_prefix, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
-                msd_plan_kernel<<<sms * 8, kRadix, 0, s>>>(lr, lists);
+                launch_k(msd_plan_kernel, sms * 8, kRadix, 0, s, lr, lists, true);
             }
             if (read_back) {
                 // read the next level's count while the scatter runs
@@ -1391,7 +1402,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             }
             {
                 LaunchScope ls_(ctx, "msd_scatter");
-                msd_scatter_kernel<K, RANK, IT><<<scatter_grid, kNtM, msd_smem, s>>>(b, lr, tile_prefix, lookback,
+                launch_k(msd_scatter_kernel<K, RANK, IT>, scatter_grid, kNtM, msd_smem, s, b, lr, tile_prefix, lookback,
                                                                                    epoch_base, ctx->d_status, more,
                                                                                    (uint32_t)levels);
                 if (read_back) {
@@ -1438,44 +1449,45 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC3, kItC3, RANK>, smem_c3))) return rc;
     { LaunchScope ls_(ctx, "thread_sort");
-        thread_sort_kernel<K, 16><<<sms * 8, 256, 0, st>>>(b, lists.t, &ctr[kCtrLocalT]);
+        launch_k(thread_sort_kernel<K, 16>, sms * 8, 256, 0, st, b, lists.t, &ctr[kCtrLocalT]);
     }
     if constexpr (sizeof(K) <= 4) {
         LaunchScope ls_(ctx, "thread_sort_32");
-        thread_sort_kernel<K, 32><<<sms * 8, 256, 0, st>>>(b, lists.t32, &ctr[kCtrLocalT32]);
+        launch_k(thread_sort_kernel<K, 32>, sms * 8, 256, 0, st, b, lists.t32, &ctr[kCtrLocalT32]);
     }
     { LaunchScope ls_(ctx, "warp_sort");
-        warp_sort_kernel<K, RANK><<<sms * 16, 256, 0, st>>>(b, lists.a, &ctr[kCtrLocalA]);
+        launch_k(warp_sort_kernel<K, RANK>, sms * 16, 256, 0, st, b, lists.a, &ctr[kCtrLocalA]);
     }
     { LaunchScope ls_(ctx, "block_sort_512");
-        block_sort_kernel<K, kNtB1, kItB1, RANK><<<sms * (1024 / kNtB1), kNtB1, smem_b1, st>>>(b, lists.b1,
+        launch_k(block_sort_kernel<K, kNtB1, kItB1, RANK>, sms * (1024 / kNtB1), kNtB1, smem_b1, st, b, lists.b1,
                                                                                            &ctr[kCtrLocalB1]);
     }
     { LaunchScope ls_(ctx, "block_sort_1024");
-        block_sort_kernel<K, kNtB2, kItB2, RANK><<<sms * (1024 / kNtB2), kNtB2, smem_b2, st>>>(b, lists.b2,
+        launch_k(block_sort_kernel<K, kNtB2, kItB2, RANK>, sms * (1024 / kNtB2), kNtB2, smem_b2, st, b, lists.b2,
                                                                                            &ctr[kCtrLocalB2]);
     }
     { LaunchScope ls_(ctx, "block_sort_2048");
-        block_sort_kernel<K, kNtC1, kItC1, RANK><<<sms * (1024 / kNtC1), kNtC1, smem_c1, st>>>(b, lists.c1,
+        launch_k(block_sort_kernel<K, kNtC1, kItC1, RANK>, sms * (1024 / kNtC1), kNtC1, smem_c1, st, b, lists.c1,
                                                                                            &ctr[kCtrLocalC1]);
     }
     { LaunchScope ls_(ctx, "block_sort_4096");
-        block_sort_kernel<K, kNtC2, kItC2, RANK><<<sms * (1024 / kNtC2), kNtC2, smem_c2, st>>>(b, lists.c2,
+        launch_k(block_sort_kernel<K, kNtC2, kItC2, RANK>, sms * (1024 / kNtC2), kNtC2, smem_c2, st, b, lists.c2,
                                                                                            &ctr[kCtrLocalC2]);
     }
     { LaunchScope ls_(ctx, "block_sort_8192");
-        block_sort_kernel<K, kNtC3, kItC3, RANK><<<sms * (1024 / kNtC3), kNtC3, smem_c3, st>>>(b, lists.c3,
+        launch_k(block_sort_kernel<K, kNtC3, kItC3, RANK>, sms * (1024 / kNtC3), kNtC3, smem_c3, st, b, lists.c3,
                                                                                            &ctr[kCtrLocalC3]);
     }
     { LaunchScope ls_(ctx, "copy");
-        copy_kernel<K><<<sms * 4, 256, 0, st>>>(b, lists.copy, &ctr[kCtrCopy]);
+        launch_k(copy_kernel<K>, sms * 4, 256, 0, st, b, lists.copy, &ctr[kCtrCopy]);
     }
     { LaunchScope ls_(ctx, "tile_prefix");
-        tile_prefix_kernel<<<1, 1024, 0, st>>>(lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix, &ctr[kCtrCopyTile],
+        launch_k(tile_prefix_kernel, 1, 1024, 0, st,
+                 lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix, &ctr[kCtrCopyTile],
                                                kCopySplit);
     }
     { LaunchScope ls_(ctx, "copy_tiles");
-        copy_tiles_kernel<K><<<sms * 8, 256, 0, st>>>(b, lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix);
+        launch_k(copy_tiles_kernel<K>, sms * 8, 256, 0, st, b, lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix);
     }
     FMCS_LAUNCH_CHECK("local tiers");
     return FMCS_OK;
@@ -1492,6 +1504,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
 __global__ void lsd_set_pass_kernel(LargeSeg *seg, uint32_t *hist_row, uint32_t *nseg, uint32_t n, uint32_t shift,
                                     int first)
 {
+    kernel_prologue();
     if (threadIdx.x == 0) {
         uint32_t src = kSrcBuf0;
         if (!first) {
@@ -1507,6 +1520,7 @@ __global__ void lsd_set_pass_kernel(LargeSeg *seg, uint32_t *hist_row, uint32_t 
 template <typename K>
 __global__ void lsd_finalize_kernel(Bufs<K> b, const LargeSeg *seg, uint64_t n)
 {
+    kernel_prologue();
     const LargeSeg last = seg[0];
     const uint32_t where = (last.src & kSkipBit) ? (last.src & 3u) : ((last.src & 3u) == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
     if (where != kSrcBuf1) return;
@@ -1557,26 +1571,26 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
     for (uint32_t lo = 0; lo < bits; lo += kRadixBits, ++pass) {
         const uint32_t shift = std::min(bits, lo + kRadixBits);
         { LaunchScope ls_(ctx, "lsd_set_pass");
-            lsd_set_pass_kernel<<<1, 256, 0, st>>>(seg, hist, &ctr[kCtrLarge0], (uint32_t)n, shift, pass == 0);
+            launch_k(lsd_set_pass_kernel, 1, 256, 0, st, seg, hist, &ctr[kCtrLarge0], (uint32_t)n, shift, pass == 0);
         }
         { LaunchScope ls_(ctx, "tile_prefix");
-            level_prefix_kernel<<<1, 1024, 0, st>>>(lr, tile_prefix, tile_rows);
+            launch_k(level_prefix_kernel, 1, 1024, 0, st, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_hist");
-            msd_hist_kernel<K><<<sms * 8, kNtM, 0, st>>>(b, lr, tile_prefix, tile_rows);
+            launch_k(msd_hist_kernel<K>, sms * 8, kNtM, 0, st, b, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_plan");
-            msd_plan_kernel<<<1, kRadix, 0, st>>>(lr, none, false);
+            launch_k(msd_plan_kernel, 1, kRadix, 0, st, lr, none, false);
         }
         { LaunchScope ls_(ctx, "msd_scatter");
-            msd_scatter_kernel<K, RANK, IT><<<sms * msd_ctas_per_sm(IT), kNtM, msd_smem, st>>>(
+            launch_k(msd_scatter_kernel<K, RANK, IT>, sms * msd_ctas_per_sm(IT), kNtM, msd_smem, st, 
                 b, lr, tile_prefix, lookback, ctx->epoch++, ctx->d_status, 0, 1u);
         }
         FMCS_LAUNCH_CHECK("lsd pass");
     }
     if (pass > 0) {
         LaunchScope ls_(ctx, "lsd_finalize");
-        lsd_finalize_kernel<K><<<sms * 8, 256, 0, st>>>(b, seg, n);
+        launch_k(lsd_finalize_kernel<K>, sms * 8, 256, 0, st, b, seg, n);
     }
     FMCS_LAUNCH_CHECK("lsd finalize");
     return FMCS_OK;

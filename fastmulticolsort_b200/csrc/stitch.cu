@@ -8,6 +8,7 @@
 // consecutive rows, reads each source slice with one vector load per row
 // group, folds the slices in registers and writes the bank once: the kernel
 // moves exactly sum(source bytes) + bank bytes per row.
+#include "device_common.cuh"
 #include "fmcs_internal.h"
 
 #include <algorithm>
@@ -95,6 +96,7 @@ __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ Sti
                                                      uint64_t n, bool aligned, uint32_t *top_hist,
                                                      uint32_t hist_lo, uint32_t hist_mask)
 {
+    kernel_prologue();
     __shared__ uint32_t sh[256];
     if (top_hist) {
         for (int d = threadIdx.x; d < 256; d += blockDim.x) sh[d] = 0;
@@ -147,6 +149,7 @@ template <typename B>
 __global__ void __launch_bounds__(256) bank_update_kernel(B *bank, uint64_t n, uint32_t lshift, const void *src,
                                                           uint32_t src_bytes, uint32_t rshift, uint32_t width)
 {
+    kernel_prologue();
     const uint64_t mask = width >= 64 ? ~0ull : ((1ull << width) - 1);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         if (!src) {
@@ -173,10 +176,14 @@ int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t 
     const unsigned grid = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 8);
     LaunchScope ls_(ctx, src ? "assemble" : "shift_left");
     switch (bank_bytes) {
-    case 1: bank_update_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>((uint8_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
-    case 2: bank_update_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>((uint16_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
-    case 4: bank_update_kernel<uint32_t><<<grid, 256, 0, ctx->stream>>>((uint32_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
-    case 8: bank_update_kernel<uint64_t><<<grid, 256, 0, ctx->stream>>>((uint64_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 1: launch_k(bank_update_kernel<uint8_t>, grid, 256, 0, ctx->stream,
+                     (uint8_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 2: launch_k(bank_update_kernel<uint16_t>, grid, 256, 0, ctx->stream,
+                     (uint16_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 4: launch_k(bank_update_kernel<uint32_t>, grid, 256, 0, ctx->stream,
+                     (uint32_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
+    case 8: launch_k(bank_update_kernel<uint64_t>, grid, 256, 0, ctx->stream,
+                     (uint64_t *)bank, n, lshift, src, src_bytes, rshift, width); break;
     default: return set_error(ctx, FMCS_E_INVAL, "bank_bytes must be 1, 2, 4 or 8");
     }
     cudaError_t e = cudaGetLastError();
@@ -213,16 +220,20 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
     LaunchScope ls_(ctx, "stitch");
     switch (bank_bytes) {
     case 1:
-        stitch_kernel<uint8_t><<<grid, 256, 0, st>>>(p, (uint8_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        launch_k(stitch_kernel<uint8_t>, grid, 256, 0, st,
+                 p, (uint8_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
         break;
     case 2:
-        stitch_kernel<uint16_t><<<grid, 256, 0, st>>>(p, (uint16_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        launch_k(stitch_kernel<uint16_t>, grid, 256, 0, st,
+                 p, (uint16_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
         break;
     case 4:
-        stitch_kernel<uint32_t><<<grid, 256, 0, st>>>(p, (uint32_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        launch_k(stitch_kernel<uint32_t>, grid, 256, 0, st,
+                 p, (uint32_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
         break;
     case 8:
-        stitch_kernel<uint64_t><<<grid, 256, 0, st>>>(p, (uint64_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+        launch_k(stitch_kernel<uint64_t>, grid, 256, 0, st,
+                 p, (uint64_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
         break;
     default: return set_error(ctx, FMCS_E_INVAL, "stitch: bank_bytes must be 1, 2, 4 or 8");
     }
