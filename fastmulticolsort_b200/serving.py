@@ -88,32 +88,52 @@ def make_trace(rng, rate, duration, pool_size):
     return trace
 
 
-def run_served(torch, pool, trace, slots, budget, batch_rows_max):
-    lat, rows, batched = [], 0, 0
-    with capi.Server(0, hbm_budget_bytes=budget, slots=slots, batch_rows_max=batch_rows_max) as srv:
-        pending = []
-        t0 = time.perf_counter()
-        for arrival, k in trace:
-            now = time.perf_counter() - t0
-            if arrival > now:
-                time.sleep(arrival - now)
-            d = pool[k]
+def warm(torch, srv, pool, rounds=2):
+    """Every slot's workspace grown to what the pool needs before timing: the
+    whole pool submitted at once, so that the slots share out its large
+    requests (a workspace that grows in the middle of a trace would put its
+    cudaMalloc, a device-wide synchronisation, on some request's latency)."""
+    for _ in range(rounds):
+        keep = []
+        for d in pool:
             o = torch.empty(d["n"], dtype=torch.int32, device="cuda")
-            g = torch.empty(d["n"], dtype=torch.int32, device="cuda")
-            pending.append((srv.submit(d["cols"], d["widths"], o, g, cardinality=d["card"]), o, g, d["n"]))
-            # reap what finished, keeping memory bounded
-            while len(pending) > 4 * slots:
-                tk, _, _, n = pending.pop(0)
-                r = srv.wait(tk)
-                lat.append(r["total_ms"])
-                rows += n
-                batched += r["batched_with"] > 1
-        for tk, _, _, n in pending:
+            keep.append((srv.submit(d["cols"], d["widths"], o, cardinality=d["card"]), o))
+        for tk, _ in keep:
+            srv.wait(tk)
+
+
+def run_served(torch, srv, pool, trace, slots):
+    """The trace through the server.  Outputs come from a ring of buffers
+    allocated before timing (a buffer is reused only after its request was
+    waited for), so no allocation sits inside the timed loop."""
+    lat, rows, batched = [], 0, 0
+    depth = 4 * slots
+    maxn = max(d["n"] for d in pool)
+    ring = [(torch.empty(maxn, dtype=torch.int32, device="cuda"), torch.empty(maxn, dtype=torch.int32, device="cuda"))
+            for _ in range(depth + 2)]
+    torch.cuda.synchronize()
+    pending = []
+    t0 = time.perf_counter()
+    for i, (arrival, k) in enumerate(trace):
+        now = time.perf_counter() - t0
+        if arrival > now:
+            time.sleep(arrival - now)
+        d = pool[k]
+        o, g = ring[i % len(ring)]
+        pending.append((srv.submit(d["cols"], d["widths"], o[:d["n"]], g[:d["n"]], cardinality=d["card"]), d["n"]))
+        # reap what finished, keeping the buffers in use bounded
+        while len(pending) > depth:
+            tk, n = pending.pop(0)
             r = srv.wait(tk)
             lat.append(r["total_ms"])
             rows += n
             batched += r["batched_with"] > 1
-        wall = time.perf_counter() - t0
+    for tk, n in pending:
+        r = srv.wait(tk)
+        lat.append(r["total_ms"])
+        rows += n
+        batched += r["batched_with"] > 1
+    wall = time.perf_counter() - t0
     return lat, rows, wall, batched
 
 
@@ -151,12 +171,10 @@ def benchmark(rate=200.0, duration=5.0, pool_size=32, slots=4, budget=150 << 30,
     rng = np.random.default_rng(seed)
     pool = [make_request_data(torch, rng) for _ in range(pool_size)]
     trace = make_trace(rng, rate, duration, pool_size)
-    # warm the served path (plan search, workspace) on every pool entry
     with capi.Server(0, hbm_budget_bytes=budget, slots=slots, batch_rows_max=batch_rows_max) as srv:
-        for d in pool:
-            o = torch.empty(d["n"], dtype=torch.int32, device="cuda")
-            srv.wait(srv.submit(d["cols"], d["widths"], o, cardinality=d["card"]))
-    lat, rows, wall, batched = run_served(torch, pool, trace, slots, budget, batch_rows_max)
+        warm(torch, srv, pool)
+        torch.cuda.synchronize()
+        lat, rows, wall, batched = run_served(torch, srv, pool, trace, slots)
     with capi.Context(0) as ctx:
         plat, prows, pwall = run_serial_plain(torch, ctx, pool, trace)
     return {
