@@ -79,8 +79,13 @@ __device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, uint32_t f
 //   kRankMatch:  one match.any.sync on the digit;
 //   kRankBallot: one ballot per digit bit, peers = AND over bits of the
 //                ballot or its complement (the ballot-based multisplit).
+//   kRankOr:     (scatter kernels with a per-warp peer array in shared
+//                memory) each lane ORs its bit into the word of its digit;
+//                after a warp barrier that word is the peer set.  Elsewhere
+//                kRankOr ranks as kRankBallot.
 constexpr int kRankMatch = 0;
 constexpr int kRankBallot = 1;
+constexpr int kRankOr = 2;
 
 template <int MODE>
 __device__ __forceinline__ uint32_t peers_of(uint32_t digit, bool valid, uint32_t width)
@@ -143,6 +148,28 @@ __device__ __forceinline__ uint32_t wlms_rank_full(uint32_t digit, uint32_t *whi
     base = __shfl_sync(0xFFFFFFFFu, base, leader);
     __syncwarp();
     return base + __popc(peers & lanemask_lt());
+}
+
+// wlms_rank by shared-memory OR: `peerw` is the warp's kRadix-word peer array,
+// all zero on entry and left all zero (each digit's leader clears its word).
+__device__ __forceinline__ uint32_t wlms_rank_or(uint32_t digit, bool valid, uint32_t *whist, uint32_t *peerw)
+{
+    const uint32_t lane = lane_id();
+    if (valid) atomicOr(&peerw[digit], 1u << lane);
+    __syncwarp();
+    uint32_t peers = 0, base = 0;
+    if (valid) {
+        peers = peerw[digit];
+        base = whist[digit];
+    }
+    __syncwarp();
+    const uint32_t below = __popc(peers & lanemask_lt());
+    if (valid && below == 0) {
+        whist[digit] = base + __popc(peers);
+        peerw[digit] = 0;
+    }
+    __syncwarp();
+    return base + below;
 }
 
 // Exclusive scan of kRadix counters in shared memory by a block of NT threads.

@@ -88,7 +88,7 @@ struct fmcs_ctx {
     unsigned long long launches = 0;   // kernels launched by this context
     cudaEvent_t ev_level = nullptr;    // host-side read-back point of the sort levels
     // tuned knobs (the autotuner's tuning/b200.json, FMCS_TUNING, or fmcs_set_tuning)
-    int rank_mode = 0;                 // 0: match.any multi-split, 1: ballot multi-split
+    int rank_mode = 0;                 // 0: match.any multi-split, 1: ballot, 2: shared-memory OR
     uint32_t local_max = 8192;         // segments above this many rows take the MSD levels
     uint32_t msd_items = 8;            // items per thread of an MSD tile (8 or 16)
     int prof_round = -1;               // round tag of the launches being profiled

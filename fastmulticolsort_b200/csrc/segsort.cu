@@ -485,6 +485,7 @@ struct MsdSmem {
     uint32_t tile, seg;
     K keys[kNtM * IT];
     uint32_t vals[kNtM * IT];
+    static_assert(kNtM * IT >= (kNtM / 32) * kRadix, "the peer words of kRankOr fit in vals");
 };
 
 template <typename K, int RANK, int IT>
@@ -540,7 +541,13 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
         const uint64_t tbeg = (uint64_t)sg.start + (uint64_t)k * kTileM;
         const uint64_t send = (uint64_t)sg.start + sg.len;
         const uint32_t cnt = (uint32_t)min((uint64_t)kTileM, send - tbeg);
-        for (int d = lane; d < kRadix; d += 32) sm.whist[warp][d] = 0;
+        // kRankOr's per-warp peer words live in the vals staging area, which
+        // is free until the ranks are known
+        uint32_t *peerw = &sm.vals[warp * kRadix];
+        for (int d = lane; d < kRadix; d += 32) {
+            sm.whist[warp][d] = 0;
+            if constexpr (RANK == kRankOr) peerw[d] = 0;
+        }
         __syncwarp();
 
         K key[IT];
@@ -553,14 +560,20 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
 #pragma unroll
             for (int j = 0; j < IT; ++j) {
                 const uint32_t d = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
-                rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
+                if constexpr (RANK == kRankOr)
+                    rd[j] = wlms_rank_or(d, true, sm.whist[warp], peerw) | (d << 16);
+                else
+                    rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
             }
         } else {
 #pragma unroll
             for (int j = 0; j < IT; ++j) {
                 const uint32_t p = wbase + j * 32 + lane;
                 const uint32_t d = digit_of(key[j], lo, width);
-                rd[j] = wlms_rank<RANK>(d, p < cnt, sm.whist[warp], width) | (d << 16);
+                if constexpr (RANK == kRankOr)
+                    rd[j] = wlms_rank_or(d, p < cnt, sm.whist[warp], peerw) | (d << 16);
+                else
+                    rd[j] = wlms_rank<RANK>(d, p < cnt, sm.whist[warp], width) | (d << 16);
             }
         }
         __syncthreads();
@@ -656,7 +669,7 @@ template <typename K, int NT, int IT>
 struct BucketSmem {
     unsigned long long cs[NT * IT];   // compound keys, bucketed
     uint32_t vals[NT * IT];
-    uint32_t off[NT * IT + 1];        // per bucket: count -> start; then (as u16) final place -> slot
+    uint32_t off[NT * IT + 1];        // per bucket: count -> start
     uint16_t orig[NT * IT];           // position in the segment, when the compound key has no room for it
     uint32_t tmp[NT / 32 + 1];
     unsigned long long any, all;      // OR and AND of the segment's keys
@@ -804,57 +817,58 @@ __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, cons
         __syncthreads();
         return false;   // uniform across the block
     }
+    // rows land bucketed; each keeps its bucket's start and size (start | size << 16)
+    uint32_t bk[IT];
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         const uint32_t p = wbase + j * 32 + lane;
+        bk[j] = 0;
         if (j < (int)steps && p < len) {
-            const uint32_t pos = sm.off[(uint32_t)(c[j] >> dshift)] + slot[j];
+            const uint32_t bi = (uint32_t)(c[j] >> dshift);
+            const uint32_t bs = sm.off[bi];
+            const uint32_t be = bi + 1 < nb ? sm.off[bi + 1] : len;
+            const uint32_t pos = bs + slot[j];
+            bk[j] = bs | ((be - bs) << 16);
             sm.cs[pos] = c[j];
             sm.vals[pos] = val[j];
             if (!packed) sm.orig[pos] = (uint16_t)p;
         }
     }
     __syncthreads();
-    uint16_t *perm = reinterpret_cast<uint16_t *>(sm.off);   // off is not needed any more
-    for (uint32_t p = threadIdx.x; p < len; p += NT) {
-        const unsigned long long c = sm.cs[p];
-        const unsigned long long d = c >> dshift;
-        uint32_t r = 0, before = 0;
-        if (packed) {
-            for (int q = (int)p - 1; q >= 0; --q) {
-                const unsigned long long cq = sm.cs[q];
-                if ((cq >> dshift) != d) break;
-                ++before;
-                r += cq < c;
-            }
-            for (uint32_t q = p + 1; q < len; ++q) {
-                const unsigned long long cq = sm.cs[q];
-                if ((cq >> dshift) != d) break;
-                r += cq < c;
-            }
-        } else {
-            const uint32_t o = sm.orig[p];
-            for (int q = (int)p - 1; q >= 0; --q) {
-                const unsigned long long cq = sm.cs[q];
-                if ((cq >> dshift) != d) break;
-                ++before;
-                r += (cq < c) | ((cq == c) & ((uint32_t)sm.orig[q] < o));
-            }
-            for (uint32_t q = p + 1; q < len; ++q) {
-                const unsigned long long cq = sm.cs[q];
-                if ((cq >> dshift) != d) break;
-                r += (cq < c) | ((cq == c) & ((uint32_t)sm.orig[q] < o));
+    // a row alone in its bucket is in its place; the others count the rows of
+    // their bucket that sort before them (by compound key, then position)
+    uint32_t fin[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t bs = bk[j] & 0xFFFFu, bn = bk[j] >> 16;
+        uint32_t r = 0;
+        if (bn > 1) {
+            if (packed) {
+                for (uint32_t q = 0; q < bn; ++q) r += sm.cs[bs + q] < c[j];
+            } else {
+                const uint32_t o = wbase + j * 32 + lane;
+                for (uint32_t q = 0; q < bn; ++q) {
+                    const unsigned long long cq = sm.cs[bs + q];
+                    r += (cq < c[j]) | ((cq == c[j]) & ((uint32_t)sm.orig[bs + q] < o));
+                }
             }
         }
-        perm[p - before + r] = (uint16_t)p;
+        fin[j] = bs + r;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        if ((bk[j] >> 16) > 1) {
+            sm.cs[fin[j]] = c[j];
+            sm.vals[fin[j]] = val[j];
+        }
     }
     __syncthreads();
     // every load of this segment is done (barriers above) before the first
     // store into BUF0, which may alias the EXT oids of the range
     for (uint32_t p = threadIdx.x; p < len; p += NT) {
-        const uint32_t q = perm[p];
-        ko[p] = (K)(prefix | (sm.cs[q] >> sh));
-        vo[p] = sm.vals[q];
+        ko[p] = (K)(prefix | (sm.cs[p] >> sh));
+        vo[p] = sm.vals[p];
     }
     __syncthreads();
     return true;
@@ -1613,6 +1627,8 @@ template <typename K>
 static int sort_dispatch(fmcs_ctx *ctx, const SortArgs &a)
 {
     const bool big = ctx->msd_items >= 16;
+    if (ctx->rank_mode == 2)
+        return big ? sort_segments_t<K, kRankOr, 16>(ctx, a) : sort_segments_t<K, kRankOr, 8>(ctx, a);
     if (ctx->rank_mode)
         return big ? sort_segments_t<K, kRankBallot, 16>(ctx, a) : sort_segments_t<K, kRankBallot, 8>(ctx, a);
     return big ? sort_segments_t<K, kRankMatch, 16>(ctx, a) : sort_segments_t<K, kRankMatch, 8>(ctx, a);
