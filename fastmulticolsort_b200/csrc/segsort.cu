@@ -370,12 +370,23 @@ __global__ void __launch_bounds__(1024) level_prefix_kernel(LevelRefs r, uint32_
 }
 
 
-__device__ __forceinline__ uint32_t find_segment(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
+// The segment of tile t (tile_prefix[s] <= t < tile_prefix[s + 1]), found by
+// a whole warp (t the same in every lane): each round the 32 lanes probe 32
+// evenly spaced prefixes, so the range shrinks 32-fold per dependent load (two
+// rounds for 1,024 segments) instead of 2-fold as in a binary search.
+__device__ __forceinline__ uint32_t find_segment_warp(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
 {
     uint32_t lo = 0, hi = nseg;  // tile_prefix[lo] <= t < tile_prefix[hi]
+    const uint32_t lane = lane_id();
     while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (tile_prefix[mid] <= t) lo = mid; else hi = mid;
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t m = lo + lane * step;
+        // the prefixes do not decrease: the lanes whose probe is <= t are a
+        // prefix of the warp, and lane 0 (probing lo) is one of them
+        const bool le = m < hi && tile_prefix[m] <= t;
+        const uint32_t c = __popc(__ballot_sync(0xFFFFFFFFu, le));
+        lo += (c - 1) * step;
+        hi = min(hi, lo + step);
     }
     return lo;
 }
@@ -402,7 +413,7 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, 
     const uint32_t T = tile_prefix[nseg];
     const int warp = threadIdx.x >> 5;
     for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
-        const uint32_t s = find_segment(tile_prefix, nseg, t);
+        const uint32_t s = find_segment_warp(tile_prefix, nseg, t);
         const LargeSeg sg = segs[s];
         const uint32_t k = t - tile_prefix[s];
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
@@ -529,7 +540,7 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
         __syncthreads();
         const uint32_t t = sm.tile;
         if (t >= T) break;
-        const uint32_t s = find_segment(tile_prefix, nseg, t);
+        const uint32_t s = find_segment_warp(tile_prefix, nseg, t);
         const LargeSeg sg = segs[s];
         if (sg.src & kSkipBit) {
             __syncthreads();
@@ -1257,7 +1268,7 @@ __global__ void __launch_bounds__(256) copy_tiles_kernel(Bufs<K> b, const LargeS
     if (count == 0) return;
     const uint32_t T = tile_prefix[count];
     for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
-        const uint32_t s = find_segment(tile_prefix, count, t);
+        const uint32_t s = find_segment_warp(tile_prefix, count, t);
         const LargeSeg sg = list[s];
         const uint64_t beg = (uint64_t)sg.start + (uint64_t)(t - tile_prefix[s]) * kCopySplit;
         const uint64_t end = min((uint64_t)sg.start + sg.len, beg + kCopySplit);
