@@ -11,6 +11,7 @@
 #include "device_common.cuh"
 #include "fmcs_internal.h"
 
+#include <algorithm>
 #include <mutex>
 
 namespace fmcs {
@@ -22,22 +23,44 @@ constexpr int kScanItems = 16;                  // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kScanWarps = kScanThreads / 32;
 
-// kScanItems consecutive values starting at i0 (zero past n); 16-byte vector
-// loads when the run is whole and VEC (the caller checked the alignment).
-template <typename T, bool VEC>
-__device__ __forceinline__ void load_run(const T *__restrict__ p, uint64_t i0, uint64_t n, T (&v)[kScanItems])
+// P consecutive values of a starting at p (zero past n), as one 4-, 8- or
+// 16-byte-multiple vector load when VEC and the run is whole.
+template <typename T, int P, bool VEC>
+__device__ __forceinline__ void load_chunk(const T *__restrict__ a, uint64_t p, uint64_t n, T (&out)[P])
 {
-    if (VEC && i0 + kScanItems <= n) {
-        constexpr int W = kScanItems * (int)sizeof(T) / 16;
-        const uint4 *q = reinterpret_cast<const uint4 *>(p + i0);
-        uint4 t[W];
+    constexpr int B = P * (int)sizeof(T);
+    if (VEC && p + P <= n) {
+        if constexpr (B == 4) {
+            const uint32_t w = *reinterpret_cast<const uint32_t *>(a + p);
+            memcpy(&out[0], &w, 4);
+        } else if constexpr (B == 8) {
+            const uint2 w = *reinterpret_cast<const uint2 *>(a + p);
+            memcpy(&out[0], &w, 8);
+        } else {
+            static_assert(B % 16 == 0, "chunk bytes");
+            uint4 w[B / 16];
 #pragma unroll
-        for (int w = 0; w < W; ++w) t[w] = q[w];
-        memcpy(&v[0], &t[0], sizeof(t));
+            for (int i = 0; i < B / 16; ++i) w[i] = reinterpret_cast<const uint4 *>(a + p)[i];
+            memcpy(&out[0], &w[0], B);
+        }
     } else {
 #pragma unroll
-        for (int k = 0; k < kScanItems; ++k) v[k] = i0 + k < n ? p[i0 + k] : T(0);
+        for (int j = 0; j < P; ++j) out[j] = p + j < n ? a[p + j] : T(0);
     }
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_up_any(T v, int d)
+{
+    if constexpr (sizeof(T) == 8) return (T)__shfl_up_sync(0xFFFFFFFFu, (unsigned long long)v, d);
+    else return (T)__shfl_up_sync(0xFFFFFFFFu, (uint32_t)v, d);
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_any(T v, int src)
+{
+    if constexpr (sizeof(T) == 8) return (T)__shfl_sync(0xFFFFFFFFu, (unsigned long long)v, src);
+    else return (T)__shfl_sync(0xFFFFFFFFu, (uint32_t)v, src);
 }
 
 // Decoupled look-back by one warp: each lane reads one predecessor's word
@@ -63,144 +86,267 @@ __device__ __forceinline__ uint32_t warp_lookback(unsigned long long *lookback, 
     }
 }
 
-// One tile of kScanTile positions per block; thread t owns the kScanItems
-// consecutive positions starting at tile base + t * kScanItems.
-template <typename K, bool VEC>
-__global__ void __launch_bounds__(kScanThreads)
+// What the scan reads: sorted keys, the previous round's group ids, both, or
+// precomputed boundary flags.
+enum ScanMode { kScanKeys = 1, kScanGroup = 2, kScanKeysGroup = 3, kScanFlags = 4 };
+
+// Position layout of a tile.  Warp w owns the 512 positions starting at
+// tile base + w * 512, in C chunks of 32 * P; in chunk c lane l owns the P
+// consecutive positions starting at c * 32 * P + l * P.  P is chosen so that
+// a lane's run of the widest array read is 16 bytes: each warp load
+// instruction then reads 512 contiguous bytes (whole sectors, each once).
+template <typename K, int MODE>
+struct ScanLayout {
+    static constexpr bool kKeys = (MODE & kScanKeys) != 0;
+    static constexpr bool kGroup = (MODE & kScanGroup) != 0;
+    static constexpr bool kFlags = MODE == kScanFlags;
+    static constexpr int kKeyBytes = kKeys ? (int)sizeof(K) : 1;
+    static constexpr int kWidest = kFlags ? 1 : (kGroup && kKeyBytes < 4 ? 4 : kKeyBytes);
+    static constexpr int P = 16 / kWidest;
+    static constexpr int C = kScanItems / P;
+    // per-chunk counts packed into one 64-bit word, in fields wide enough for
+    // a warp's sum (at most 32 * P)
+    static constexpr int FW = 32 * P <= 255 ? 8 : 16;
+    static_assert(C * FW <= 64, "packed chunk counts");
+};
+
+// Persistent blocks (as many as are resident); each claims tiles of
+// kScanTile positions in order from the tile counter.  Once a tile's boundary
+// flags are known its rows are no longer needed, so the block claims its next
+// tile and issues that tile's loads before the look-back: the look-back's
+// waits and the next loads overlap.
+template <typename K, int MODE, bool VEC>
+__global__ void __launch_bounds__(kScanThreads, 2)
 boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group,
                      const uint8_t *__restrict__ flags, uint32_t *__restrict__ out_group, uint32_t *__restrict__ seg_start,
                      uint64_t n, uint32_t *tile_counter, unsigned long long *lookback,
                      uint32_t epoch, uint32_t *d_count, int *status)
 {
     kernel_prologue();
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warp[kScanWarps + 1];
-    __shared__ uint32_t s_excl;
+    using L = ScanLayout<K, MODE>;
+    constexpr int P = L::P, C = L::C, FW = L::FW;
+    constexpr uint32_t kChunkMask = (1u << P) - 1u;
+    constexpr unsigned long long kFieldMask = (1ull << FW) - 1ull;
+    // double-buffered per tile, so that one tile's readers and the next
+    // tile's writers need no barrier between them
+    __shared__ uint32_t s_tile[2];
+    __shared__ uint32_t s_warp[2][kScanWarps + 1];
+    __shared__ uint32_t s_excl[2];
 
-    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint64_t base = (uint64_t)tile * kScanTile;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
 
-    // boundary flags of the thread's positions, bit k = position i0 + k
-    uint32_t fl = 0;
-    if (i0 < n) {
-        if (flags) {
-            uint8_t f[kScanItems];
-            load_run<uint8_t, VEC>(flags, i0, n, f);
+    K v[C][P];
+    K vprev = K(0);        // lane 0: the key before the warp's first position
+    uint32_t g[C][P];
+    uint32_t gprev = 0;
+    uint8_t f[C][P];
+    auto load = [&](uint32_t tile) {
+        const uint64_t wb = (uint64_t)tile * kScanTile + (uint64_t)warp * (32 * kScanItems);
+        if (tile >= tiles || wb >= n) return;
 #pragma unroll
-            for (int k = 0; k < kScanItems; ++k) fl |= (uint32_t)(f[k] != 0) << k;
-        } else {
-            if (keys) {
-                K v[kScanItems];
-                load_run<K, VEC>(keys, i0, n, v);
-                K prev = i0 > 0 ? keys[i0 - 1] : K(0);
-#pragma unroll
-                for (int k = 0; k < kScanItems; ++k) {
-                    fl |= (uint32_t)(v[k] != prev) << k;
-                    prev = v[k];
-                }
-            }
-            if (in_group) {
-                uint32_t g[kScanItems];
-                load_run<uint32_t, VEC>(in_group, i0, n, g);
-                uint32_t prev = i0 > 0 ? in_group[i0 - 1] : 0u;
-#pragma unroll
-                for (int k = 0; k < kScanItems; ++k) {
-                    fl |= (uint32_t)(g[k] != prev) << k;
-                    prev = g[k];
-                }
-            }
-            if (i0 == 0) fl |= 1u;
+        for (int c = 0; c < C; ++c) {
+            const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+            if constexpr (L::kKeys) load_chunk<K, P, VEC>(keys, p, n, v[c]);
+            if constexpr (L::kGroup) load_chunk<uint32_t, P, VEC>(in_group, p, n, g[c]);
+            if constexpr (L::kFlags) load_chunk<uint8_t, P, VEC>(flags, p, n, f[c]);
         }
-        if (n - i0 < (uint64_t)kScanItems) fl &= (1u << (uint32_t)(n - i0)) - 1u;   // positions past n
-    }
-    const uint32_t cnt = __popc(fl);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
+        if (lane == 0 && wb > 0) {
+            if constexpr (L::kKeys) vprev = keys[wb - 1];
+            if constexpr (L::kGroup) gprev = in_group[wb - 1];
+        }
+    };
+
+    if (threadIdx.x == 0) s_tile[0] = atomicAdd(tile_counter, 1u);
     __syncthreads();
-    if (warp == 0) {
-        uint32_t wv = lane < kScanWarps ? s_warp[lane] : 0u;
-        uint32_t wi = wv;
+    uint32_t tile = s_tile[0];
+    load(tile);
+    int buf = 0;
+    while (tile < tiles) {
+        const uint64_t base = (uint64_t)tile * kScanTile;
+        const uint64_t wb = base + (uint64_t)warp * (32 * kScanItems);
+        uint32_t claim = 0;
+        if (threadIdx.x == 0) claim = atomicAdd(tile_counter, 1u);
+        // boundary flags, bit c * P + j = position wb + c * 32 * P + lane * P + j
+        uint32_t fl = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+            uint32_t bits = 0;
+            if constexpr (L::kFlags) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) bits |= (uint32_t)(f[c][j] != 0) << j;
+            } else {
+                if constexpr (L::kKeys) {
+                    // the item before each lane's run: the previous lane's
+                    // last, the last lane's of the previous chunk, or vprev
+                    const K up = shfl_up_any(v[c][P - 1], 1);
+                    const K wrap = c > 0 ? shfl_any(v[c > 0 ? c - 1 : 0][P - 1], 31) : vprev;
+                    K prev = lane == 0 ? wrap : up;
+#pragma unroll
+                    for (int j = 0; j < P; ++j) {
+                        bits |= (uint32_t)(v[c][j] != prev) << j;
+                        prev = v[c][j];
+                    }
+                }
+                if constexpr (L::kGroup) {
+                    const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, g[c][P - 1], 1);
+                    const uint32_t wrap = c > 0 ? __shfl_sync(0xFFFFFFFFu, g[c > 0 ? c - 1 : 0][P - 1], 31) : gprev;
+                    uint32_t prev = lane == 0 ? wrap : up;
+#pragma unroll
+                    for (int j = 0; j < P; ++j) {
+                        bits |= (uint32_t)(g[c][j] != prev) << j;
+                        prev = g[c][j];
+                    }
+                }
+                if (p == 0) bits |= 1u;
+            }
+            // positions past n
+            if (p >= n) bits = 0;
+            else if (n - p < (uint64_t)P) bits &= (1u << (uint32_t)(n - p)) - 1u;
+            fl |= bits << (c * P);
+        }
+        // per chunk: the lane's exclusive count within the warp, packed
+        unsigned long long wcnt = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) wcnt |= (unsigned long long)__popc((fl >> (c * P)) & kChunkMask) << (c * FW);
+        unsigned long long incl = wcnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-            if (lane >= o) wi += y;
+            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
         }
-        const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, kScanWarps - 1);
-        if (lane < kScanWarps) s_warp[lane] = wi - wv;
-        uint32_t excl = 0;
-        if (tile == 0) {
-            if (lane == 0) st_volatile_u64(&lookback[0], lb_word(epoch, kFlagInclusive, agg));
-        } else {
-            if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagAggregate, agg));
-            excl = warp_lookback(lookback, tile, epoch, status);
-            if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
-        }
-        if (lane == 0) {
-            s_excl = excl;
-            s_warp[kScanWarps] = agg;
-            if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
-        }
-    }
-    __syncthreads();
-    if (i0 < n) {
-        // 1-based id of the group holding position i0 + k, for every k
-        uint32_t id = s_excl + s_warp[warp] + incl - cnt;
-        if (out_group) {
-            uint32_t o[kScanItems];
+        const unsigned long long tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const unsigned long long excl_l = incl - wcnt;
+        if (lane == 31) {
+            uint32_t wsum = 0;   // the warp's count
 #pragma unroll
-            for (int k = 0; k < kScanItems; ++k) {
-                id += (fl >> k) & 1u;
-                o[k] = id - 1u;
+            for (int c = 0; c < C; ++c) wsum += (uint32_t)((tot >> (c * FW)) & kFieldMask);
+            s_warp[buf][warp] = wsum;
+        }
+        if (threadIdx.x == 0) s_tile[buf ^ 1] = claim;
+        __syncthreads();
+        const uint32_t next = s_tile[buf ^ 1];
+        load(next);
+        if (warp == 0) {
+            uint32_t wv = lane < kScanWarps ? s_warp[buf][lane] : 0u;
+            uint32_t wi = wv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+                if (lane >= o) wi += y;
             }
-            if (VEC && i0 + kScanItems <= n) {
-                uint4 *q = reinterpret_cast<uint4 *>(out_group + i0);
-#pragma unroll
-                for (int w = 0; w < kScanItems / 4; ++w) q[w] = make_uint4(o[4 * w], o[4 * w + 1], o[4 * w + 2], o[4 * w + 3]);
+            const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, kScanWarps - 1);
+            if (lane < kScanWarps) s_warp[buf][lane] = wi - wv;
+            uint32_t excl = 0;
+            if (tile == 0) {
+                if (lane == 0) st_volatile_u64(&lookback[0], lb_word(epoch, kFlagInclusive, agg));
             } else {
+                if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagAggregate, agg));
+                excl = warp_lookback(lookback, tile, epoch, status);
+                if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
+            }
+            if (lane == 0) {
+                s_excl[buf] = excl;
+                s_warp[buf][kScanWarps] = agg;
+                if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
+            }
+        }
+        __syncthreads();
+        // groups started before the chunk's run: before the warp, in the
+        // warp's earlier chunks, in this chunk's earlier lanes
+        uint32_t first = s_excl[buf] + s_warp[buf][warp];
 #pragma unroll
-                for (int k = 0; k < kScanItems; ++k)
-                    if (i0 + k < n) out_group[i0 + k] = o[k];
+        for (int c = 0; c < C; ++c) {
+            const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+            const uint32_t cfirst = first + (uint32_t)((excl_l >> (c * FW)) & kFieldMask);
+            first += (uint32_t)((tot >> (c * FW)) & kFieldMask);
+            if (p >= n) continue;
+            const uint32_t bits = (fl >> (c * P)) & kChunkMask;
+            if (out_group) {
+                // 1-based id of the group holding position p + j, minus one
+                uint32_t o[P];
+                uint32_t id = cfirst;
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    id += (bits >> j) & 1u;
+                    o[j] = id - 1u;
+                }
+                if (VEC && p + P <= n) {
+                    if constexpr (P == 2) {
+                        *reinterpret_cast<uint2 *>(out_group + p) = make_uint2(o[0], o[1]);
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < P / 4; ++w)
+                            reinterpret_cast<uint4 *>(out_group + p)[w] =
+                                make_uint4(o[4 * w], o[4 * w + 1], o[4 * w + 2], o[4 * w + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < P; ++j)
+                        if (p + j < n) out_group[p + j] = o[j];
+                }
+            }
+            if (seg_start) {
+                uint32_t sid = cfirst;
+                for (uint32_t m = bits; m; m &= m - 1) seg_start[sid++] = (uint32_t)(p + (__ffs(m) - 1));
             }
         }
-        if (seg_start) {
-            uint32_t sid = s_excl + s_warp[warp] + incl - cnt;
-            for (uint32_t m = fl; m; m &= m - 1) {
-                const uint32_t k = __ffs(m) - 1;
-                seg_start[sid++] = (uint32_t)(i0 + k);
-            }
+        if (seg_start && base + kScanTile >= n && threadIdx.x == 0) {
+            // the end sentinel after the last segment
+            seg_start[s_excl[buf] + s_warp[buf][kScanWarps]] = (uint32_t)n;
         }
-    }
-    if (seg_start && base + kScanTile >= n && threadIdx.x == 0) {
-        // the end sentinel after the last segment
-        seg_start[s_excl + s_warp[kScanWarps]] = (uint32_t)n;
+        tile = next;
+        buf ^= 1;
     }
 }
 
-// Launches the scan, with 16-byte vector accesses when every array allows.
+// Resident blocks of a scan kernel on this device (the persistent grid).
+template <typename F>
+unsigned scan_grid(F *kernel, uint64_t tiles)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kScanThreads, 0);
+    const uint64_t resident = (uint64_t)std::max(sms, 1) * (uint64_t)std::max(per_sm, 1);
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, resident));
+}
+
+template <typename K, int MODE, bool VEC>
+void launch_scan_mode(cudaStream_t st, const K *keys, const uint32_t *in_group, const uint8_t *flags,
+                      uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_counter,
+                      unsigned long long *lookback, uint32_t epoch, uint32_t *d_count, int *status)
+{
+    auto *kern = boundary_scan_kernel<K, MODE, VEC>;
+    const unsigned grid = scan_grid(kern, (n + kScanTile - 1) / kScanTile);
+    launch_k(kern, grid, kScanThreads, 0, st, keys, in_group, flags, out_group, seg_start, n, tile_counter,
+             lookback, epoch, d_count, status);
+}
+
+// Launches the scan for what it reads, with 16-byte vector accesses when
+// every array allows.
 template <typename K>
-void launch_scan(unsigned grid, cudaStream_t st, const K *keys, const uint32_t *in_group, const uint8_t *flags,
+void launch_scan(cudaStream_t st, const K *keys, const uint32_t *in_group, const uint8_t *flags,
                  uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_counter,
                  unsigned long long *lookback, uint32_t epoch, uint32_t *d_count, int *status)
 {
     const bool vec = (((uintptr_t)keys | (uintptr_t)in_group | (uintptr_t)flags | (uintptr_t)out_group) & 15u) == 0;
-    if (vec)
-        launch_k(boundary_scan_kernel<K, true>, grid, kScanThreads, 0, st,
-                 keys, in_group, flags, out_group, seg_start, n,
-                                                                      tile_counter, lookback, epoch, d_count, status);
-    else
-        launch_k(boundary_scan_kernel<K, false>, grid, kScanThreads, 0, st,
-                 keys, in_group, flags, out_group, seg_start, n,
-                                                                       tile_counter, lookback, epoch, d_count, status);
+    const int mode = flags ? kScanFlags : (keys ? kScanKeys : 0) | (in_group ? kScanGroup : 0);
+#define FMCS_SCAN_MODE(M)                                                                                      \
+    (vec ? launch_scan_mode<K, M, true>(st, keys, in_group, flags, out_group, seg_start, n, tile_counter,     \
+                                        lookback, epoch, d_count, status)                                    \
+         : launch_scan_mode<K, M, false>(st, keys, in_group, flags, out_group, seg_start, n, tile_counter,    \
+                                         lookback, epoch, d_count, status))
+    switch (mode) {
+    case kScanKeys: FMCS_SCAN_MODE(kScanKeys); break;
+    case kScanKeysGroup: FMCS_SCAN_MODE(kScanKeysGroup); break;
+    case kScanFlags: FMCS_SCAN_MODE(kScanFlags); break;
+    case kScanGroup: FMCS_SCAN_MODE(kScanGroup); break;
+    default: FMCS_SCAN_MODE(0); break;   // nothing to compare: one group
+    }
+#undef FMCS_SCAN_MODE
 }
 
 int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const uint32_t *in_group,
@@ -220,28 +366,27 @@ int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const
     uint32_t *tile_counter = (uint32_t *)cnt;  // word 0 of the counters slot
     cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), ctx->stream);
     const uint32_t epoch = ctx->epoch++;
-    const unsigned grid = (unsigned)tiles;
     unsigned long long *lbw = (unsigned long long *)lb;
     LaunchScope ls_(ctx, "boundary_scan");
     switch (keys ? key_bytes : 0) {
     case 0:
-        launch_scan<uint32_t>(grid, ctx->stream, nullptr, in_group, flags, out_group, seg_start, n, tile_counter, lbw,
+        launch_scan<uint32_t>(ctx->stream, nullptr, in_group, flags, out_group, seg_start, n, tile_counter, lbw,
                               epoch, d_count, ctx->d_status);
         break;
     case 1:
-        launch_scan<uint8_t>(grid, ctx->stream, (const uint8_t *)keys, in_group, flags, out_group, seg_start, n,
+        launch_scan<uint8_t>(ctx->stream, (const uint8_t *)keys, in_group, flags, out_group, seg_start, n,
                              tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     case 2:
-        launch_scan<uint16_t>(grid, ctx->stream, (const uint16_t *)keys, in_group, flags, out_group, seg_start, n,
+        launch_scan<uint16_t>(ctx->stream, (const uint16_t *)keys, in_group, flags, out_group, seg_start, n,
                               tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     case 4:
-        launch_scan<uint32_t>(grid, ctx->stream, (const uint32_t *)keys, in_group, flags, out_group, seg_start, n,
+        launch_scan<uint32_t>(ctx->stream, (const uint32_t *)keys, in_group, flags, out_group, seg_start, n,
                               tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     case 8:
-        launch_scan<uint64_t>(grid, ctx->stream, (const uint64_t *)keys, in_group, flags, out_group, seg_start, n,
+        launch_scan<uint64_t>(ctx->stream, (const uint64_t *)keys, in_group, flags, out_group, seg_start, n,
                               tile_counter, lbw, epoch, d_count, ctx->d_status);
         break;
     default:
@@ -384,22 +529,21 @@ extern "C" int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t k
     if (e == cudaSuccess) e = cudaMemsetAsync(tile_counter, 0, 3 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return FMCS_E_CUDA;
     const uint32_t epoch = 1;
-    const unsigned grid = (unsigned)tiles;
     switch (key_bytes) {
     case 1:
-        launch_scan<uint8_t>(grid, st, (const uint8_t *)keys, in_group, nullptr, out_group, nullptr, n,
+        launch_scan<uint8_t>(st, (const uint8_t *)keys, in_group, nullptr, out_group, nullptr, n,
                              tile_counter, lookback, epoch, d_count, status);
         break;
     case 2:
-        launch_scan<uint16_t>(grid, st, (const uint16_t *)keys, in_group, nullptr, out_group, nullptr, n,
+        launch_scan<uint16_t>(st, (const uint16_t *)keys, in_group, nullptr, out_group, nullptr, n,
                               tile_counter, lookback, epoch, d_count, status);
         break;
     case 4:
-        launch_scan<uint32_t>(grid, st, (const uint32_t *)keys, in_group, nullptr, out_group, nullptr, n,
+        launch_scan<uint32_t>(st, (const uint32_t *)keys, in_group, nullptr, out_group, nullptr, n,
                               tile_counter, lookback, epoch, d_count, status);
         break;
     default:
-        launch_scan<uint64_t>(grid, st, (const uint64_t *)keys, in_group, nullptr, out_group, nullptr, n,
+        launch_scan<uint64_t>(st, (const uint64_t *)keys, in_group, nullptr, out_group, nullptr, n,
                               tile_counter, lookback, epoch, d_count, status);
         break;
     }

@@ -687,57 +687,97 @@ struct BucketSmem {
     uint32_t maxb;
 };
 
-// Exclusive scan of off[0, nb) by the block, also leaving the largest count
-// in *maxb.  Warp w scans its own run of 32-bin rows (lanes read consecutive
-// bins: no bank conflicts), then the warps' totals are scanned and added.
-template <int NT>
-__device__ __forceinline__ void block_scan_bins(uint32_t *off, uint32_t nb, uint32_t *tmp, uint32_t *maxb)
+// Exclusive scan of off[0, nb) by the block (nb a power of two, at most
+// NT * IT, so at most 16 * NT), also leaving the largest count in *maxb.  Thread t scans its own
+// run of PER = nb / NT consecutive bins (one bin each for the first nb
+// threads when nb < NT), read as vectors and summed, then, after the runs'
+// totals are scanned across the block, read again and written back as
+// exclusive offsets (the run is not held in registers across the barriers).
+template <int NT, int PER>
+__device__ __forceinline__ void scan_bin_runs(uint32_t *off, uint32_t nb, uint32_t *tmp, uint32_t *maxb)
 {
     constexpr int NW = NT / 32;
+    constexpr int VW = PER >= 4 ? 4 : PER;   // words per vector access
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const uint32_t rows = (nb + 31) / 32;
-    const uint32_t rpw = (rows + NW - 1) / NW;
-    const uint32_t r0 = warp * rpw, r1 = min(rows, r0 + rpw);
-    uint32_t carry = 0, mx = 0;
-    for (uint32_t r = r0; r < r1; ++r) {
-        const uint32_t i = r * 32 + lane;
-        const uint32_t v = i < nb ? off[i] : 0u;
-        uint32_t incl = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += y;
+    const uint32_t b0 = threadIdx.x * PER;
+    const bool mine = b0 < nb;
+    auto ld = [&](int q, uint32_t (&x)[VW]) {
+        if constexpr (VW == 4) {
+            const uint4 w = reinterpret_cast<const uint4 *>(off + b0)[q];
+            x[0] = w.x; x[1] = w.y; x[2] = w.z; x[3] = w.w;
+        } else if constexpr (VW == 2) {
+            const uint2 w = reinterpret_cast<const uint2 *>(off + b0)[q];
+            x[0] = w.x; x[1] = w.y;
+        } else {
+            x[0] = off[b0 + q];
         }
-        if (i < nb) off[i] = carry + incl - v;
-        carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
-        mx = max(mx, v);
+    };
+    uint32_t sum = 0, mx = 0;
+    if (mine) {
+#pragma unroll
+        for (int q = 0; q < PER / VW; ++q) {
+            uint32_t x[VW];
+            ld(q, x);
+#pragma unroll
+            for (int i = 0; i < VW; ++i) {
+                sum += x[i];
+                mx = max(mx, x[i]);
+            }
+        }
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-    if (lane == 0) {
-        tmp[warp] = carry;
-        atomicMax(maxb, mx);
-    }
+    if (lane == 31) tmp[warp] = incl;
+    if (lane == 0 && mx) atomicMax(maxb, mx);
     __syncthreads();
     if (warp == 0) {
-        const uint32_t v = lane < NW ? tmp[lane] : 0u;
-        uint32_t incl = v;
+        const uint32_t w = lane < NW ? tmp[lane] : 0u;
+        uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += y;
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= o) wi += y;
         }
-        if (lane < NW) tmp[lane] = incl - v;
+        if (lane < NW) tmp[lane] = wi - w;
     }
     __syncthreads();
-    const uint32_t add = tmp[warp];
-    if (add)
-        for (uint32_t r = r0; r < r1; ++r) {
-            const uint32_t i = r * 32 + lane;
-            if (i < nb) off[i] += add;
+    if (mine) {
+        uint32_t run = tmp[warp] + incl - sum;
+#pragma unroll
+        for (int q = 0; q < PER / VW; ++q) {
+            uint32_t x[VW];
+            ld(q, x);
+#pragma unroll
+            for (int i = 0; i < VW; ++i) {
+                const uint32_t c = x[i];
+                x[i] = run;
+                run += c;
+            }
+            if constexpr (VW == 4) reinterpret_cast<uint4 *>(off + b0)[q] = make_uint4(x[0], x[1], x[2], x[3]);
+            else if constexpr (VW == 2) reinterpret_cast<uint2 *>(off + b0)[q] = make_uint2(x[0], x[1]);
+            else off[b0 + q] = x[0];
         }
+    }
     __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ void block_scan_bins(uint32_t *off, uint32_t nb, uint32_t *tmp, uint32_t *maxb)
+{
+    switch (nb >= (uint32_t)NT ? nb / NT : 1u) {
+    case 1: scan_bin_runs<NT, 1>(off, nb, tmp, maxb); break;
+    case 2: scan_bin_runs<NT, 2>(off, nb, tmp, maxb); break;
+    case 4: scan_bin_runs<NT, 4>(off, nb, tmp, maxb); break;
+    case 8: scan_bin_runs<NT, 8>(off, nb, tmp, maxb); break;
+    default: scan_bin_runs<NT, 16>(off, nb, tmp, maxb); break;
+    }
 }
 
 // The fast path above.  Rows are in registers (warp w holds positions
@@ -749,10 +789,10 @@ __device__ __forceinline__ void block_scan_bins(uint32_t *off, uint32_t nb, uint
 // every row), shifted left by nbits with the row's position in the low
 // nbits when they fit in 64 bits, so that compound keys are all distinct and
 // compare like (key, position).  Otherwise the position is kept beside it.
-// A row's bucket is the top `width` bits of its compound key; its final place
-// is its bucket's start plus the rows of the bucket with a smaller compound
-// key, found by scanning the neighbouring slots while they hold the same
-// bucket (buckets hold about one row).
+// A row's bucket is the top `width` bits of its compound key (about one row
+// per bucket); its final place is its bucket's start plus the rows of the
+// bucket with a smaller compound key.  A row alone in its bucket is in its
+// place without comparisons.
 template <typename K, int NT, int IT>
 __device__ __forceinline__ bool bucket_rank_sort(BucketSmem<K, NT, IT> &sm, const K (&key)[IT],
                                                  const uint32_t (&val)[IT], uint32_t steps, uint32_t wbase,

@@ -1,0 +1,66 @@
+"""The group-boundary scan (dense group ids of sorted keys, optionally within
+the runs of a previous round's group ids) on every key width, at sizes on
+and around the kernel's chunk and tile edges, with 16-byte-aligned and
+misaligned arrays (vector and scalar loads).
+
+Called through fmcs_group_ids_noalloc, which runs the same scan kernel as a
+sort round; the expected ids are the oracle's (extractGroupInfo,
+src/composer.cpp:630-678, restated in oracle/fmcs_oracle.c) for keys that are
+already in order, so that its stable sort leaves them in place.  Integer ids:
+the comparison is exact."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 2, 33, 1000, 8191, 8192, 8193, 70_001, 1_000_003]
+
+
+def _as_int(a):
+    return a.view({1: np.int8, 2: np.int16, 4: np.int32, 8: np.int64}[a.dtype.itemsize])
+
+
+def _case(n, dtype, segmented, seed):
+    """Keys in order within each run of in_group (or overall), with repeats."""
+    rng = np.random.default_rng(seed)
+    hi = min(int(np.iinfo(dtype).max), max(2, n // 8))
+    keys = rng.integers(0, hi, size=n, dtype=np.uint64).astype(dtype)
+    ig = None
+    if segmented:
+        starts = np.zeros(n, np.uint32)
+        starts[rng.integers(0, n, size=max(1, n // 500))] = 1
+        starts[0] = 0
+        ig = np.cumsum(starts).astype(np.uint32)
+        keys = keys[np.lexsort((keys, ig))]
+    else:
+        keys = np.sort(keys)
+    return keys, ig
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.uint32, np.uint64])
+@pytest.mark.parametrize("segmented", [False, True])
+@pytest.mark.parametrize("misaligned", [False, True])
+def test_boundary_scan_matches_oracle(dtype, segmented, misaligned):
+    torch = pytest.importorskip("torch")
+    from fastmulticolsort_b200 import capi
+
+    def dev(a):
+        # a misaligned view starts one element into its buffer, so that its
+        # address is not 16-byte aligned (the scalar-load path)
+        if not misaligned:
+            return torch.from_numpy(_as_int(a)).cuda()
+        return torch.from_numpy(_as_int(np.concatenate([a[:1], a]))).cuda()[1:]
+
+    for n in SIZES:
+        keys, ig = _case(n, dtype, segmented, seed=n * 7 + np.dtype(dtype).itemsize)
+        _, g_ref, _, ng_ref = O.sort_round(keys, order=np.arange(n, dtype=np.uint32), in_group=ig)
+        kd = dev(keys)
+        igd = None if ig is None else dev(ig)
+        outv = dev(np.full(n, 0xFFFFFFFF, np.uint32))
+        ng = capi.group_ids_noalloc(kd, outv, in_group=igd)
+        torch.cuda.synchronize()
+        got = outv.cpu().numpy().view(np.uint32)
+        assert ng == ng_ref, (n, ng, ng_ref)
+        assert np.array_equal(got, g_ref), n
