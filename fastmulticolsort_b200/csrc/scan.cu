@@ -63,29 +63,6 @@ __device__ __forceinline__ T shfl_any(T v, int src)
     else return (T)__shfl_sync(0xFFFFFFFFu, (uint32_t)v, src);
 }
 
-// Decoupled look-back by one warp: each lane reads one predecessor's word
-// (bounded waits), and the warp adds the aggregates back to the nearest
-// inclusive prefix.  Returns the exclusive prefix of `tile` (every lane).
-__device__ __forceinline__ uint32_t warp_lookback(unsigned long long *lookback, uint32_t tile, uint32_t epoch,
-                                                  int *status)
-{
-    const int lane = threadIdx.x & 31;
-    uint32_t excl = 0;
-    int64_t last = (int64_t)tile - 1;   // the window is tiles last - lane
-    for (;;) {
-        const int64_t p = last - lane;
-        const unsigned long long w = p >= 0 ? lb_wait(&lookback[p], epoch, status) : lb_word(epoch, kFlagInclusive, 0);
-        const uint32_t inc = __ballot_sync(0xFFFFFFFFu, ((uint32_t)(w >> 32) & 3u) == kFlagInclusive);
-        const int first = inc ? __ffs(inc) - 1 : 32;   // nearest inclusive predecessor
-        uint32_t v = lane <= first ? (uint32_t)w : 0u;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        excl += v;
-        if (inc) return excl;
-        last -= 32;
-    }
-}
-
 // What the scan reads: sorted keys, the previous round's group ids, both, or
 // precomputed boundary flags.
 enum ScanMode { kScanKeys = 1, kScanGroup = 2, kScanKeysGroup = 3, kScanFlags = 4 };
@@ -110,11 +87,44 @@ struct ScanLayout {
     static_assert(C * FW <= 64, "packed chunk counts");
 };
 
+// Decoupled look-back by the whole block: each round thread i reads the word
+// of tile last - i (kScanThreads predecessors per round trip), and the block
+// adds the aggregates back to the nearest inclusive prefix.  Returns the
+// exclusive prefix of `tile` in every thread.  Ends with a block barrier.
+__device__ __forceinline__ uint32_t block_lookback(unsigned long long *lookback, uint32_t tile, uint32_t epoch,
+                                                   int *status, uint32_t *s_first, uint32_t *s_sum)
+{
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    uint32_t excl = 0;
+    int64_t last = (int64_t)tile - 1;
+    for (;;) {
+        const int64_t p = last - threadIdx.x;
+        const unsigned long long w = p >= 0 ? lb_wait(&lookback[p], epoch, status) : lb_word(epoch, kFlagInclusive, 0);
+        const uint32_t inc = __ballot_sync(0xFFFFFFFFu, ((uint32_t)(w >> 32) & 3u) == kFlagInclusive);
+        if (lane == 0) s_first[warp] = inc ? (uint32_t)(warp * 32 + __ffs(inc) - 1) : 0xFFFFFFFFu;
+        __syncthreads();
+        uint32_t first = 0xFFFFFFFFu;   // the nearest inclusive predecessor's thread
+#pragma unroll
+        for (int i = 0; i < kScanWarps; ++i) first = min(first, s_first[i]);
+        uint32_t v = threadIdx.x <= first ? (uint32_t)w : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        if (lane == 0) s_sum[warp] = v;
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kScanWarps; ++i) excl += s_sum[i];
+        __syncthreads();   // s_first and s_sum are read before they are written again
+        if (first != 0xFFFFFFFFu) return excl;
+        last -= kScanThreads;
+    }
+}
+
 // Persistent blocks (as many as are resident); each claims tiles of
-// kScanTile positions in order from the tile counter.  Once a tile's boundary
-// flags are known its rows are no longer needed, so the block claims its next
-// tile and issues that tile's loads before the look-back: the look-back's
-// waits and the next loads overlap.
+// kScanTile positions in order from the tile counter, one at a time.  A
+// tile's aggregate is published as soon as its flags are counted, and its
+// exclusive prefix comes from a block-wide look-back: the other resident
+// tiles are at most one round trip of predecessors away.
 template <typename K, int MODE, bool VEC>
 __global__ void __launch_bounds__(kScanThreads, 2)
 boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group,
@@ -127,85 +137,77 @@ boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in
     constexpr int P = L::P, C = L::C, FW = L::FW;
     constexpr uint32_t kChunkMask = (1u << P) - 1u;
     constexpr unsigned long long kFieldMask = (1ull << FW) - 1ull;
-    // double-buffered per tile, so that one tile's readers and the next
-    // tile's writers need no barrier between them
-    __shared__ uint32_t s_tile[2];
-    __shared__ uint32_t s_warp[2][kScanWarps + 1];
-    __shared__ uint32_t s_excl[2];
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp[kScanWarps + 1];
+    __shared__ uint32_t s_first[kScanWarps], s_sum[kScanWarps];
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
 
-    K v[C][P];
-    K vprev = K(0);        // lane 0: the key before the warp's first position
-    uint32_t g[C][P];
-    uint32_t gprev = 0;
-    uint8_t f[C][P];
-    auto load = [&](uint32_t tile) {
-        const uint64_t wb = (uint64_t)tile * kScanTile + (uint64_t)warp * (32 * kScanItems);
-        if (tile >= tiles || wb >= n) return;
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
-            if constexpr (L::kKeys) load_chunk<K, P, VEC>(keys, p, n, v[c]);
-            if constexpr (L::kGroup) load_chunk<uint32_t, P, VEC>(in_group, p, n, g[c]);
-            if constexpr (L::kFlags) load_chunk<uint8_t, P, VEC>(flags, p, n, f[c]);
-        }
-        if (lane == 0 && wb > 0) {
-            if constexpr (L::kKeys) vprev = keys[wb - 1];
-            if constexpr (L::kGroup) gprev = in_group[wb - 1];
-        }
-    };
-
-    if (threadIdx.x == 0) s_tile[0] = atomicAdd(tile_counter, 1u);
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
-    uint32_t tile = s_tile[0];
-    load(tile);
-    int buf = 0;
+    uint32_t tile = s_tile;
     while (tile < tiles) {
         const uint64_t base = (uint64_t)tile * kScanTile;
         const uint64_t wb = base + (uint64_t)warp * (32 * kScanItems);
-        uint32_t claim = 0;
-        if (threadIdx.x == 0) claim = atomicAdd(tile_counter, 1u);
         // boundary flags, bit c * P + j = position wb + c * 32 * P + lane * P + j
         uint32_t fl = 0;
+        if (wb < n) {
+            K v[C][P];
+            K vprev = K(0);        // lane 0: the key before the warp's first position
+            uint32_t g[C][P];
+            uint32_t gprev = 0;
+            uint8_t f[C][P];
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
-            uint32_t bits = 0;
-            if constexpr (L::kFlags) {
-#pragma unroll
-                for (int j = 0; j < P; ++j) bits |= (uint32_t)(f[c][j] != 0) << j;
-            } else {
-                if constexpr (L::kKeys) {
-                    // the item before each lane's run: the previous lane's
-                    // last, the last lane's of the previous chunk, or vprev
-                    const K up = shfl_up_any(v[c][P - 1], 1);
-                    const K wrap = c > 0 ? shfl_any(v[c > 0 ? c - 1 : 0][P - 1], 31) : vprev;
-                    K prev = lane == 0 ? wrap : up;
-#pragma unroll
-                    for (int j = 0; j < P; ++j) {
-                        bits |= (uint32_t)(v[c][j] != prev) << j;
-                        prev = v[c][j];
-                    }
-                }
-                if constexpr (L::kGroup) {
-                    const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, g[c][P - 1], 1);
-                    const uint32_t wrap = c > 0 ? __shfl_sync(0xFFFFFFFFu, g[c > 0 ? c - 1 : 0][P - 1], 31) : gprev;
-                    uint32_t prev = lane == 0 ? wrap : up;
-#pragma unroll
-                    for (int j = 0; j < P; ++j) {
-                        bits |= (uint32_t)(g[c][j] != prev) << j;
-                        prev = g[c][j];
-                    }
-                }
-                if (p == 0) bits |= 1u;
+            for (int c = 0; c < C; ++c) {
+                const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+                if constexpr (L::kKeys) load_chunk<K, P, VEC>(keys, p, n, v[c]);
+                if constexpr (L::kGroup) load_chunk<uint32_t, P, VEC>(in_group, p, n, g[c]);
+                if constexpr (L::kFlags) load_chunk<uint8_t, P, VEC>(flags, p, n, f[c]);
             }
-            // positions past n
-            if (p >= n) bits = 0;
-            else if (n - p < (uint64_t)P) bits &= (1u << (uint32_t)(n - p)) - 1u;
-            fl |= bits << (c * P);
+            if (lane == 0 && wb > 0) {
+                if constexpr (L::kKeys) vprev = keys[wb - 1];
+                if constexpr (L::kGroup) gprev = in_group[wb - 1];
+            }
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+                uint32_t bits = 0;
+                if constexpr (L::kFlags) {
+#pragma unroll
+                    for (int j = 0; j < P; ++j) bits |= (uint32_t)(f[c][j] != 0) << j;
+                } else {
+                    if constexpr (L::kKeys) {
+                        // the item before each lane's run: the previous lane's
+                        // last, the last lane's of the previous chunk, or vprev
+                        const K up = shfl_up_any(v[c][P - 1], 1);
+                        const K wrap = c > 0 ? shfl_any(v[c > 0 ? c - 1 : 0][P - 1], 31) : vprev;
+                        K prev = lane == 0 ? wrap : up;
+#pragma unroll
+                        for (int j = 0; j < P; ++j) {
+                            bits |= (uint32_t)(v[c][j] != prev) << j;
+                            prev = v[c][j];
+                        }
+                    }
+                    if constexpr (L::kGroup) {
+                        const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, g[c][P - 1], 1);
+                        const uint32_t wrap =
+                            c > 0 ? __shfl_sync(0xFFFFFFFFu, g[c > 0 ? c - 1 : 0][P - 1], 31) : gprev;
+                        uint32_t prev = lane == 0 ? wrap : up;
+#pragma unroll
+                        for (int j = 0; j < P; ++j) {
+                            bits |= (uint32_t)(g[c][j] != prev) << j;
+                            prev = g[c][j];
+                        }
+                    }
+                    if (p == 0) bits |= 1u;
+                }
+                // positions past n
+                if (p >= n) bits = 0;
+                else if (n - p < (uint64_t)P) bits &= (1u << (uint32_t)(n - p)) - 1u;
+                fl |= bits << (c * P);
+            }
         }
         // per chunk: the lane's exclusive count within the warp, packed
         unsigned long long wcnt = 0;
@@ -223,14 +225,11 @@ boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in
             uint32_t wsum = 0;   // the warp's count
 #pragma unroll
             for (int c = 0; c < C; ++c) wsum += (uint32_t)((tot >> (c * FW)) & kFieldMask);
-            s_warp[buf][warp] = wsum;
+            s_warp[warp] = wsum;
         }
-        if (threadIdx.x == 0) s_tile[buf ^ 1] = claim;
         __syncthreads();
-        const uint32_t next = s_tile[buf ^ 1];
-        load(next);
         if (warp == 0) {
-            uint32_t wv = lane < kScanWarps ? s_warp[buf][lane] : 0u;
+            const uint32_t wv = lane < kScanWarps ? s_warp[lane] : 0u;
             uint32_t wi = wv;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -238,25 +237,22 @@ boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in
                 if (lane >= o) wi += y;
             }
             const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, kScanWarps - 1);
-            if (lane < kScanWarps) s_warp[buf][lane] = wi - wv;
-            uint32_t excl = 0;
-            if (tile == 0) {
-                if (lane == 0) st_volatile_u64(&lookback[0], lb_word(epoch, kFlagInclusive, agg));
-            } else {
-                if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagAggregate, agg));
-                excl = warp_lookback(lookback, tile, epoch, status);
-                if (lane == 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
-            }
+            if (lane < kScanWarps) s_warp[lane] = wi - wv;
             if (lane == 0) {
-                s_excl[buf] = excl;
-                s_warp[buf][kScanWarps] = agg;
-                if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
+                s_warp[kScanWarps] = agg;
+                st_volatile_u64(&lookback[tile], lb_word(epoch, tile == 0 ? kFlagInclusive : kFlagAggregate, agg));
             }
         }
         __syncthreads();
+        const uint32_t agg = s_warp[kScanWarps];
+        const uint32_t excl = tile == 0 ? 0u : block_lookback(lookback, tile, epoch, status, s_first, s_sum);
+        if (threadIdx.x == 0) {
+            if (tile > 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
+            if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
+        }
         // groups started before the chunk's run: before the warp, in the
         // warp's earlier chunks, in this chunk's earlier lanes
-        uint32_t first = s_excl[buf] + s_warp[buf][warp];
+        uint32_t first = excl + s_warp[warp];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
@@ -295,10 +291,13 @@ boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in
         }
         if (seg_start && base + kScanTile >= n && threadIdx.x == 0) {
             // the end sentinel after the last segment
-            seg_start[s_excl[buf] + s_warp[buf][kScanWarps]] = (uint32_t)n;
+            seg_start[excl + agg] = (uint32_t)n;
         }
-        tile = next;
-        buf ^= 1;
+        // the next tile, once every thread has read this one's shared words
+        if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        tile = s_tile;
+        __syncthreads();   // every thread has read s_tile before it is written again
     }
 }
 
