@@ -688,37 +688,43 @@ struct BucketSmem {
 };
 
 // Exclusive scan of off[0, nb) by the block (nb a power of two, at most
-// NT * IT, so at most 16 * NT), also leaving the largest count in *maxb.  Thread t scans its own
-// run of PER = nb / NT consecutive bins (one bin each for the first nb
-// threads when nb < NT), read as vectors and summed, then, after the runs'
-// totals are scanned across the block, read again and written back as
-// exclusive offsets (the run is not held in registers across the barriers).
+// NT * IT, so at most 16 * NT), also leaving the largest count in *maxb.
+// Thread t scans its own run of PER = nb / NT consecutive bins (one bin each
+// for the first nb threads when nb < NT), read as vectors and summed, then,
+// after the runs' totals are scanned across the block, read again and written
+// back as exclusive offsets (the run is not held in registers across the
+// barriers).  A run of NV > 1 16-byte vectors is visited starting at vector
+// (t * PER / 32) mod NV, so that the 8 threads of a shared-memory wavefront
+// touch 8 different bank groups instead of 2 to 4.
 template <int NT, int PER>
 __device__ __forceinline__ void scan_bin_runs(uint32_t *off, uint32_t nb, uint32_t *tmp, uint32_t *maxb)
 {
     constexpr int NW = NT / 32;
     constexpr int VW = PER >= 4 ? 4 : PER;   // words per vector access
+    constexpr int NV = PER / VW;             // vectors per run
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const uint32_t b0 = threadIdx.x * PER;
     const bool mine = b0 < nb;
-    auto ld = [&](int q, uint32_t (&x)[VW]) {
+    const uint32_t rot = NV > 1 ? (threadIdx.x * PER / 32) : 0u;
+    auto vec_of = [&](int q) -> uint32_t { return ((uint32_t)q + rot) & (uint32_t)(NV - 1); };
+    auto ld = [&](uint32_t v, uint32_t (&x)[VW]) {
         if constexpr (VW == 4) {
-            const uint4 w = reinterpret_cast<const uint4 *>(off + b0)[q];
+            const uint4 w = reinterpret_cast<const uint4 *>(off + b0)[v];
             x[0] = w.x; x[1] = w.y; x[2] = w.z; x[3] = w.w;
         } else if constexpr (VW == 2) {
-            const uint2 w = reinterpret_cast<const uint2 *>(off + b0)[q];
+            const uint2 w = reinterpret_cast<const uint2 *>(off + b0)[v];
             x[0] = w.x; x[1] = w.y;
         } else {
-            x[0] = off[b0 + q];
+            x[0] = off[b0 + v];
         }
     };
     uint32_t sum = 0, mx = 0;
     if (mine) {
 #pragma unroll
-        for (int q = 0; q < PER / VW; ++q) {
+        for (int q = 0; q < NV; ++q) {
             uint32_t x[VW];
-            ld(q, x);
+            ld(vec_of(q), x);
 #pragma unroll
             for (int i = 0; i < VW; ++i) {
                 sum += x[i];
@@ -749,20 +755,32 @@ __device__ __forceinline__ void scan_bin_runs(uint32_t *off, uint32_t nb, uint32
     }
     __syncthreads();
     if (mine) {
-        uint32_t run = tmp[warp] + incl - sum;
+        const uint32_t run = tmp[warp] + incl - sum;
+        // the run's vectors in visiting order, with their sums
+        uint32_t x[NV][VW], vs[NV];
 #pragma unroll
-        for (int q = 0; q < PER / VW; ++q) {
-            uint32_t x[VW];
-            ld(q, x);
+        for (int q = 0; q < NV; ++q) {
+            ld(vec_of(q), x[q]);
+            vs[q] = 0;
+#pragma unroll
+            for (int i = 0; i < VW; ++i) vs[q] += x[q][i];
+        }
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            // the vector's first offset: the run's plus every vector before it
+            uint32_t r = run;
+#pragma unroll
+            for (int u = 0; u < NV; ++u) r += vec_of(u) < vec_of(q) ? vs[u] : 0u;
 #pragma unroll
             for (int i = 0; i < VW; ++i) {
-                const uint32_t c = x[i];
-                x[i] = run;
-                run += c;
+                const uint32_t c = x[q][i];
+                x[q][i] = r;
+                r += c;
             }
-            if constexpr (VW == 4) reinterpret_cast<uint4 *>(off + b0)[q] = make_uint4(x[0], x[1], x[2], x[3]);
-            else if constexpr (VW == 2) reinterpret_cast<uint2 *>(off + b0)[q] = make_uint2(x[0], x[1]);
-            else off[b0 + q] = x[0];
+            const uint32_t v = vec_of(q);
+            if constexpr (VW == 4) reinterpret_cast<uint4 *>(off + b0)[v] = make_uint4(x[q][0], x[q][1], x[q][2], x[q][3]);
+            else if constexpr (VW == 2) reinterpret_cast<uint2 *>(off + b0)[v] = make_uint2(x[q][0], x[q][1]);
+            else off[b0 + v] = x[q][0];
         }
     }
     __syncthreads();
