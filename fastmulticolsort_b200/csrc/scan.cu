@@ -1,13 +1,18 @@
-// scan.cu -- (d) group-boundary scan and segment extraction, one pass each.
+// scan.cu -- (d) group-boundary scan and segment extraction.
 //
 // Reference: Composer::extractGroupInfo<T> (src/composer.cpp:630-678) computes
 //   g[0] = 0;  g[i] = g[i-1] + (v[i] != v[i-1] || in[i] != in[i-1])
-// with a scalar loop.  Here one kernel reads each key (and in_group word) once:
-// adjacent difference -> warp ballot -> popc prefix -> block scan -> decoupled
-// look-back across tiles (bounded waits) -> dense ids.  The same kernel, given
-// only in_group, emits the start position of every run of equal in_group (the
-// segments that the next round sorts; the reference finds them with a scalar
-// walk, src/composer.cpp:1280-1335).
+// with a scalar loop.  Here, in three launches with no waits between blocks:
+// (1) every tile of 8192 positions counts its group starts (adjacent
+// difference -> per-lane bit masks -> popc) and stores the masks (2 bytes per
+// 16 rows), (2) one block scans the tile counts, (3) every tile reads its
+// masks back and writes dense ids from its prefix (warp and block scans inside
+// the tile).  The keys are read once.  (The allocation-free entry point has no
+// room for the masks: its pass 3 recomputes them from the keys, last tile
+// first, so that the keys (1) read last are still in L2.)  The same kernels, given only in_group,
+// emit the start position of every run of equal in_group (the segments that
+// the next round sorts; the reference finds them with a scalar walk,
+// src/composer.cpp:1280-1335).
 #include "device_common.cuh"
 #include "fmcs_internal.h"
 
@@ -18,7 +23,7 @@ namespace fmcs {
 
 namespace {
 
-constexpr int kScanThreads = 512;              // a tile of 8192 positions: half as many look-back steps
+constexpr int kScanThreads = 512;              // a tile of 8192 positions
 constexpr int kScanItems = 16;                  // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kScanWarps = kScanThreads / 32;
@@ -87,257 +92,270 @@ struct ScanLayout {
     static_assert(C * FW <= 64, "packed chunk counts");
 };
 
-// Decoupled look-back by the whole block: each round thread i reads the word
-// of tile last - i (kScanThreads predecessors per round trip), and the block
-// adds the aggregates back to the nearest inclusive prefix.  Returns the
-// exclusive prefix of `tile` in every thread.  Ends with a block barrier.
-__device__ __forceinline__ uint32_t block_lookback(unsigned long long *lookback, uint32_t tile, uint32_t epoch,
-                                                   int *status, uint32_t *s_first, uint32_t *s_sum)
+// The boundary flags of one lane's rows: bit c * P + j is set when position
+// wb + c * 32 * P + lane * P + j starts a group (its key or in_group differs
+// from the previous position's, or it is position 0; or its flag is set).
+// wb is the first position of the calling warp's 32 * kScanItems.  The whole
+// warp calls it.
+template <typename K, int MODE, bool VEC>
+__device__ __forceinline__ uint32_t lane_flags(const K *__restrict__ keys, const uint32_t *__restrict__ in_group,
+                                               const uint8_t *__restrict__ flags, uint64_t n, uint64_t wb, int lane)
 {
+    using L = ScanLayout<K, MODE>;
+    constexpr int P = L::P, C = L::C;
+    uint32_t fl = 0;
+    if (wb >= n) return 0;   // warp-uniform
+    K v[C][P];
+    K vprev = K(0);        // lane 0: the key before the warp's first position
+    uint32_t g[C][P];
+    uint32_t gprev = 0;
+    uint8_t f[C][P];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+        if constexpr (L::kKeys) load_chunk<K, P, VEC>(keys, p, n, v[c]);
+        if constexpr (L::kGroup) load_chunk<uint32_t, P, VEC>(in_group, p, n, g[c]);
+        if constexpr (L::kFlags) load_chunk<uint8_t, P, VEC>(flags, p, n, f[c]);
+    }
+    if (lane == 0 && wb > 0) {
+        if constexpr (L::kKeys) vprev = keys[wb - 1];
+        if constexpr (L::kGroup) gprev = in_group[wb - 1];
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+        uint32_t bits = 0;
+        if constexpr (L::kFlags) {
+#pragma unroll
+            for (int j = 0; j < P; ++j) bits |= (uint32_t)(f[c][j] != 0) << j;
+        } else {
+            if constexpr (L::kKeys) {
+                // the item before each lane's run: the previous lane's last,
+                // the last lane's of the previous chunk, or vprev
+                const K up = shfl_up_any(v[c][P - 1], 1);
+                const K wrap = c > 0 ? shfl_any(v[c > 0 ? c - 1 : 0][P - 1], 31) : vprev;
+                K prev = lane == 0 ? wrap : up;
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    bits |= (uint32_t)(v[c][j] != prev) << j;
+                    prev = v[c][j];
+                }
+            }
+            if constexpr (L::kGroup) {
+                const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, g[c][P - 1], 1);
+                const uint32_t wrap = c > 0 ? __shfl_sync(0xFFFFFFFFu, g[c > 0 ? c - 1 : 0][P - 1], 31) : gprev;
+                uint32_t prev = lane == 0 ? wrap : up;
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    bits |= (uint32_t)(g[c][j] != prev) << j;
+                    prev = g[c][j];
+                }
+            }
+            if (p == 0) bits |= 1u;
+        }
+        // positions past n
+        if (p >= n) bits = 0;
+        else if (n - p < (uint64_t)P) bits &= (1u << (uint32_t)(n - p)) - 1u;
+        fl |= bits << (c * P);
+    }
+    return fl;
+}
+
+// Pass 1: the number of group starts in every tile of kScanTile positions
+// (one block per tile; the keys stream through once).  With `masks`, each
+// thread also stores its 16-bit boundary mask (2 bytes per 16 rows), so that
+// pass 3 need not read the keys again.
+template <typename K, int MODE, bool VEC>
+__global__ void __launch_bounds__(kScanThreads, 2)
+scan_count_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group, const uint8_t *__restrict__ flags,
+                  uint64_t n, uint32_t *__restrict__ tile_count, uint16_t *__restrict__ masks)
+{
+    kernel_prologue();
+    static_assert(kScanItems == 16, "one 16-bit mask per thread");
+    __shared__ uint32_t s_warp[kScanWarps];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    uint32_t excl = 0;
-    int64_t last = (int64_t)tile - 1;
-    for (;;) {
-        const int64_t p = last - threadIdx.x;
-        const unsigned long long w = p >= 0 ? lb_wait(&lookback[p], epoch, status) : lb_word(epoch, kFlagInclusive, 0);
-        const uint32_t inc = __ballot_sync(0xFFFFFFFFu, ((uint32_t)(w >> 32) & 3u) == kFlagInclusive);
-        if (lane == 0) s_first[warp] = inc ? (uint32_t)(warp * 32 + __ffs(inc) - 1) : 0xFFFFFFFFu;
-        __syncthreads();
-        uint32_t first = 0xFFFFFFFFu;   // the nearest inclusive predecessor's thread
+    const uint64_t wb = (uint64_t)blockIdx.x * kScanTile + (uint64_t)warp * (32 * kScanItems);
+    const uint32_t fl = lane_flags<K, MODE, VEC>(keys, in_group, flags, n, wb, lane);
+    if (masks) masks[(uint64_t)blockIdx.x * kScanThreads + threadIdx.x] = (uint16_t)fl;
+    uint32_t c = __popc(fl);
 #pragma unroll
-        for (int i = 0; i < kScanWarps; ++i) first = min(first, s_first[i]);
-        uint32_t v = threadIdx.x <= first ? (uint32_t)w : 0u;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if (lane == 0) s_warp[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        if (lane == 0) s_sum[warp] = v;
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < kScanWarps; ++i) excl += s_sum[i];
-        __syncthreads();   // s_first and s_sum are read before they are written again
-        if (first != 0xFFFFFFFFu) return excl;
-        last -= kScanThreads;
+        for (int w = 0; w < kScanWarps; ++w) t += s_warp[w];
+        tile_count[blockIdx.x] = t;
     }
 }
 
-// Persistent blocks (as many as are resident); each claims tiles of
-// kScanTile positions in order from the tile counter, one at a time.  A
-// tile's aggregate is published as soon as its flags are counted, and its
-// exclusive prefix comes from a block-wide look-back: the other resident
-// tiles are at most one round trip of predecessors away.
-template <typename K, int MODE, bool VEC>
+// Pass 2 (one block): exclusive prefix of the tile counts; the total is the
+// group count, and (for segment extraction) the sentinel after the last
+// segment start.
+__global__ void __launch_bounds__(1024) scan_prefix_kernel(const uint32_t *__restrict__ tile_count, uint32_t tiles,
+                                                           uint32_t *__restrict__ tile_prefix, uint32_t *d_count,
+                                                           uint32_t *seg_start, uint64_t n)
+{
+    kernel_prologue();
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_carry;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < tiles; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < tiles ? tile_count[i] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0u;
+            uint32_t wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+                if (lane >= o) wi += y;
+            }
+            s_warp[lane] = wi - w;
+        }
+        __syncthreads();
+        const uint32_t excl = s_carry + s_warp[warp] + incl - v;
+        if (i < tiles) tile_prefix[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (d_count) *d_count = s_carry;
+        if (seg_start) seg_start[s_carry] = (uint32_t)n;
+    }
+}
+
+// Pass 3: the group ids (and segment starts) of every tile, from its prefix
+// and the boundary masks of pass 1 (or, without them, the masks recomputed
+// from the keys; tiles are then taken last first, since the keys that pass 1
+// read last are the ones still in L2).
+template <typename K, int MODE, bool VEC, bool MASKS>
 __global__ void __launch_bounds__(kScanThreads, 2)
-boundary_scan_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group,
-                     const uint8_t *__restrict__ flags, uint32_t *__restrict__ out_group, uint32_t *__restrict__ seg_start,
-                     uint64_t n, uint32_t *tile_counter, unsigned long long *lookback,
-                     uint32_t epoch, uint32_t *d_count, int *status)
+scan_ids_kernel(const K *__restrict__ keys, const uint32_t *__restrict__ in_group, const uint8_t *__restrict__ flags,
+                uint64_t n, const uint32_t *__restrict__ tile_prefix, const uint16_t *__restrict__ masks,
+                uint32_t *__restrict__ out_group, uint32_t *__restrict__ seg_start)
 {
     kernel_prologue();
     using L = ScanLayout<K, MODE>;
     constexpr int P = L::P, C = L::C, FW = L::FW;
     constexpr uint32_t kChunkMask = (1u << P) - 1u;
     constexpr unsigned long long kFieldMask = (1ull << FW) - 1ull;
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warp[kScanWarps + 1];
-    __shared__ uint32_t s_first[kScanWarps], s_sum[kScanWarps];
-
+    __shared__ uint32_t s_warp[kScanWarps];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
-
-    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    uint32_t tile = s_tile;
-    while (tile < tiles) {
-        const uint64_t base = (uint64_t)tile * kScanTile;
-        const uint64_t wb = base + (uint64_t)warp * (32 * kScanItems);
-        // boundary flags, bit c * P + j = position wb + c * 32 * P + lane * P + j
-        uint32_t fl = 0;
-        if (wb < n) {
-            K v[C][P];
-            K vprev = K(0);        // lane 0: the key before the warp's first position
-            uint32_t g[C][P];
-            uint32_t gprev = 0;
-            uint8_t f[C][P];
+    const uint32_t tile = MASKS ? blockIdx.x : gridDim.x - 1 - blockIdx.x;
+    const uint64_t wb = (uint64_t)tile * kScanTile + (uint64_t)warp * (32 * kScanItems);
+    uint32_t fl;
+    if constexpr (MASKS) fl = masks[(uint64_t)tile * kScanThreads + threadIdx.x];
+    else fl = lane_flags<K, MODE, VEC>(keys, in_group, flags, n, wb, lane);
+    // per chunk: the lane's exclusive count within the warp, packed
+    unsigned long long wcnt = 0;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
-                if constexpr (L::kKeys) load_chunk<K, P, VEC>(keys, p, n, v[c]);
-                if constexpr (L::kGroup) load_chunk<uint32_t, P, VEC>(in_group, p, n, g[c]);
-                if constexpr (L::kFlags) load_chunk<uint8_t, P, VEC>(flags, p, n, f[c]);
-            }
-            if (lane == 0 && wb > 0) {
-                if constexpr (L::kKeys) vprev = keys[wb - 1];
-                if constexpr (L::kGroup) gprev = in_group[wb - 1];
-            }
+    for (int c = 0; c < C; ++c) wcnt |= (unsigned long long)__popc((fl >> (c * P)) & kChunkMask) << (c * FW);
+    unsigned long long incl = wcnt;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
-                uint32_t bits = 0;
-                if constexpr (L::kFlags) {
-#pragma unroll
-                    for (int j = 0; j < P; ++j) bits |= (uint32_t)(f[c][j] != 0) << j;
-                } else {
-                    if constexpr (L::kKeys) {
-                        // the item before each lane's run: the previous lane's
-                        // last, the last lane's of the previous chunk, or vprev
-                        const K up = shfl_up_any(v[c][P - 1], 1);
-                        const K wrap = c > 0 ? shfl_any(v[c > 0 ? c - 1 : 0][P - 1], 31) : vprev;
-                        K prev = lane == 0 ? wrap : up;
-#pragma unroll
-                        for (int j = 0; j < P; ++j) {
-                            bits |= (uint32_t)(v[c][j] != prev) << j;
-                            prev = v[c][j];
-                        }
-                    }
-                    if constexpr (L::kGroup) {
-                        const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, g[c][P - 1], 1);
-                        const uint32_t wrap =
-                            c > 0 ? __shfl_sync(0xFFFFFFFFu, g[c > 0 ? c - 1 : 0][P - 1], 31) : gprev;
-                        uint32_t prev = lane == 0 ? wrap : up;
-#pragma unroll
-                        for (int j = 0; j < P; ++j) {
-                            bits |= (uint32_t)(g[c][j] != prev) << j;
-                            prev = g[c][j];
-                        }
-                    }
-                    if (p == 0) bits |= 1u;
-                }
-                // positions past n
-                if (p >= n) bits = 0;
-                else if (n - p < (uint64_t)P) bits &= (1u << (uint32_t)(n - p)) - 1u;
-                fl |= bits << (c * P);
-            }
-        }
-        // per chunk: the lane's exclusive count within the warp, packed
-        unsigned long long wcnt = 0;
-#pragma unroll
-        for (int c = 0; c < C; ++c) wcnt |= (unsigned long long)__popc((fl >> (c * P)) & kChunkMask) << (c * FW);
-        unsigned long long incl = wcnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const unsigned long long tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        const unsigned long long excl_l = incl - wcnt;
-        if (lane == 31) {
-            uint32_t wsum = 0;   // the warp's count
-#pragma unroll
-            for (int c = 0; c < C; ++c) wsum += (uint32_t)((tot >> (c * FW)) & kFieldMask);
-            s_warp[warp] = wsum;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t wv = lane < kScanWarps ? s_warp[lane] : 0u;
-            uint32_t wi = wv;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-                if (lane >= o) wi += y;
-            }
-            const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, kScanWarps - 1);
-            if (lane < kScanWarps) s_warp[lane] = wi - wv;
-            if (lane == 0) {
-                s_warp[kScanWarps] = agg;
-                st_volatile_u64(&lookback[tile], lb_word(epoch, tile == 0 ? kFlagInclusive : kFlagAggregate, agg));
-            }
-        }
-        __syncthreads();
-        const uint32_t agg = s_warp[kScanWarps];
-        const uint32_t excl = tile == 0 ? 0u : block_lookback(lookback, tile, epoch, status, s_first, s_sum);
-        if (threadIdx.x == 0) {
-            if (tile > 0) st_volatile_u64(&lookback[tile], lb_word(epoch, kFlagInclusive, excl + agg));
-            if (base + kScanTile >= n && d_count) *d_count = excl + agg;  // the last tile
-        }
-        // groups started before the chunk's run: before the warp, in the
-        // warp's earlier chunks, in this chunk's earlier lanes
-        uint32_t first = excl + s_warp[warp];
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
-            const uint32_t cfirst = first + (uint32_t)((excl_l >> (c * FW)) & kFieldMask);
-            first += (uint32_t)((tot >> (c * FW)) & kFieldMask);
-            if (p >= n) continue;
-            const uint32_t bits = (fl >> (c * P)) & kChunkMask;
-            if (out_group) {
-                // 1-based id of the group holding position p + j, minus one
-                uint32_t o[P];
-                uint32_t id = cfirst;
-#pragma unroll
-                for (int j = 0; j < P; ++j) {
-                    id += (bits >> j) & 1u;
-                    o[j] = id - 1u;
-                }
-                if (VEC && p + P <= n) {
-                    if constexpr (P == 2) {
-                        *reinterpret_cast<uint2 *>(out_group + p) = make_uint2(o[0], o[1]);
-                    } else {
-#pragma unroll
-                        for (int w = 0; w < P / 4; ++w)
-                            reinterpret_cast<uint4 *>(out_group + p)[w] =
-                                make_uint4(o[4 * w], o[4 * w + 1], o[4 * w + 2], o[4 * w + 3]);
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < P; ++j)
-                        if (p + j < n) out_group[p + j] = o[j];
-                }
-            }
-            if (seg_start) {
-                uint32_t sid = cfirst;
-                for (uint32_t m = bits; m; m &= m - 1) seg_start[sid++] = (uint32_t)(p + (__ffs(m) - 1));
-            }
-        }
-        if (seg_start && base + kScanTile >= n && threadIdx.x == 0) {
-            // the end sentinel after the last segment
-            seg_start[excl + agg] = (uint32_t)n;
-        }
-        // the next tile, once every thread has read this one's shared words
-        if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-        __syncthreads();
-        tile = s_tile;
-        __syncthreads();   // every thread has read s_tile before it is written again
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
     }
-}
-
-// Resident blocks of a scan kernel on this device (the persistent grid).
-template <typename F>
-unsigned scan_grid(F *kernel, uint64_t tiles)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kScanThreads, 0);
-    const uint64_t resident = (uint64_t)std::max(sms, 1) * (uint64_t)std::max(per_sm, 1);
-    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, resident));
+    const unsigned long long tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    const unsigned long long excl_l = incl - wcnt;
+    if (lane == 31) {
+        uint32_t wsum = 0;   // the warp's count
+#pragma unroll
+        for (int c = 0; c < C; ++c) wsum += (uint32_t)((tot >> (c * FW)) & kFieldMask);
+        s_warp[warp] = wsum;
+    }
+    __syncthreads();
+    // groups started before the warp: before the tile, in its earlier warps
+    uint32_t first = tile_prefix[tile];
+    for (int w = 0; w < warp; ++w) first += s_warp[w];
+    if (wb >= n) return;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const uint64_t p = wb + (uint64_t)c * (32 * P) + (uint64_t)lane * P;
+        // groups started before this lane's run in the chunk
+        const uint32_t cfirst = first + (uint32_t)((excl_l >> (c * FW)) & kFieldMask);
+        first += (uint32_t)((tot >> (c * FW)) & kFieldMask);
+        if (p >= n) continue;
+        const uint32_t bits = (fl >> (c * P)) & kChunkMask;
+        if (out_group) {
+            // 1-based id of the group holding position p + j, minus one
+            uint32_t o[P];
+            uint32_t id = cfirst;
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                id += (bits >> j) & 1u;
+                o[j] = id - 1u;
+            }
+            if (VEC && p + P <= n) {
+                if constexpr (P == 2) {
+                    *reinterpret_cast<uint2 *>(out_group + p) = make_uint2(o[0], o[1]);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < P / 4; ++w)
+                        reinterpret_cast<uint4 *>(out_group + p)[w] =
+                            make_uint4(o[4 * w], o[4 * w + 1], o[4 * w + 2], o[4 * w + 3]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < P; ++j)
+                    if (p + j < n) out_group[p + j] = o[j];
+            }
+        }
+        if (seg_start) {
+            uint32_t sid = cfirst;
+            for (uint32_t m = bits; m; m &= m - 1) seg_start[sid++] = (uint32_t)(p + (__ffs(m) - 1));
+        }
+    }
 }
 
 template <typename K, int MODE, bool VEC>
 void launch_scan_mode(cudaStream_t st, const K *keys, const uint32_t *in_group, const uint8_t *flags,
-                      uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_counter,
-                      unsigned long long *lookback, uint32_t epoch, uint32_t *d_count, int *status)
+                      uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_work, uint16_t *masks,
+                      uint32_t *d_count)
 {
-    auto *kern = boundary_scan_kernel<K, MODE, VEC>;
-    const unsigned grid = scan_grid(kern, (n + kScanTile - 1) / kScanTile);
-    launch_k(kern, grid, kScanThreads, 0, st, keys, in_group, flags, out_group, seg_start, n, tile_counter,
-             lookback, epoch, d_count, status);
+    const uint32_t tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
+    uint32_t *tile_count = tile_work, *tile_prefix = tile_work + tiles;
+    launch_k(scan_count_kernel<K, MODE, VEC>, tiles, kScanThreads, 0, st, keys, in_group, flags, n, tile_count, masks);
+    launch_k(scan_prefix_kernel, 1, 1024, 0, st, (const uint32_t *)tile_count, tiles, tile_prefix, d_count, seg_start, n);
+    if (masks)
+        launch_k(scan_ids_kernel<K, MODE, VEC, true>, tiles, kScanThreads, 0, st, keys, in_group, flags, n,
+                 (const uint32_t *)tile_prefix, (const uint16_t *)masks, out_group, seg_start);
+    else
+        launch_k(scan_ids_kernel<K, MODE, VEC, false>, tiles, kScanThreads, 0, st, keys, in_group, flags, n,
+                 (const uint32_t *)tile_prefix, (const uint16_t *)masks, out_group, seg_start);
 }
 
-// Launches the scan for what it reads, with 16-byte vector accesses when
-// every array allows.
+// Launches the three passes for what the scan reads, with vector accesses
+// when every array is 16-byte aligned.  tile_work holds 2 words per tile;
+// masks (optional) kScanThreads 16-bit words per tile.
 template <typename K>
 void launch_scan(cudaStream_t st, const K *keys, const uint32_t *in_group, const uint8_t *flags,
-                 uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_counter,
-                 unsigned long long *lookback, uint32_t epoch, uint32_t *d_count, int *status)
+                 uint32_t *out_group, uint32_t *seg_start, uint64_t n, uint32_t *tile_work, uint16_t *masks,
+                 uint32_t *d_count)
 {
     const bool vec = (((uintptr_t)keys | (uintptr_t)in_group | (uintptr_t)flags | (uintptr_t)out_group) & 15u) == 0;
     const int mode = flags ? kScanFlags : (keys ? kScanKeys : 0) | (in_group ? kScanGroup : 0);
-#define FMCS_SCAN_MODE(M)                                                                                      \
-    (vec ? launch_scan_mode<K, M, true>(st, keys, in_group, flags, out_group, seg_start, n, tile_counter,     \
-                                        lookback, epoch, d_count, status)                                    \
-         : launch_scan_mode<K, M, false>(st, keys, in_group, flags, out_group, seg_start, n, tile_counter,    \
-                                         lookback, epoch, d_count, status))
+#define FMCS_SCAN_MODE(M)                                                                                        \
+    (vec ? launch_scan_mode<K, M, true>(st, keys, in_group, flags, out_group, seg_start, n, tile_work, masks,    \
+                                        d_count)                                                               \
+         : launch_scan_mode<K, M, false>(st, keys, in_group, flags, out_group, seg_start, n, tile_work, masks,   \
+                                         d_count))
     switch (mode) {
     case kScanKeys: FMCS_SCAN_MODE(kScanKeys); break;
     case kScanKeysGroup: FMCS_SCAN_MODE(kScanKeysGroup); break;
@@ -357,36 +375,33 @@ int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const
         return FMCS_OK;
     }
     const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
-    void *lb = nullptr, *cnt = nullptr;
-    int rc = ws_get(ctx, kSlotScanTiles, tiles * sizeof(unsigned long long), &lb, true);
+    if (tiles > 0xFFFFFFFFull) return set_error(ctx, FMCS_E_INVAL, "boundary scan: too many rows");
+    void *tw = nullptr;
+    int rc = ws_get(ctx, kSlotScanTiles, tiles * (2 * sizeof(uint32_t) + kScanThreads * sizeof(uint16_t)), &tw);
     if (rc) return rc;
-    rc = ws_get(ctx, kSlotCounters, 4096, &cnt);
-    if (rc) return rc;
-    uint32_t *tile_counter = (uint32_t *)cnt;  // word 0 of the counters slot
-    cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), ctx->stream);
-    const uint32_t epoch = ctx->epoch++;
-    unsigned long long *lbw = (unsigned long long *)lb;
+    uint32_t *tile_work = (uint32_t *)tw;   // per tile: group-start count, then prefix
+    uint16_t *masks = (uint16_t *)(tile_work + 2 * tiles);   // per thread of every tile: its boundary mask
     LaunchScope ls_(ctx, "boundary_scan");
     switch (keys ? key_bytes : 0) {
     case 0:
-        launch_scan<uint32_t>(ctx->stream, nullptr, in_group, flags, out_group, seg_start, n, tile_counter, lbw,
-                              epoch, d_count, ctx->d_status);
+        launch_scan<uint32_t>(ctx->stream, nullptr, in_group, flags, out_group, seg_start, n, tile_work, masks,
+                              d_count);
         break;
     case 1:
-        launch_scan<uint8_t>(ctx->stream, (const uint8_t *)keys, in_group, flags, out_group, seg_start, n,
-                             tile_counter, lbw, epoch, d_count, ctx->d_status);
+        launch_scan<uint8_t>(ctx->stream, (const uint8_t *)keys, in_group, flags, out_group, seg_start, n, tile_work,
+                             masks, d_count);
         break;
     case 2:
         launch_scan<uint16_t>(ctx->stream, (const uint16_t *)keys, in_group, flags, out_group, seg_start, n,
-                              tile_counter, lbw, epoch, d_count, ctx->d_status);
+                              tile_work, masks, d_count);
         break;
     case 4:
         launch_scan<uint32_t>(ctx->stream, (const uint32_t *)keys, in_group, flags, out_group, seg_start, n,
-                              tile_counter, lbw, epoch, d_count, ctx->d_status);
+                              tile_work, masks, d_count);
         break;
     case 8:
         launch_scan<uint64_t>(ctx->stream, (const uint64_t *)keys, in_group, flags, out_group, seg_start, n,
-                              tile_counter, lbw, epoch, d_count, ctx->d_status);
+                              tile_work, masks, d_count);
         break;
     default:
         return set_error(ctx, FMCS_E_INVAL, "boundary scan: bad key width");
@@ -448,16 +463,17 @@ int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64
 // that reserve all of HBM up front in their own pool (a cudaMalloc from inside
 // the library would fail or fragment that pool), and latency-critical callers
 // that cannot afford the device-wide synchronization that cudaMalloc/cudaFree
-// imply.  fmcs_group_ids_noalloc serves them: the same one-pass boundary scan
-// as the group ids of a sort round, with its scratch (the decoupled look-back
-// words, the tile counter, the group count and the wait status) in the
-// file-scope device array below instead of the context's workspace.  The
-// caller passes device inputs and outputs; no context is needed.
+// imply.  fmcs_group_ids_noalloc serves them: the same boundary scan as the
+// group ids of a sort round, with its scratch (the per-tile group-start counts
+// and their prefixes, the group count and a status word) in the file-scope
+// device array below instead of the context's workspace.  The caller passes
+// device inputs and outputs; no context is needed.
 //
-// The array is modest (kNoAllocTiles look-back words, 128 KiB) and every GPU
+// The array is modest (kNoAllocTiles 64-bit words, 128 KiB) and every GPU
 // that loads the library holds it until the process exits.  n is bounded at
 // 67,108,864 rows (at most 8,192 scan tiles).  All calls share it and it keeps the
-// last call's contents, so each call clears the words that must start at zero;
+// last call's contents, so each call clears the words that must start at zero
+// (the counts and prefixes are written before they are read);
 // calls whose work overlaps on the GPU (two streams, or two host threads)
 // race on it and must be serialized by the caller.
 // ---------------------------------------------------------------------------
@@ -466,9 +482,10 @@ namespace {
 
 constexpr uint64_t kNoAllocTiles = 16384;
 constexpr uint64_t kNoAllocMaxRows = 67108864;
-static_assert(kNoAllocMaxRows / kScanTile <= kNoAllocTiles, "look-back words for every tile");
-// layout (64-bit words): [0, kNoAllocTiles) look-back; then the tile counter,
-// the group count and the status word, one 64-bit word each
+static_assert(kNoAllocMaxRows / kScanTile <= kNoAllocTiles, "a count and a prefix word for every tile");
+// layout (64-bit words): [0, kNoAllocTiles) the tiles' counts and prefixes
+// (two 32-bit words per tile); then a spare word, the group count and the
+// status word, one 64-bit word each
 constexpr uint64_t kNoAllocWords = kNoAllocTiles + 4;
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
 
@@ -517,38 +534,33 @@ extern "C" int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t k
     int rc = noalloc_scratch(&scratch);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
-    unsigned long long *lookback = scratch;
-    uint32_t *tile_counter = (uint32_t *)(scratch + kNoAllocTiles);
+    uint32_t *tile_work = (uint32_t *)scratch;   // per tile: group-start count, then prefix
     uint32_t *d_count = (uint32_t *)(scratch + kNoAllocTiles + 1);
     int *status = (int *)(scratch + kNoAllocTiles + 2);
-    // the previous call's words: look-back of the tiles this call uses, counter,
-    // count and status all start at zero
-    cudaError_t e = cudaMemsetAsync(lookback, 0, tiles * sizeof(unsigned long long), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(tile_counter, 0, 3 * sizeof(unsigned long long), st);
+    // the previous call's count and status words start at zero
+    cudaError_t e = cudaMemsetAsync(d_count, 0, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return FMCS_E_CUDA;
-    const uint32_t epoch = 1;
     switch (key_bytes) {
     case 1:
-        launch_scan<uint8_t>(st, (const uint8_t *)keys, in_group, nullptr, out_group, nullptr, n,
-                             tile_counter, lookback, epoch, d_count, status);
+        launch_scan<uint8_t>(st, (const uint8_t *)keys, in_group, nullptr, out_group, nullptr, n, tile_work, nullptr,
+                             d_count);
         break;
     case 2:
-        launch_scan<uint16_t>(st, (const uint16_t *)keys, in_group, nullptr, out_group, nullptr, n,
-                              tile_counter, lookback, epoch, d_count, status);
+        launch_scan<uint16_t>(st, (const uint16_t *)keys, in_group, nullptr, out_group, nullptr, n, tile_work,
+                              nullptr, d_count);
         break;
     case 4:
-        launch_scan<uint32_t>(st, (const uint32_t *)keys, in_group, nullptr, out_group, nullptr, n,
-                              tile_counter, lookback, epoch, d_count, status);
+        launch_scan<uint32_t>(st, (const uint32_t *)keys, in_group, nullptr, out_group, nullptr, n, tile_work,
+                              nullptr, d_count);
         break;
     default:
-        launch_scan<uint64_t>(st, (const uint64_t *)keys, in_group, nullptr, out_group, nullptr, n,
-                              tile_counter, lookback, epoch, d_count, status);
+        launch_scan<uint64_t>(st, (const uint64_t *)keys, in_group, nullptr, out_group, nullptr, n, tile_work,
+                              nullptr, d_count);
         break;
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return FMCS_E_CUDA;
-    // read the count and the wait status back (into the caller's stack: no
+    // read the count and the status word back (into the caller's stack: no
     // allocation) and finish the call
     uint32_t back[3] = {0, 0, 0};
     e = cudaMemcpyAsync(back, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);

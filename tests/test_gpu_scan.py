@@ -64,3 +64,27 @@ def test_boundary_scan_matches_oracle(dtype, segmented, misaligned):
         got = outv.cpu().numpy().view(np.uint32)
         assert ng == ng_ref, (n, ng, ng_ref)
         assert np.array_equal(got, g_ref), n
+
+
+@pytest.mark.parametrize("dtype", [np.uint16, np.uint32, np.uint64])
+@pytest.mark.parametrize("segmented", [False, True])
+def test_sort_round_group_ids_of_ordered_keys(dtype, segmented):
+    """The same sweep through a context's sort round (whose scan keeps the
+    boundary masks of its first pass in the workspace): keys already in order
+    stay in place, and the group ids are the scan's."""
+    torch = pytest.importorskip("torch")
+    from fastmulticolsort_b200 import capi
+
+    with capi.Context(0) as ctx:
+        for n in SIZES[1:]:
+            keys, ig = _case(n, dtype, segmented, seed=n * 11 + np.dtype(dtype).itemsize)
+            o_ref, g_ref, _, ng_ref = O.sort_round(keys, order=np.arange(n, dtype=np.uint32), in_group=ig)
+            kd = torch.from_numpy(_as_int(keys)).cuda()
+            igd = None if ig is None else torch.from_numpy(_as_int(ig)).cuda()
+            order = torch.arange(n, dtype=torch.int32, device="cuda")
+            grp = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+            ng = ctx.sort_round(kd, 8 * np.dtype(dtype).itemsize, order, in_group=igd, out_group=grp)
+            torch.cuda.synchronize()
+            assert ng == ng_ref, (n, ng, ng_ref)
+            assert np.array_equal(order.cpu().numpy().view(np.uint32), o_ref), n
+            assert np.array_equal(grp.cpu().numpy().view(np.uint32), g_ref), n
