@@ -54,6 +54,7 @@ constexpr int kNtC2 = 512, kItC2 = 8, kCapC2 = kNtC2 * kItC2;   // 4096
 constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
 constexpr int kCapLocal = kCapC3;   // largest segment a local tier can take; larger: MSD levels
 constexpr int kNtM = 256;           // MSD tile: 256 threads x IT items (IT = 8 or 16, tuned)
+constexpr int kHistCtas = 4;         // resident histogram CTAs per SM (the grid is one wave)
 constexpr int kMsdCtas16 = 3;       // resident scatter CTAs per SM with 16 rows per thread
 
 // counters slot words
@@ -391,12 +392,12 @@ __device__ __forceinline__ uint32_t find_segment_warp(const uint32_t *tile_prefi
     return lo;
 }
 
-// Top-digit histogram of every large segment.  A block takes one tile at a
-// time; each thread issues all of its tile's loads before counting (up to 16
+// Top-digit histogram of every large segment.  A block takes a contiguous run
+// of tiles; each thread issues all of a tile's loads before counting (up to 16
 // in flight), and each warp counts into its own shared sub-histogram so that
 // skewed digits do not serialize the whole block on one counter.
 template <typename K>
-__global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, const uint32_t *tile_prefix,
+__global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, LevelRefs r, const uint32_t *tile_prefix,
                                                         uint32_t tile_rows)
 {
     kernel_prologue();
@@ -412,14 +413,42 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, 
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
     const int warp = threadIdx.x >> 5;
-    for (uint32_t t = blockIdx.x; t < T; t += gridDim.x) {
-        const uint32_t s = find_segment_warp(tile_prefix, nseg, t);
-        const LargeSeg sg = segs[s];
-        const uint32_t k = t - tile_prefix[s];
+    // a contiguous run of tiles per block; the per-warp counts are added to
+    // the segment's histogram when the run moves to the next segment (every
+    // large segment has at least one tile) and at its end
+    const uint32_t per = (T + gridDim.x - 1) / gridDim.x;
+    const uint32_t t0 = blockIdx.x * per;
+    const uint32_t t1 = min(T, t0 + per);
+    if (t0 >= T) return;
+    for (int d = threadIdx.x; d < NW * kRadix; d += blockDim.x) (&sh[0][0])[d] = 0;
+    uint32_t s = find_segment_warp(tile_prefix, nseg, t0);
+    LargeSeg sg = segs[s];
+    uint32_t sfirst = tile_prefix[s], snext = tile_prefix[s + 1];
+    auto flush = [&]() {
+        __syncthreads();
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+            uint32_t c = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                c += sh[w][d];
+                sh[w][d] = 0;
+            }
+            if (c) atomicAdd(&hist[(uint64_t)s * kRadix + d], c);
+        }
+        __syncthreads();
+    };
+    __syncthreads();
+    for (uint32_t t = t0; t < t1; ++t) {
+        if (t >= snext) {
+            flush();
+            ++s;
+            sg = segs[s];
+            sfirst = snext;
+            snext = tile_prefix[s + 1];
+        }
+        const uint32_t k = t - sfirst;
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
         const uint32_t lo = sg.shift - width;
-        for (int d = threadIdx.x; d < NW * kRadix; d += blockDim.x) (&sh[0][0])[d] = 0;
-        __syncthreads();
         const uint64_t beg = (uint64_t)sg.start + (uint64_t)k * tile_rows;
         const uint64_t end = min((uint64_t)sg.start + sg.len, beg + tile_rows);
         K key[MAXJ];
@@ -433,15 +462,8 @@ __global__ void __launch_bounds__(kNtM) msd_hist_kernel(Bufs<K> b, LevelRefs r, 
             const uint64_t i = beg + threadIdx.x + (uint64_t)j * kNtM;
             if (i < end) atomicAdd(&sh[warp][digit_of(key[j], lo, width)], 1u);
         }
-        __syncthreads();
-        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
-            uint32_t c = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) c += sh[w][d];
-            if (c) atomicAdd(&hist[(uint64_t)s * kRadix + d], c);
-        }
-        __syncthreads();
     }
+    flush();
 }
 
 // Per large segment: exclusive digit offsets, skip detection, children.
@@ -1471,7 +1493,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             if (!(hist0_ready && host_lvl == 0 && read_back)) {
                 // (inside a graph the launch stays and returns at once on level 0)
                 LaunchScope ls_(ctx, "msd_hist");
-                launch_k(msd_hist_kernel<K>, sms * 8, kNtM, 0, s, b, lr, tile_prefix, tile_rows);
+                launch_k(msd_hist_kernel<K>, sms * kHistCtas, kNtM, 0, s, b, lr, tile_prefix, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
                 launch_k(msd_plan_kernel, sms * 8, kRadix, 0, s, lr, lists, true);
@@ -1660,7 +1682,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
             launch_k(level_prefix_kernel, 1, 1024, 0, st, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_hist");
-            launch_k(msd_hist_kernel<K>, sms * 8, kNtM, 0, st, b, lr, tile_prefix, tile_rows);
+            launch_k(msd_hist_kernel<K>, sms * kHistCtas, kNtM, 0, st, b, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_plan");
             launch_k(msd_plan_kernel, 1, kRadix, 0, st, lr, none, false);
