@@ -3,11 +3,12 @@ the runs of a previous round's group ids) on every key width, at sizes on
 and around the kernel's chunk and tile edges, with 16-byte-aligned and
 misaligned arrays (vector and scalar loads).
 
-Called through fmcs_group_ids_noalloc, which runs the same scan kernel as a
-sort round; the expected ids are the oracle's (extractGroupInfo,
-src/composer.cpp:630-678, restated in oracle/fmcs_oracle.c) for keys that are
-already in order, so that its stable sort leaves them in place.  Integer ids:
-the comparison is exact."""
+Called through fmcs_group_ids_noalloc (the scan's count and prefix passes, its
+id pass recomputing the boundary masks from the keys) and through a context's
+sort round (the id pass reading the masks that the count pass kept); the
+expected ids are the oracle's (extractGroupInfo, src/composer.cpp:630-678,
+restated in oracle/fmcs_oracle.c) for keys that are already in order, so that
+its stable sort leaves them in place.  Integer ids: the comparison is exact."""
 import numpy as np
 import pytest
 
