@@ -69,21 +69,29 @@ def test_boundary_scan_matches_oracle(dtype, segmented, misaligned):
 
 @pytest.mark.parametrize("dtype", [np.uint16, np.uint32, np.uint64])
 @pytest.mark.parametrize("segmented", [False, True])
-def test_sort_round_group_ids_of_ordered_keys(dtype, segmented):
+@pytest.mark.parametrize("misaligned", [False, True])
+def test_sort_round_group_ids_of_ordered_keys(dtype, segmented, misaligned):
     """The same sweep through a context's sort round (whose scan keeps the
     boundary masks of its first pass in the workspace): keys already in order
-    stay in place, and the group ids are the scan's."""
+    stay in place, and the group ids are the scan's.  Misaligned: the caller's
+    in_group and group arrays start one element into their buffers, so the
+    scans that read or write them take their scalar paths."""
     torch = pytest.importorskip("torch")
     from fastmulticolsort_b200 import capi
+
+    def dev(a):
+        if not misaligned:
+            return torch.from_numpy(_as_int(a)).cuda()
+        return torch.from_numpy(_as_int(np.concatenate([a[:1], a]))).cuda()[1:]
 
     with capi.Context(0) as ctx:
         for n in SIZES[1:]:
             keys, ig = _case(n, dtype, segmented, seed=n * 11 + np.dtype(dtype).itemsize)
             o_ref, g_ref, _, ng_ref = O.sort_round(keys, order=np.arange(n, dtype=np.uint32), in_group=ig)
             kd = torch.from_numpy(_as_int(keys)).cuda()
-            igd = None if ig is None else torch.from_numpy(_as_int(ig)).cuda()
+            igd = None if ig is None else dev(ig)
             order = torch.arange(n, dtype=torch.int32, device="cuda")
-            grp = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+            grp = dev(np.full(n, 0xFFFFFFFF, np.uint32))
             ng = ctx.sort_round(kd, 8 * np.dtype(dtype).itemsize, order, in_group=igd, out_group=grp)
             torch.cuda.synchronize()
             assert ng == ng_ref, (n, ng, ng_ref)
