@@ -319,10 +319,23 @@ def zipf_segmented(ctx, stream, n: int, reps: int):
 
     out = {"rows": n, "columns": "20-bit Zipf(1.0) over 2^20 codes (u32), 24-bit (u32), 40-bit (u64)",
            "largest_group": int(sizes.max()), "groups_col0": card[0], "plan_chosen": plan}
+    results = {}
     for name, fn in (("plain_ms", plain), ("segmented_ms", segmented), ("massaged_ms", massaged)):
         fn()
         total, per = time_steps(ctx, stream, fn, reps)
         out[name] = round(total / reps, 3)
+        torch.cuda.synchronize()
+        results[name] = (order.clone(), group.clone())   # every variant's last round writes `group`
+    # the three variants must agree exactly, and the result must be a sorted,
+    # canonically tie-ordered, densely grouped permutation
+    from fastmulticolsort_b200 import batch_bench as BB
+    same = all(torch.equal(results["plain_ms"][i], results[k][i])
+               for k in ("segmented_ms", "massaged_ms") for i in (0, 1))
+    props = BB.sorted_properties(torch, dcols, *results["segmented_ms"])
+    out["check"] = {"variants_equal": bool(same), "properties": props,
+                    "digest_order_group": BB._digest(torch, *results["segmented_ms"])}
+    out["checked"] = bool(same and all(props.values()))
+    del results
     best = min(out["segmented_ms"], out["massaged_ms"])
     out["speedup_vs_plain"] = round(out["plain_ms"] / best, 3)
     out["value_mrows_s"] = round(n / (best / 1e3) / 1e6, 1)
@@ -377,6 +390,11 @@ def run_fmcs(args):
     total_ms = dist_max(total_ms, world)
     ms_per_step = total_ms / args.steps
     value = world * n / (ms_per_step / 1e3) / 1e6
+    # the timed replays' result: a sorted, canonically tie-ordered, densely
+    # grouped permutation of the rows (size-independent checks on the device)
+    from fastmulticolsort_b200 import batch_bench as BB
+    head_props = BB.sorted_properties(torch, dcols, dorder, dgroup)
+    head_check = {"properties": head_props, "digest_order_group": BB._digest(torch, dorder, dgroup)}
     # the same K steps as eager C-ABI calls, with the library's CUDA events
     # around every kernel: the per-kernel split and the roofline.  An eager
     # step launches the same kernels as a replay (the replay's level loop runs
@@ -510,6 +528,8 @@ def run_fmcs(args):
                           "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)), "d2h_bytes_per_step": int(8 * n)},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "check": head_check,
+        "checked": all(head_props.values()),
     }
     if not args.no_zipf:
         line["zipf_segmented"] = zipf_segmented(ctx, stream, args.zipf_rows, max(3, min(args.steps, 10)))

@@ -116,16 +116,17 @@ def calibrate(ctx, quick: bool) -> dict:
         src = _dev(rng.integers(0, 1 << min(bits, 62), size=n, dtype=np.uint64).astype(np.dtype(f"u{nb}")))
         dst = torch.empty(n, dtype=dt, device="cuda")
         gather.append(_time(lambda: ctx.gather(src, order, dst), 7) / mrows)
-        keys = torch.sort(src.view(torch.int64) if nb == 8 else src)[0].contiguous().view(dt)
-        grp = torch.empty(n, dtype=torch.int32, device="cuda")
-        boundary.append(_time(lambda: capi.group_ids_noalloc(keys, grp), 7) / mrows)
-        # one HBM radix level: round 0 over uniform keys, MSD kernels only
+        # one HBM radix level (round 0 over uniform keys, MSD kernels only) and
+        # the boundary scan of the round's group ids, both timed inside the
+        # round as the library runs them
         o = torch.empty(n, dtype=torch.int32, device="cuda")
-        ctx.sort_round(src, bits, o)
+        grp = torch.empty(n, dtype=torch.int32, device="cuda")
+        ctx.sort_round(src, bits, o, out_group=grp)
         ctx.profile(True)
-        ctx.sort_round(src, bits, o)
+        ctx.sort_round(src, bits, o, out_group=grp)
         prof = ctx.profile_report()
         ctx.profile(False)
+        boundary.append(prof["boundary_scan"]["ms"] / mrows)
         lvl_ms = sum(v["ms"] for k, v in prof.items() if k.startswith(("msd_", "tile_prefix")))
         rows = prof.get("msd_scatter", {}).get("units", 0) or n
         msd.append(lvl_ms / (rows / 1e6))

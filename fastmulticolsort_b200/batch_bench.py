@@ -81,9 +81,12 @@ def _time_ms(torch, stream, fn, reps):
     return a.elapsed_time(b) / reps
 
 
-def instances(torch, ctx, stream, reps=3, plain=True):
+def instance_workload(torch, count=INSTANCE_COUNT):
+    """The many-instances shape on the device: (cols, sizes, bw, split, est_ms).
+    est_ms is the cost model's estimate for ONE instance of the mean size
+    (the plan is chosen for that instance)."""
     rng = W.rng_for(4)
-    sizes = np.floor(2.0 ** rng.uniform(10, 20, size=INSTANCE_COUNT)).astype(np.int64)
+    sizes = np.floor(2.0 ** rng.uniform(10, 20, size=count)).astype(np.int64)
     total = int(sizes.sum())
     bw = [8, 24, 40]
     cols = [_pool_column(torch, rng, total, 8, 16), _uniform_column(torch, rng, total, 24),
@@ -91,6 +94,55 @@ def instances(torch, ctx, stream, reps=3, plain=True):
     col_bytes = [c.element_size() for c in cols]
     mean_n = int(sizes.mean())
     split, _, est = capi.optimize_plan(bw, [16, min(mean_n, 1 << 24), mean_n], col_bytes, mean_n)
+    return cols, sizes, bw, split, est
+
+
+def wide_workload(torch):
+    """The wide table on the device: (cols, card, ORDER BY split, GROUP BY
+    (split, column order))."""
+    rng = W.rng_for(4, salt=1)
+    n = WIDE_ROWS
+    cols = []
+    for w, k in zip(WIDE_BITS, WIDE_CARD):
+        cols.append(_uniform_column(torch, rng, n, w) if k >= (1 << w) else _pool_column(torch, rng, n, w, k))
+    col_bytes = [c.element_size() for c in cols]
+    card = [min(k, n) for k in WIDE_CARD]
+    split, _, _ = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=True)
+    gsplit, gorder, _ = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=False)
+    return cols, card, split, (gsplit, gorder)
+
+
+def sample_instances(sizes, count=20, seed=7):
+    """Indices of `count` instances spread over the size range (smallest,
+    largest and a seeded sample between), for the oracle check."""
+    rng = np.random.default_rng(seed)
+    k = len(sizes)
+    pick = {int(np.argmin(sizes)), int(np.argmax(sizes))}
+    pick.update(int(i) for i in rng.choice(k, size=min(k, count) - len(pick), replace=False))
+    return sorted(pick)[:count]
+
+
+def check_instances_vs_oracle(cols, sizes, bw, split, order, group, counts, picks):
+    """Each picked instance's instance-local order and group ids, and its group
+    count, against the oracle on that instance's rows (host copies)."""
+    from oracle import oracle as O
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    for i in picks:
+        a, b = int(offs[i]), int(offs[i + 1])
+        sub = [c[a:b].cpu().numpy() for c in cols]
+        sub = [x.view(np.uint16 if x.dtype == np.int16 else (np.uint32 if x.dtype == np.int32 else np.uint64))
+               for x in sub]
+        o, g, ng = O.run_plan_sort(sub, bw, split)
+        if not (np.array_equal(order[a:b].cpu().numpy().view(np.uint32), o)
+                and np.array_equal(group[a:b].cpu().numpy().view(np.uint32), g) and int(counts[i]) == ng):
+            return False, i
+    return True, None
+
+
+def instances(torch, ctx, stream, reps=3, plain=True):
+    cols, sizes, bw, split, est = instance_workload(torch)
+    total = int(sizes.sum())
+    col_bytes = [c.element_size() for c in cols]
     order = torch.empty(total, dtype=torch.int32, device="cuda")
     group = torch.empty(total, dtype=torch.int32, device="cuda")
     offs = np.concatenate([[0], np.cumsum(sizes)])
@@ -115,15 +167,30 @@ def instances(torch, ctx, stream, reps=3, plain=True):
 
     out = {"instances": INSTANCE_COUNT, "rows": total, "rows_min": int(sizes.min()), "rows_max": int(sizes.max()),
            "rows_mean": round(float(sizes.mean()), 1), "columns": "8-bit (16 distinct values, u16), 24-bit (u32), "
-           "40-bit (u64)", "plan": split, "plan_est_ms": round(est, 3),
+           "40-bit (u64)", "plan": split, "plan_est_ms_mean_instance": round(est, 3),
            "column_bytes": int(total * sum(col_bytes))}
-    batched()
+    counts = ctx.run_batch(cols, bw, split, sizes, order, group)
     out["batched_ms"] = round(_time_ms(torch, stream, batched, reps), 3)
+    torch.cuda.synchronize()
+    b_order, b_group = order.clone(), group.clone()
     per_instance()
     out["per_instance_ms"] = round(_time_ms(torch, stream, per_instance, 1), 3)
+    torch.cuda.synchronize()
+    same_pi = bool(torch.equal(order, b_order) and torch.equal(group, b_group))
     if plain:
         plain_path()
         out["plain_ms"] = round(_time_ms(torch, stream, plain_path, 1), 3)
+        torch.cuda.synchronize()
+        same_plain = bool(torch.equal(order, b_order) and torch.equal(group, b_group))
+    else:
+        same_plain = True
+    picks = sample_instances(sizes)
+    ok, bad = check_instances_vs_oracle(cols, sizes, bw, split, b_order, b_group, counts, picks)
+    out["check"] = {"batched_equals_per_instance": same_pi, "batched_equals_plain": same_plain,
+                    "oracle_instances": len(picks), "oracle_equal": ok, "first_mismatch": bad,
+                    "digest_order_group": _digest(torch, b_order, b_group)}
+    out["checked"] = bool(same_pi and same_plain and ok)
+    del b_order, b_group
     for k in ("batched", "per_instance", "plain"):
         if f"{k}_ms" in out:
             out[f"{k}_mrows_s"] = round(total / (out[f"{k}_ms"] / 1e3) / 1e6, 1)
@@ -136,15 +203,8 @@ def instances(torch, ctx, stream, reps=3, plain=True):
 
 
 def wide(torch, ctx, stream, reps=3):
-    rng = W.rng_for(4, salt=1)
     n = WIDE_ROWS
-    cols = []
-    for w, k in zip(WIDE_BITS, WIDE_CARD):
-        cols.append(_uniform_column(torch, rng, n, w) if k >= (1 << w) else _pool_column(torch, rng, n, w, k))
-    col_bytes = [c.element_size() for c in cols]
-    card = [min(k, n) for k in WIDE_CARD]
-    split, _, est_o = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=True)
-    gsplit, gorder, est_g = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=False)
+    cols, card, split, (gsplit, gorder) = wide_workload(torch)
     order = torch.empty(n, dtype=torch.int32, device="cuda")
     group = torch.empty(n, dtype=torch.int32, device="cuda")
     g2 = torch.empty_like(group)
@@ -163,15 +223,91 @@ def wide(torch, ctx, stream, reps=3):
 
     out = {"rows": n, "bits": WIDE_BITS, "distinct": WIDE_CARD, "order_by_plan": split,
            "group_by_plan": gsplit, "group_by_column_order": gorder}
+    results = {}
     for name, fn in (("order_by", order_by), ("group_by", group_by), ("plain", plain_path)):
         fn()
         ms = _time_ms(torch, stream, fn, reps)
         out[f"{name}_ms"] = round(ms, 3)
         out[f"{name}_mrows_s"] = round(n / (ms / 1e3) / 1e6, 1)
+        torch.cuda.synchronize()
+        # the plain path's last round leaves its group ids in `group` or `g2`
+        fin = group if name != "plain" or len(WIDE_BITS) % 2 == 1 else g2
+        results[name] = (order.clone(), fin.clone())
     out["speedup_order_by_vs_plain"] = round(out["plain_ms"] / out["order_by_ms"], 2)
+    same = bool(torch.equal(results["order_by"][0], results["plain"][0])
+                and torch.equal(results["order_by"][1], results["plain"][1]))
+    props = sorted_properties(torch, cols, results["order_by"][0], results["order_by"][1])
+    same_groups = same_grouping(torch, results["order_by"], results["group_by"], n)
+    out["check"] = {"order_by_equals_plain": same, "order_by_properties": props,
+                    "group_by_same_groups_as_order_by": same_groups,
+                    "digest_order_by": _digest(torch, *results["order_by"]),
+                    "digest_group_by": _digest(torch, *results["group_by"])}
+    out["checked"] = bool(same and all(props.values()) and same_groups)
+    del results
     del cols, order, group, g2
     torch.cuda.empty_cache()
     return out
+
+
+def _digest(torch, *arrays) -> str:
+    """sha256 of the arrays' bytes (host copies), a fingerprint of a result."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(a.cpu().numpy().tobytes())
+    return h.hexdigest()[:16]
+
+
+def _as_u64(torch, c):
+    """A column's codes as non-negative int64 (u16 / u32 bits stored signed)."""
+    if c.dtype == torch.int16:
+        return c.to(torch.int64) & 0xFFFF
+    if c.dtype == torch.int32:
+        return c.to(torch.int64) & 0xFFFFFFFF
+    return c
+
+
+def sorted_properties(torch, cols, order, group):
+    """Size-independent checks of an ORDER BY result on the device: order is a
+    permutation, the key tuples read through it do not decrease, the group id
+    goes up by one exactly where the tuple changes, and equal tuples keep
+    ascending row ids (the canonical tie order)."""
+    n = order.shape[0]
+    o = order.to(torch.int64)
+    perm = bool(torch.equal(torch.sort(o).values, torch.arange(n, device=o.device)))
+    gt = torch.zeros(n - 1, dtype=torch.bool, device=o.device)   # tuple[i+1] > tuple[i] decided
+    eq = torch.ones(n - 1, dtype=torch.bool, device=o.device)    # equal so far
+    lt = torch.zeros(n - 1, dtype=torch.bool, device=o.device)
+    for c in cols:
+        v = _as_u64(torch, c)[o]
+        a, b = v[:-1], v[1:]
+        if v.dtype == torch.int64 and c.dtype == torch.int64:
+            # full 64-bit codes: compare as unsigned
+            a, b = a ^ (-(1 << 63)), b ^ (-(1 << 63))
+        gt |= eq & (b > a)
+        lt |= eq & (b < a)
+        eq &= (b == a)
+    nondecreasing = not bool(lt.any())
+    g = group.to(torch.int64)
+    dense = bool(int(g[0]) == 0 and torch.equal(g[1:] - g[:-1], (~eq).to(torch.int64)))
+    ties = bool((o[1:][eq] > o[:-1][eq]).all())
+    return {"permutation": perm, "tuples_nondecreasing": nondecreasing, "dense_group_ids": dense,
+            "canonical_ties": ties}
+
+
+def same_grouping(torch, sort_res, hash_res, n):
+    """The hash plan groups rows exactly as the sort plan does: per row id,
+    (sort group, hash group) pairs form a one-to-one map."""
+    so, sg = sort_res
+    ho, hg = hash_res
+    a = torch.empty(n, dtype=torch.int64, device=so.device)
+    b = torch.empty(n, dtype=torch.int64, device=so.device)
+    a[so.to(torch.int64)] = sg.to(torch.int64)
+    b[ho.to(torch.int64)] = hg.to(torch.int64)
+    na = int(a.max()) + 1
+    nb = int(b.max()) + 1
+    pairs = torch.unique(a * nb + b).numel()
+    return bool(na == nb == pairs)
 
 
 def benchmark(reps=3, plain=True):

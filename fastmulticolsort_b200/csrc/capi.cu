@@ -149,9 +149,12 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
     if ((rc = ws_get(ctx, kSlotGroupB, n * 4, &p))) return rc;
     g[1] = (uint32_t *)p;
     uint32_t *segs[2];
-    if ((rc = ws_get(ctx, kSlotSegStart, 2 * (n + 2) * sizeof(uint32_t), &p))) return rc;
-    segs[0] = (uint32_t *)p;
-    segs[1] = segs[0] + (n + 2);
+    if ((rc = ws_get(ctx, kSlotSegStart, 2 * carve_round((n + 2) * sizeof(uint32_t)), &p))) return rc;
+    {
+        Carver cv(p);
+        segs[0] = cv.take<uint32_t>(n + 2);
+        segs[1] = cv.take<uint32_t>(n + 2);
+    }
     uint32_t *d_nseg[2] = {w + kCtrNgroups + 2, w + kCtrNgroups + 3};
     const uint32_t *in_group = nullptr;
     const uint32_t *seg_in = nullptr;
@@ -385,8 +388,9 @@ extern "C" int fmcs_sort_round_plain(fmcs_ctx *ctx, const void *bank, uint32_t b
     if ((rc = stage_out(ctx, sorted_bank, n * bank_bytes, kSlotStageOut2, &dkeys, &h_keys))) return rc;
     void *kg;
     if ((rc = ws_get(ctx, kSlotKeys0, n * bank_bytes, &kg))) return rc;
-    if ((rc = ws_get(ctx, kSlotMisc, 3 * n * sizeof(uint32_t), &p))) return rc;
-    uint32_t *pos = (uint32_t *)p, *grp = pos + n, *tmp = grp + n;
+    if ((rc = ws_get(ctx, kSlotMisc, 3 * carve_round(n * sizeof(uint32_t)), &p))) return rc;
+    Carver cv(p);
+    uint32_t *pos = cv.take<uint32_t>(n), *grp = cv.take<uint32_t>(n), *tmp = cv.take<uint32_t>(n);
     uint32_t *w;
     if ((rc = counters(ctx, &w))) return rc;
     uint32_t *d_ng = w + kCtrNgroups;
@@ -661,12 +665,16 @@ extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint
     void *p;
     cudaStream_t st = ctx->stream;
     // instance starts, ids per row, bases and counts
-    if ((rc = ws_get(ctx, kSlotMisc, (2 * (size_t)ninst + 2) * sizeof(uint32_t) + n * sizeof(uint32_t) + 1024, &p)))
+    if ((rc = ws_get(ctx, kSlotMisc,
+                     carve_total({(ninst + 1) * sizeof(uint32_t), ninst * sizeof(uint32_t),
+                                  (ninst + 1) * sizeof(uint32_t), n * sizeof(uint32_t)}),
+                     &p)))
         return rc;
-    uint32_t *d_starts = (uint32_t *)p;
-    uint32_t *d_base = d_starts + ninst + 1;
-    uint32_t *d_count = d_base + ninst;
-    uint32_t *inst_id = d_count + ninst + 1;
+    Carver cv(p);
+    uint32_t *d_starts = cv.take<uint32_t>(ninst + 1);
+    uint32_t *d_base = cv.take<uint32_t>(ninst);
+    uint32_t *d_count = cv.take<uint32_t>(ninst + 1);
+    uint32_t *inst_id = cv.take<uint32_t>(n);
     cudaError_t e = cudaMemcpyAsync(d_starts, starts.data(), (ninst + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "fmcs_run_batch upload");
     {
@@ -709,9 +717,12 @@ extern "C" int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint
     if ((rc = ws_get(ctx, kSlotGroupB, n * 4, &p))) return rc;
     g[1] = (uint32_t *)p;
     uint32_t *segs[2];
-    if ((rc = ws_get(ctx, kSlotSegStart, 2 * (n + 2) * sizeof(uint32_t), &p))) return rc;
-    segs[0] = (uint32_t *)p;
-    segs[1] = segs[0] + (n + 2);
+    if ((rc = ws_get(ctx, kSlotSegStart, 2 * carve_round((n + 2) * sizeof(uint32_t)), &p))) return rc;
+    {
+        Carver cv(p);
+        segs[0] = cv.take<uint32_t>(n + 2);
+        segs[1] = cv.take<uint32_t>(n + 2);
+    }
     uint32_t *d_nseg[2] = {w + kCtrNgroups + 2, w + kCtrNgroups + 3};
     // round 0 is segmented by instance: instance ids are the incoming groups
     const uint32_t *in_group = inst_id;

@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <functional>
+#include <initializer_list>
 #include <string>
 #include <utility>
 #include <vector>
@@ -95,6 +96,34 @@ struct fmcs_ctx {
 };
 
 namespace fmcs {
+
+// Sub-arrays carved out of one workspace slot.  Each starts on a
+// kCarveAlign-byte boundary (a slot comes from cudaMalloc, so its base is
+// 256-byte aligned), whatever the sizes of the sub-arrays before it: a kernel
+// may read any of them with 16-byte vectors.
+constexpr size_t kCarveAlign = 256;
+inline size_t carve_round(size_t bytes) { return (bytes + kCarveAlign - 1) & ~(kCarveAlign - 1); }
+// Bytes of a slot that holds sub-arrays of these sizes in bytes.
+inline size_t carve_total(std::initializer_list<size_t> sizes)
+{
+    size_t t = 0;
+    for (size_t b : sizes) t += carve_round(b);
+    return t;
+}
+class Carver {
+  public:
+    explicit Carver(void *base) : cur_(static_cast<char *>(base)) {}
+    template <typename T>
+    T *take(size_t count)
+    {
+        T *p = reinterpret_cast<T *>(cur_);
+        cur_ += carve_round(count * sizeof(T));
+        return p;
+    }
+
+  private:
+    char *cur_;
+};
 
 int set_error(fmcs_ctx *ctx, int code, const std::string &msg);
 int cuda_fail(fmcs_ctx *ctx, cudaError_t e, const char *what);

@@ -164,11 +164,12 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     unsigned long long *slots = (unsigned long long *)p;
     cudaMemsetAsync(slots, 0xFF, cap * sizeof(unsigned long long), st);
     // per-row scratch: slot_of / rank (n), fpos (n), run ids (n), first flags (n bytes)
-    if ((rc = ws_get(ctx, kSlotHashIdx, n * 3 * sizeof(uint32_t) + n + 64, &p))) return rc;
-    uint32_t *slot_of = (uint32_t *)p;
-    uint32_t *fpos = slot_of + n;
-    uint32_t *run = fpos + n;
-    uint8_t *first = (uint8_t *)(run + n);
+    if ((rc = ws_get(ctx, kSlotHashIdx, 3 * carve_round(n * sizeof(uint32_t)) + carve_round(n), &p))) return rc;
+    Carver cv(p);
+    uint32_t *slot_of = cv.take<uint32_t>(n);
+    uint32_t *fpos = cv.take<uint32_t>(n);
+    uint32_t *run = cv.take<uint32_t>(n);
+    uint8_t *first = cv.take<uint8_t>(n);
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     uint32_t *d_cnt = (uint32_t *)p + 32;   // words 32..39 belong to the hash round
     uint32_t *seg_start = nullptr;

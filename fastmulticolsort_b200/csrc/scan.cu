@@ -377,10 +377,12 @@ int run_boundary_scan(fmcs_ctx *ctx, const void *keys, uint32_t key_bytes, const
     const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
     if (tiles > 0xFFFFFFFFull) return set_error(ctx, FMCS_E_INVAL, "boundary scan: too many rows");
     void *tw = nullptr;
-    int rc = ws_get(ctx, kSlotScanTiles, tiles * (2 * sizeof(uint32_t) + kScanThreads * sizeof(uint16_t)), &tw);
+    int rc = ws_get(ctx, kSlotScanTiles,
+                    carve_total({tiles * 2 * sizeof(uint32_t), tiles * kScanThreads * sizeof(uint16_t)}), &tw);
     if (rc) return rc;
-    uint32_t *tile_work = (uint32_t *)tw;   // per tile: group-start count, then prefix
-    uint16_t *masks = (uint16_t *)(tile_work + 2 * tiles);   // per thread of every tile: its boundary mask
+    Carver cv(tw);
+    uint32_t *tile_work = cv.take<uint32_t>(2 * tiles);   // per tile: group-start count, then prefix
+    uint16_t *masks = cv.take<uint16_t>(tiles * kScanThreads);   // per thread of every tile: its boundary mask
     LaunchScope ls_(ctx, "boundary_scan");
     switch (keys ? key_bytes : 0) {
     case 0:
@@ -465,17 +467,23 @@ int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64
 // that cannot afford the device-wide synchronization that cudaMalloc/cudaFree
 // imply.  fmcs_group_ids_noalloc serves them: the same boundary scan as the
 // group ids of a sort round, with its scratch (the per-tile group-start counts
-// and their prefixes, the group count and a status word) in the file-scope
-// device array below instead of the context's workspace.  The caller passes
-// device inputs and outputs; no context is needed.
+// and their prefixes, and the group count) in the file-scope device array
+// below instead of the context's workspace.  The caller passes device inputs
+// and outputs on the current device; no context is needed.
 //
 // The array is modest (kNoAllocTiles 64-bit words, 128 KiB) and every GPU
 // that loads the library holds it until the process exits.  n is bounded at
 // 67,108,864 rows (at most 8,192 scan tiles).  All calls share it and it keeps the
-// last call's contents, so each call clears the words that must start at zero
-// (the counts and prefixes are written before they are read);
+// last call's contents, so each call clears the word that must start at zero
+// (the group count; the counts and prefixes are written before they are read);
 // calls whose work overlaps on the GPU (two streams, or two host threads)
-// race on it and must be serialized by the caller.
+// race on it and must be serialized by the caller.  The scan's three passes
+// have no waits between blocks, so the call has no timeout path.
+//
+// The call is synchronous: it waits for its stream before it returns the
+// group count.  Its first call on a device resolves the array's device address
+// (cudaGetSymbolAddress, once per device, with that device current); make that
+// first call before any stream capture begins on the device.
 // ---------------------------------------------------------------------------
 namespace fmcs {
 namespace {
@@ -484,14 +492,29 @@ constexpr uint64_t kNoAllocTiles = 16384;
 constexpr uint64_t kNoAllocMaxRows = 67108864;
 static_assert(kNoAllocMaxRows / kScanTile <= kNoAllocTiles, "a count and a prefix word for every tile");
 // layout (64-bit words): [0, kNoAllocTiles) the tiles' counts and prefixes
-// (two 32-bit words per tile); then a spare word, the group count and the
-// status word, one 64-bit word each
-constexpr uint64_t kNoAllocWords = kNoAllocTiles + 4;
+// (two 32-bit words per tile); then a spare word and the group count, one
+// 64-bit word each
+constexpr uint64_t kNoAllocWords = kNoAllocTiles + 2;
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned long long *g_noalloc_ptr[kMaxDevices] = {};
+
+// True when p is device (or managed) memory that the current device can use
+// as its own: device memory of another GPU is refused.
+bool on_current_device(const void *p)
+{
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (attr.type == cudaMemoryTypeManaged) return true;
+    if (attr.type != cudaMemoryTypeDevice) return false;
+    int dev = -1;
+    return cudaGetDevice(&dev) == cudaSuccess && attr.device == dev;
+}
 
 // Host code cannot use g_noalloc_scratch's name as a device address: resolve
 // the device address once per device, with that device current.
@@ -527,18 +550,19 @@ extern "C" int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t k
     if (!(key_bytes == 1 || key_bytes == 2 || key_bytes == 4 || key_bytes == 8)) return FMCS_E_INVAL;
     if (n > kNoAllocMaxRows) return FMCS_E_INVAL;   // beyond the static scratch: 67,108,864 rows
     if (n == 0) return FMCS_OK;
-    if (!keys || !out_group || !is_device_ptr(keys) || !is_device_ptr(out_group) ||
-        (in_group && !is_device_ptr(in_group)))
-        return FMCS_E_INVAL;   // device pointers only: staging host data would allocate
+    // device pointers of the current device only: staging host data would
+    // allocate, and the scratch and the launches belong to the current device
+    if (!keys || !out_group || !on_current_device(keys) || !on_current_device(out_group) ||
+        (in_group && !on_current_device(in_group)))
+        return FMCS_E_INVAL;
     unsigned long long *scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t *tile_work = (uint32_t *)scratch;   // per tile: group-start count, then prefix
     uint32_t *d_count = (uint32_t *)(scratch + kNoAllocTiles + 1);
-    int *status = (int *)(scratch + kNoAllocTiles + 2);
-    // the previous call's count and status words start at zero
-    cudaError_t e = cudaMemsetAsync(d_count, 0, 2 * sizeof(unsigned long long), st);
+    // the previous call's group count starts at zero
+    cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return FMCS_E_CUDA;
     switch (key_bytes) {
     case 1:
@@ -560,15 +584,12 @@ extern "C" int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t k
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return FMCS_E_CUDA;
-    // read the count and the status word back (into the caller's stack: no
-    // allocation) and finish the call
-    uint32_t back[3] = {0, 0, 0};
-    e = cudaMemcpyAsync(back, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(back + 1, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    // read the count back (into the caller's stack: no allocation) and finish
+    // the call
+    uint32_t back = 0;
+    e = cudaMemcpyAsync(&back, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return FMCS_E_CUDA;
-    if ((int)back[1] == kDevTimeout) return FMCS_E_TIMEOUT;
-    if (back[1] != 0) return FMCS_E_CUDA;
-    if (ngroups) *ngroups = back[0];
+    if (ngroups) *ngroups = back;
     return FMCS_OK;
 }

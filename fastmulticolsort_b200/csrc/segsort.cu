@@ -1417,26 +1417,37 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     large[1] = (LargeSeg *)p;
     Lists lists;
     {
-        const uint64_t tot = cap_t + cap_t32 + cap_a + cap_b1 + cap_b2 + cap_c1 + cap_c2 + cap_c3;
-        if ((rc = ws_get(ctx, kSlotLocalA, tot * sizeof(uint2), &p))) return rc;
-        lists.t = (uint2 *)p;
-        lists.t32 = lists.t + cap_t;
-        lists.a = lists.t32 + cap_t32;
+        const size_t e = sizeof(uint2);
+        if ((rc = ws_get(ctx, kSlotLocalA,
+                         carve_total({cap_t * e, cap_t32 * e, cap_a * e, cap_b1 * e, cap_b2 * e, cap_c1 * e,
+                                      cap_c2 * e, cap_c3 * e}),
+                         &p)))
+            return rc;
+        Carver cv(p);
+        lists.t = cv.take<uint2>(cap_t);
+        lists.t32 = cv.take<uint2>(cap_t32);
+        lists.a = cv.take<uint2>(cap_a);
         lists.cap_t32 = sizeof(K) <= 4 ? kCapT32 : 0;
-        lists.b1 = lists.a + cap_a;
-        lists.b2 = lists.b1 + cap_b1;
-        lists.c1 = lists.b2 + cap_b2;
-        lists.c2 = lists.c1 + cap_c1;
-        lists.c3 = lists.c2 + cap_c2;
-        if ((rc = ws_get(ctx, kSlotLocalC, (cap_copy + cap_large) * sizeof(LargeSeg), &p))) return rc;
-        lists.copy = (LargeSeg *)p;
-        lists.copy_large = lists.copy + cap_copy;
+        lists.b1 = cv.take<uint2>(cap_b1);
+        lists.b2 = cv.take<uint2>(cap_b2);
+        lists.c1 = cv.take<uint2>(cap_c1);
+        lists.c2 = cv.take<uint2>(cap_c2);
+        lists.c3 = cv.take<uint2>(cap_c3);
+        if ((rc = ws_get(ctx, kSlotLocalC, carve_total({cap_copy * sizeof(LargeSeg), cap_large * sizeof(LargeSeg)}),
+                         &p)))
+            return rc;
+        Carver cc(p);
+        lists.copy = cc.take<LargeSeg>(cap_copy);
+        lists.copy_large = cc.take<LargeSeg>(cap_large);
         lists.local_max = local_max;
     }
     uint32_t *hists[2], *tile_prefix;
-    if ((rc = ws_get(ctx, kSlotSegHist, 2 * cap_large * kRadix * sizeof(uint32_t), &p))) return rc;
-    hists[0] = (uint32_t *)p;
-    hists[1] = hists[0] + cap_large * kRadix;
+    if ((rc = ws_get(ctx, kSlotSegHist, 2 * carve_round(cap_large * kRadix * sizeof(uint32_t)), &p))) return rc;
+    {
+        Carver cv(p);
+        hists[0] = cv.take<uint32_t>(cap_large * kRadix);
+        hists[1] = cv.take<uint32_t>(cap_large * kRadix);
+    }
     if ((rc = ws_get(ctx, kSlotTilePrefix, (cap_large + 1) * sizeof(uint32_t), &p))) return rc;
     tile_prefix = (uint32_t *)p;
     const uint64_t max_tiles = n / tile_rows + cap_large + 1;

@@ -291,17 +291,20 @@ FMCS_API int fmcs_optimize_plan(const uint32_t *bw, const uint64_t *cardinality,
  * equal in_group (in_group may be NULL):
  *   out_group[0] = 0; out_group[i] = out_group[i-1] +
  *       (keys[i] != keys[i-1] || in_group[i] != in_group[i-1]).
- * keys, in_group and out_group must be DEVICE pointers (host pointers are
- * rejected: staging them would allocate); stream is a cudaStream_t (NULL = the
- * default stream); *ngroups (optional, host) receives the group count.  The
- * call returns when the result is complete.
+ * keys, in_group and out_group must be DEVICE pointers of the current device
+ * (host pointers are rejected, as staging them would allocate, and so is
+ * another GPU's memory); stream is a cudaStream_t (NULL = the default stream);
+ * *ngroups (optional, host) receives the group count.  The call is
+ * synchronous: it waits for the stream and returns when the result is
+ * complete.
  * Scratch lives in a file-scope device array of the library (128 KiB, held by
  * every GPU that loads the library until exit), so n is limited to
  * 67,108,864 rows; larger n returns FMCS_E_INVAL.  The first call on a device
- * resolves that array's device address, so make a first call on each device
- * before any stream capture.  All calls share the array: calls that overlap on
- * the GPU race and must be serialized by the caller.  Nothing is allocated:
- * no cudaMalloc, no cudaFree, no allocating library routine. */
+ * resolves that array's device address (cudaGetSymbolAddress), so make that
+ * first call on each device before any stream capture begins there.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialized by the caller.  Nothing is allocated: no cudaMalloc, no cudaFree,
+ * no allocating library routine. */
 FMCS_API int fmcs_group_ids_noalloc(void *stream, const void *keys, uint32_t key_bytes,
                                     const uint32_t *in_group, uint32_t *out_group, uint64_t n,
                                     uint32_t *ngroups);

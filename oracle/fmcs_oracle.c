@@ -342,14 +342,21 @@ int orc_hash_unordered(const void *bank, uint32_t bank_bytes, const uint32_t *in
 /* whole plans                                                               */
 /* ------------------------------------------------------------------------ */
 static int build_banks(const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
-                       uint32_t ncols, const uint32_t *split, uint32_t nbanks, uint64_t n,
-                       int hash_path, void **banks, uint32_t *bank_bytes)
+                       uint32_t ncols, const uint32_t *col_order, const uint32_t *split, uint32_t nbanks,
+                       uint64_t n, int hash_path, void **banks, uint32_t *bank_bytes)
 {
     orc_record rec[256];
     uint32_t nrec[128];
     uint32_t order_cols[128];
+    uint8_t seen[128] = {0};
     if (ncols > 128 || nbanks > 128 || ncols + nbanks > 256) return -1;
-    for (uint32_t c = 0; c < ncols; ++c) order_cols[c] = c;
+    /* col_order[k] = the column whose bits come k-th (the reference's
+     * columnOrder, src/stitch_composer.cpp:568-612); NULL = 0..ncols-1 */
+    for (uint32_t c = 0; c < ncols; ++c) {
+        order_cols[c] = col_order ? col_order[c] : c;
+        if (order_cols[c] >= ncols || seen[order_cols[c]]) return -1;
+        seen[order_cols[c]] = 1;
+    }
     int nr = orc_plan_records(bw, ncols, order_cols, split, nbanks, rec, nrec);
     if (nr < 0) return -1;
     uint32_t r0 = 0;
@@ -374,14 +381,14 @@ static int build_banks(const void *const *cols, const uint32_t *col_bytes, const
 }
 
 int orc_run_plan_sort(const void *const *cols, const uint32_t *col_bytes,
-                      const uint32_t *bw, uint32_t ncols,
+                      const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
                       const uint32_t *split, uint32_t nbanks, uint64_t n,
                       uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
 {
     void *banks[128] = {0};
     uint32_t bb[128];
     if (nbanks == 0 || nbanks > 128) return -1;
-    int rc = build_banks(cols, col_bytes, bw, ncols, split, nbanks, n, 0, banks, bb);
+    int rc = build_banks(cols, col_bytes, bw, ncols, col_order, split, nbanks, n, 0, banks, bb);
     uint32_t *g0 = NULL, *g1 = NULL;
     if (rc == 0 && n > 0) {
         g0 = (uint32_t *)malloc(n * sizeof(uint32_t));
@@ -403,14 +410,14 @@ int orc_run_plan_sort(const void *const *cols, const uint32_t *col_bytes,
 }
 
 int orc_run_plan_hash(const void *const *cols, const uint32_t *col_bytes,
-                      const uint32_t *bw, uint32_t ncols,
+                      const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
                       const uint32_t *split, uint32_t nbanks, uint64_t n,
                       uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups)
 {
     void *banks[128] = {0};
     uint32_t bb[128];
     if (nbanks == 0 || nbanks > 128) return -1;
-    int rc = build_banks(cols, col_bytes, bw, ncols, split, nbanks, n, 1, banks, bb);
+    int rc = build_banks(cols, col_bytes, bw, ncols, col_order, split, nbanks, n, 1, banks, bb);
     uint32_t *g0 = NULL, *g1 = NULL, *idx = NULL;
     if (rc == 0 && n > 0) {
         g0 = (uint32_t *)malloc(n * sizeof(uint32_t));

@@ -103,19 +103,22 @@ int orc_hash_unordered(const void *bank, uint32_t bank_bytes, const uint32_t *in
 /* Whole plan, sort path: stitch each bank then chain the rounds
  * (run_single_plan, src/stitch_composer.cpp:555-806 + multiRoundSorting,
  * src/composer.cpp:48-135).  cols[c] has col_bytes[c] bytes per row and
- * declared width bw[c]; column order is 0..ncols-1 (RunAnInstance,
- * src/stitch_composer.cpp:4051-4120).  order_out / group_out receive the final
- * order and the final round's group vector (computed even for the last round). */
+ * declared width bw[c]; col_order[k] is the column whose bits come k-th (the
+ * reference's columnOrder, src/stitch_composer.cpp:15-35, 568-612; NULL =
+ * 0..ncols-1 as in RunAnInstance, src/stitch_composer.cpp:4051-4120).
+ * order_out / group_out receive the final order and the final round's group
+ * vector (computed even for the last round). */
 int orc_run_plan_sort(const void *const *cols, const uint32_t *col_bytes,
-                      const uint32_t *bw, uint32_t ncols,
+                      const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
                       const uint32_t *split, uint32_t nbanks, uint64_t n,
                       uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 
 /* Whole plan, hash path (run_single_plan_hash, src/stitch_composer.cpp:808-1079 +
  * multiRoundHashing_reordered, src/composer.cpp:137-227).  order_out is the
- * last round's input order, group_out the last round's group_idx. */
+ * last round's input order, group_out the last round's group_idx; col_order as
+ * for orc_run_plan_sort. */
 int orc_run_plan_hash(const void *const *cols, const uint32_t *col_bytes,
-                      const uint32_t *bw, uint32_t ncols,
+                      const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
                       const uint32_t *split, uint32_t nbanks, uint64_t n,
                       uint32_t *order_out, uint32_t *group_out, uint32_t *ngroups);
 

@@ -59,7 +59,7 @@ def lib():
                                      C.c_void_p, C.c_uint64, C.c_int, _u32p]
         L.orc_hash_unordered.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, _u32p]
         for f in (L.orc_run_plan_sort, L.orc_run_plan_hash):
-            f.argtypes = [C.POINTER(C.c_void_p), _u32p, _u32p, C.c_uint32, _u32p, C.c_uint32,
+            f.argtypes = [C.POINTER(C.c_void_p), _u32p, _u32p, C.c_uint32, _u32p, _u32p, C.c_uint32,
                           C.c_uint64, C.c_void_p, C.c_void_p, _u32p]
         _lib = L
     return _lib
@@ -186,25 +186,30 @@ def _plan_args(cols, bw, split):
     return cols, ptrs, cb, _u32arr(bw), _u32arr(split)
 
 
-def run_plan_sort(cols, bw, split):
-    """Whole sort plan; returns (order, group, ngroups)."""
+def run_plan_sort(cols, bw, split, col_order=None):
+    """Whole sort plan; returns (order, group, ngroups).  col_order[k] is the
+    column whose bits come k-th (None: 0..ncols-1)."""
     n = cols[0].shape[0]
     keep, ptrs, cb, bwa, spa = _plan_args(cols, bw, split)
+    co = None if col_order is None else _u32arr(col_order)
     order = np.zeros(n, np.uint32)
     group = np.zeros(n, np.uint32)
     ng = C.c_uint32(0)
-    _check(lib().orc_run_plan_sort(ptrs, cb, bwa, len(cols), spa, len(split), n, _ptr(order),
+    _check(lib().orc_run_plan_sort(ptrs, cb, bwa, len(cols), co, spa, len(split), n, _ptr(order),
                                    _ptr(group), C.byref(ng)), "orc_run_plan_sort")
     return order, group, ng.value
 
 
-def run_plan_hash(cols, bw, split):
+def run_plan_hash(cols, bw, split, col_order=None):
+    """Whole hash plan; returns (order, group, ngroups); col_order as for
+    run_plan_sort."""
     n = cols[0].shape[0]
     keep, ptrs, cb, bwa, spa = _plan_args(cols, bw, split)
+    co = None if col_order is None else _u32arr(col_order)
     order = np.zeros(n, np.uint32)
     group = np.zeros(n, np.uint32)
     ng = C.c_uint32(0)
-    _check(lib().orc_run_plan_hash(ptrs, cb, bwa, len(cols), spa, len(split), n, _ptr(order),
+    _check(lib().orc_run_plan_hash(ptrs, cb, bwa, len(cols), co, spa, len(split), n, _ptr(order),
                                    _ptr(group), C.byref(ng)), "orc_run_plan_hash")
     return order, group, ng.value
 
@@ -260,5 +265,11 @@ def ref_run_plan_hash(cols, bw, split):
 
 def canonicalize(order: np.ndarray, group: np.ndarray) -> np.ndarray:
     """Sort oids ascending inside each group (groups are contiguous runs)."""
+    g = np.asarray(group, np.uint64)
+    if g.size and np.all(g[1:] >= g[:-1]):
+        # ids ascend with the position: one sort of (group << 32 | oid)
+        key = (g << np.uint64(32)) | np.asarray(order, np.uint64)
+        key.sort()
+        return (key & np.uint64(0xFFFFFFFF)).astype(np.uint32)
     idx = np.lexsort((order, group))
     return order[idx]

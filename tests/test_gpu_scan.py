@@ -16,7 +16,9 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [1, 2, 33, 1000, 8191, 8192, 8193, 70_001, 1_000_003]
+# tile counts (8,192 rows a tile) odd and even, among them 5 and 25 tiles: the
+# workspace's sub-arrays start on 256-byte boundaries whatever the tile count
+SIZES = [1, 2, 33, 1000, 8191, 8192, 8193, 40_960, 70_001, 200_000, 1_000_003]
 
 
 def _as_int(a):

@@ -118,3 +118,32 @@ def test_hash_plan_vs_reference_live(split):
     o, g, ng = O.run_plan_hash(cols, bw, split)
     ro, rg, _ = O.ref_run_plan_hash(cols, bw, split)
     assert np.array_equal(o, ro) and np.array_equal(g, rg)
+
+
+@need_ref
+@pytest.mark.parametrize("path", ["sort", "hash"])
+@pytest.mark.parametrize("col_order,split", [([2, 0, 1], [27]), ([1, 2, 0], [19, 8]), ([0, 2, 1], [8, 19])])
+def test_plan_column_order_vs_reference_live(path, col_order, split):
+    """A GROUP BY column order (src/stitch_composer.cpp:15-35, 3877-3882): the
+    oracle's col_order against the reference run on the columns permuted the
+    same way (its records take final_idx = columnOrder[k],
+    src/stitch_composer.cpp:568-612)."""
+    cols, bw = W.cols_uniform(32768, [8, 12, 7], seed_index=13, distinct=[16, 300, 0])
+    pc = [cols[c] for c in col_order]
+    pb = [bw[c] for c in col_order]
+    if path == "sort":
+        o, g, ng = O.run_plan_sort(cols, bw, split, col_order=col_order)
+        ro, rg, _ = O.ref_run_plan_sort(pc, pb, split)
+        assert np.array_equal(g, rg) and np.array_equal(o, O.canonicalize(ro, rg))
+    else:
+        o, g, ng = O.run_plan_hash(cols, bw, split, col_order=col_order)
+        ro, rg, _ = O.ref_run_plan_hash(pc, pb, split)
+        assert np.array_equal(o, ro) and np.array_equal(g, rg)
+    assert ng == int(g.max()) + 1
+
+
+def test_plan_column_order_rejects_bad_orders():
+    cols, bw = W.cols_uniform(100, [8, 12, 7], seed_index=13)
+    for bad in ([0, 0, 1], [0, 1, 3]):
+        with pytest.raises(RuntimeError):
+            O.run_plan_sort(cols, bw, [27], col_order=bad)
