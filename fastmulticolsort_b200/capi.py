@@ -34,7 +34,7 @@ EXPORTS = (
     "fmcs_server_create", "fmcs_server_submit", "fmcs_server_wait", "fmcs_server_load", "fmcs_server_destroy",
     "fmcs_graph_create", "fmcs_graph_launch", "fmcs_graph_stream", "fmcs_graph_destroy", "fmcs_graph_kernels",
     "fmcs_storage_bytes", "fmcs_text_header", "fmcs_read_columns_text", "fmcs_write_columns_text",
-    "fmcs_group_aggregate",
+    "fmcs_group_aggregate", "fmcs_selftest_wait", "fmcs_graph_create_hash",
 )
 
 
@@ -104,6 +104,7 @@ def load(path: str = LIB_PATH):
                                      u64, i32, vp, vp, u32p]
     L.fmcs_profile.argtypes = [vp, i32]
     L.fmcs_profile_report.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.fmcs_selftest_wait.argtypes = [vp, u32]
     L.fmcs_launch_count.argtypes = [vp]
     L.fmcs_launch_count.restype = C.c_ulonglong
     L.fmcs_group_ids_noalloc.argtypes = [vp, vp, u32, vp, vp, u64, u32p]
@@ -114,6 +115,8 @@ def load(path: str = LIB_PATH):
     L.fmcs_run_batch.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32, C.POINTER(Instance), u32, u64,
                                  vp, vp, u32p]
     L.fmcs_graph_create.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32p, u32, u64, vp, vp, C.POINTER(vp)]
+    L.fmcs_graph_create_hash.argtypes = [vp, C.POINTER(vp), u32p, u32p, u32, u32p, u32p, u32, u64, vp, vp,
+                                         C.POINTER(vp)]
     L.fmcs_graph_launch.argtypes = [vp, u32p]
     L.fmcs_graph_stream.argtypes = [vp]
     L.fmcs_graph_stream.restype = vp
@@ -291,6 +294,11 @@ class Context:
         self._check(self._L.fmcs_profile_report(self._h, buf, len(buf)))
         return json.loads(buf.value.decode())
 
+    def selftest_wait(self, polls: int) -> int:
+        """fmcs_selftest_wait: a bounded device wait on a word nothing writes;
+        returns the status code (FMCS_E_TIMEOUT when the wait gave up)."""
+        return int(self._L.fmcs_selftest_wait(self._h, int(polls)))
+
     def launch_count(self) -> int:
         return int(self._L.fmcs_launch_count(self._h))
 
@@ -363,8 +371,11 @@ class Context:
         return ng.value
 
     # -- CUDA graph of a whole plan -----------------------------------------
-    def plan_graph(self, cols, bw, split, order_out, group_out=None, col_order=None) -> "PlanGraph":
-        return PlanGraph(self, cols, bw, split, order_out, group_out, col_order)
+    def plan_graph(self, cols, bw, split, order_out, group_out=None, col_order=None,
+                   hash: bool = False) -> "PlanGraph":
+        """A CUDA graph of the plan (fmcs_graph_create, or with hash the
+        hash-grouping plan: fmcs_graph_create_hash)."""
+        return PlanGraph(self, cols, bw, split, order_out, group_out, col_order, hash)
 
     # -- many instances ----------------------------------------------------
     def run_batch(self, cols, bw, split, sizes, order_out, group_out=None):
@@ -417,7 +428,8 @@ class Context:
 class PlanGraph:
     """fmcs_graph: a sort plan captured once, replayed with launch()."""
 
-    def __init__(self, ctx: "Context", cols, bw, split, order_out, group_out=None, col_order=None):
+    def __init__(self, ctx: "Context", cols, bw, split, order_out, group_out=None, col_order=None,
+                 hash: bool = False):
         self._L = load()
         self._ctx = ctx
         n = _len(cols[0])
@@ -425,9 +437,10 @@ class PlanGraph:
         ptrs = (C.c_void_p * len(cols))(*[_addr(c) for c in cols])
         co = None if col_order is None else _u32arr(col_order)
         h = C.c_void_p()
-        rc = self._L.fmcs_graph_create(ctx.handle, ptrs, _u32arr([_itemsize(c) for c in cols]), _u32arr(bw),
-                                       len(cols), co, _u32arr(split), len(split), n, _addr(order_out),
-                                       _addr(group_out), C.byref(h))
+        create = self._L.fmcs_graph_create_hash if hash else self._L.fmcs_graph_create
+        rc = create(ctx.handle, ptrs, _u32arr([_itemsize(c) for c in cols]), _u32arr(bw),
+                    len(cols), co, _u32arr(split), len(split), n, _addr(order_out),
+                    _addr(group_out), C.byref(h))
         ctx._check(rc)
         self._h = h
 

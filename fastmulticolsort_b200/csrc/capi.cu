@@ -175,11 +175,18 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
         // round 0 of a sort plan over more rows than one block sorts: the
         // stitch also counts the first radix level's histogram
         uint32_t *top_hist = nullptr;
+        uint16_t *tile_cnt = nullptr;
         if (!hash && !in_group && n > ctx->local_max) {
             if ((rc = ws_get(ctx, kSlotTopHist, 256 * sizeof(uint32_t), &p))) return rc;
             top_hist = (uint32_t *)p;
+            uint32_t *tdst;
+            uint4 *tinfo;
+            unsigned long long *clb;
+            if ((rc = level_tile_arrays(ctx, n, sort_tile_rows(ctx), &tile_cnt, &tdst, &tinfo, &clb))) return rc;
         }
-        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits))) return rc;
+        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits, tile_cnt,
+                                sort_tile_rows(ctx))))
+            return rc;
         uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
         if (!hash) {
             // (b)+(d): sort, then group ids (+ the next round's segments)
@@ -196,7 +203,7 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
                 if ((rc = launch_iota(ctx, dorder, n))) return rc;
                 oin = dorder;
             }
-            if ((rc = hash_round(ctx, bank, bp.bytes, oin, dorder, in_group, og, n, last, d_ng)))
+            if ((rc = hash_round(ctx, bank, bp.bytes, oin, dorder, in_group, og, n, last, d_ng, false, fixed)))
                 return rc;
         }
         in_group = og;
@@ -791,10 +798,9 @@ extern "C" void fmcs_graph_destroy(fmcs_graph *g)
     delete g;
 }
 
-extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, const uint32_t *col_bytes,
-                                 const uint32_t *bw, uint32_t ncols, const uint32_t *col_order, const uint32_t *split,
-                                 uint32_t nbanks, uint64_t n, uint32_t *order_out, uint32_t *group_out,
-                                 fmcs_graph **out)
+static int graph_create(fmcs_ctx *parent, const void *const *cols, const uint32_t *col_bytes, const uint32_t *bw,
+                        uint32_t ncols, const uint32_t *col_order, const uint32_t *split, uint32_t nbanks, uint64_t n,
+                        bool hash, uint32_t *order_out, uint32_t *group_out, fmcs_graph **out)
 {
     if (!parent || !out) return FMCS_E_INVAL;
     *out = nullptr;
@@ -814,7 +820,7 @@ extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, cons
     for (uint32_t c = 0; c < ncols; ++c) corder[c] = col_order ? col_order[c] : c;
     Plan plan;
     std::string perr;
-    if (!build_plan(bw, ncols, corder.data(), split, nbanks, false, plan, perr))
+    if (!build_plan(bw, ncols, corder.data(), split, nbanks, hash, plan, perr))
         return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: " + perr);
     fmcs_graph *g = new fmcs_graph();
     int rc = fmcs_create(&g->ctx, parent->device, 0);
@@ -827,7 +833,7 @@ extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, cons
     ctx->local_max = parent->local_max;
     ctx->msd_items = parent->msd_items;
     // 1) one eager run of the fixed launch sequence sizes every workspace slot
-    rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, false, order_out, group_out, true, &g->d_ng);
+    rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, hash, order_out, group_out, true, &g->d_ng);
     if (!rc) rc = check_status(ctx, "fmcs_graph_create warm-up");
     // 2) capture: reset the look-back words (their epochs repeat on every
     //    replay), then the same launches
@@ -837,7 +843,7 @@ extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, cons
             for (int slot : {kSlotLookback, kSlotScanTiles})
                 if (ctx->ws.ptr[slot]) cudaMemsetAsync(ctx->ws.ptr[slot], 0, ctx->ws.cap[slot], ctx->stream);
             const unsigned long long l0 = ctx->launches;   // every launch site counts itself
-            rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, false, order_out, group_out, true, &g->d_ng);
+            rc = plan_pipeline(ctx, plan, cols, col_bytes, bw, n, hash, order_out, group_out, true, &g->d_ng);
             g->kernels = ctx->launches - l0;
             cudaGraph_t graph = nullptr;
             e = cudaStreamEndCapture(ctx->stream, &graph);
@@ -853,6 +859,24 @@ extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, cons
     }
     *out = g;
     return FMCS_OK;
+}
+
+extern "C" int fmcs_graph_create(fmcs_ctx *parent, const void *const *cols, const uint32_t *col_bytes,
+                                 const uint32_t *bw, uint32_t ncols, const uint32_t *col_order, const uint32_t *split,
+                                 uint32_t nbanks, uint64_t n, uint32_t *order_out, uint32_t *group_out,
+                                 fmcs_graph **out)
+{
+    return graph_create(parent, cols, col_bytes, bw, ncols, col_order, split, nbanks, n, false, order_out, group_out,
+                        out);
+}
+
+extern "C" int fmcs_graph_create_hash(fmcs_ctx *parent, const void *const *cols, const uint32_t *col_bytes,
+                                      const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
+                                      const uint32_t *split, uint32_t nbanks, uint64_t n, uint32_t *order_out,
+                                      uint32_t *group_out, fmcs_graph **out)
+{
+    return graph_create(parent, cols, col_bytes, bw, ncols, col_order, split, nbanks, n, true, order_out, group_out,
+                        out);
 }
 
 extern "C" int fmcs_graph_launch(fmcs_graph *g, uint32_t *ngroups)

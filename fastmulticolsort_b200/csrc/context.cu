@@ -2,6 +2,7 @@
 // on demand and are reused across calls; the reference instead mallocs and
 // frees every buffer per call, src/common.h:18-31), the device status word that
 // bounded waits report through, and error strings.
+#include "device_common.cuh"
 #include "fmcs_internal.h"
 
 #include <dlfcn.h>
@@ -73,6 +74,55 @@ int ws_get(fmcs_ctx *ctx, int slot, size_t bytes, void **out, bool zero_new)
     w.cap[slot] = want;
     ctx->held += want;
     *out = p;
+    return FMCS_OK;
+}
+
+int cond_handle(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle *h)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cond_handle: capture info");
+    if (cs != cudaStreamCaptureStatusActive) return set_error(ctx, FMCS_E_INVAL, "cond_handle: stream not capturing");
+    e = cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault);
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "cond_handle: create");
+}
+
+int capture_if(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle h,
+               const std::function<int(cudaStream_t)> &body)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: capture info");
+    if (cs != cudaStreamCaptureStatusActive) return set_error(ctx, FMCS_E_INVAL, "capture_if: stream not capturing");
+    if (!ctx->side) {
+        e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: stream");
+    }
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, deps, ndeps, &np);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: node");
+    cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: dependencies");
+    e = cudaStreamBeginCaptureToGraph(ctx->side, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: body capture");
+    cudaStream_t saved = ctx->stream;
+    ctx->stream = ctx->side;
+    int rc = body(ctx->side);
+    ctx->stream = saved;
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(ctx->side, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: body end");
     return FMCS_OK;
 }
 
@@ -400,4 +450,45 @@ extern "C" long long fmcs_get_tuning(const fmcs_ctx *ctx, const char *key)
     if (k == "local_max") return ctx->local_max;
     if (k == "msd_items") return ctx->msd_items;
     return -1;
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded device waits: one warp waits, through lb_wait (the
+// wait every look-back of the library uses), on a word of the workspace that
+// no kernel writes.  The wait must give up after `polls` polls, record
+// FMCS_E_TIMEOUT in the context's status word and return, leaving the
+// context usable.
+// ---------------------------------------------------------------------------
+namespace fmcs {
+namespace {
+__global__ void selftest_wait_kernel(const unsigned long long *word, uint32_t epoch, int *status, uint32_t polls,
+                                     uint32_t *out)
+{
+    kernel_prologue();
+    const unsigned long long w = lb_wait(word, epoch, status, polls);
+    if (threadIdx.x == 0) *out = (uint32_t)w;
+}
+}  // namespace
+}  // namespace fmcs
+
+extern "C" int fmcs_selftest_wait(fmcs_ctx *ctx, uint32_t polls)
+{
+    using namespace fmcs;
+    if (!ctx) return FMCS_E_INVAL;
+    if (polls < 1 || polls > (1u << 20)) return set_error(ctx, FMCS_E_INVAL, "polls must be in 1..2^20");
+    void *p = nullptr;
+    int rc = ws_get(ctx, kSlotMisc, 256, &p);
+    if (rc) return rc;
+    // a zero word carries epoch 0 and no flag: a wait for epoch 1 never ends
+    // on it, and nothing else writes the word while this call runs
+    cudaError_t e = cudaMemsetAsync(p, 0, 256, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "selftest memset");
+    {
+        LaunchScope ls_(ctx, "selftest_wait");
+        launch_k(selftest_wait_kernel, 1, 32, 0, ctx->stream, (const unsigned long long *)p, 1u, ctx->d_status,
+                 polls, (uint32_t *)p + 16);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "selftest launch");
+    return check_status(ctx, "fmcs_selftest_wait");
 }

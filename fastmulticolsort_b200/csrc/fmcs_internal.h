@@ -50,6 +50,8 @@ enum Slot : int {
     kSlotGroupB,      // run_plan group pong
     kSlotColStage,    // run_plan host column staging (several columns)
     kSlotTopHist,     // level-0 digit histogram of a round-0 bank, counted by the stitch
+    kSlotTileCnt,     // per-tile digit counts of an HBM radix level (level 0's from the stitch)
+    kSlotTileDst,     // per-tile digit destinations and tile descriptors of an HBM radix level
     kSlotMisc,
     kSlotCount
 };
@@ -153,6 +155,14 @@ class LaunchScope {
 int capture_while(fmcs_ctx *ctx, cudaStream_t st,
                   const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body);
 
+// A conditional handle of the graph being captured on `st` (default 0 at
+// every graph launch), and an IF node on it whose body is captured from
+// body(stream): the body runs when a kernel earlier in the graph has set the
+// handle to non-zero (cudaGraphSetConditional).
+int cond_handle(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle *h);
+int capture_if(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle h,
+               const std::function<int(cudaStream_t)> &body);
+
 // Launches a library kernel with programmatic stream serialization: it may
 // begin launching while the stream's previous kernel finishes (its prologue
 // waits for that kernel's completion).  Every kernel launched this way starts
@@ -187,9 +197,11 @@ struct StitchSlice {
 constexpr int kMaxSlices = 32;
 // With top_hist (device, 256 words), the stitch also counts the top digit
 // (bits [key_bits - min(8, key_bits), key_bits)) of every bank value: the
-// first radix level's histogram of a round-0 sort of the bank.
+// first radix level's histogram of a round-0 sort of the bank, in all
+// (top_hist) and per tile of tile_rows rows (tile_cnt, 256 u16 per tile).
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0);
+                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0, uint16_t *tile_cnt = nullptr,
+                  uint32_t tile_rows = 0);
 
 // bank[i] <<= lshift (src == NULL) or bank[i] |= (src[i] >> rshift) & mask(width)
 int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,
@@ -213,8 +225,23 @@ struct SortArgs {
     uint64_t n;
     bool fixed_launches = false;  // launch every level (no host read-back), e.g. under graph capture
     const uint32_t *top_hist = nullptr;  // round 0 only: the first level's digit histogram, already counted
+    // Device-side overrides read by the round's first kernel (no host
+    // read-back): the significant key bits (<= key_bits, which then only
+    // bounds the number of radix levels), and a flag that, when non-zero,
+    // says the rows are in order already (every segment is only copied).
+    const uint32_t *d_key_bits = nullptr;
+    const uint32_t *d_in_order = nullptr;
 };
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
+// Rows of an HBM radix tile (the context's msd_items x 256 threads), and the
+// most tiles one radix level of a sort of n rows can have.
+uint32_t sort_tile_rows(const fmcs_ctx *ctx);
+uint64_t sort_level_tiles(const fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows);
+// The per-tile arrays of the radix levels (workspace slots kSlotTileCnt,
+// kSlotTileDst, kSlotLookback), sized for a sort of n rows in tiles of
+// tile_rows rows.
+int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo,
+                      unsigned long long **clb);
 // Stable full-array LSD radix sort of (keys, vals) in place by key bits
 // [0, bits): the plain, unsegmented comparator path.
 int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits);
@@ -240,8 +267,10 @@ int launch_iota(fmcs_ctx *ctx, uint32_t *v, uint64_t n);
 int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64_t n, uint32_t *d_count);
 
 // ---------------------------------------------------------------- hash grouping
+// fixed_launches: the same launches whatever the data, with no host
+// read-back (graph capture).
 int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
                uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n,
-               bool last_round, uint32_t *d_ngroups, bool group_is_key = false);
+               bool last_round, uint32_t *d_ngroups, bool group_is_key = false, bool fixed_launches = false);
 
 }  // namespace fmcs

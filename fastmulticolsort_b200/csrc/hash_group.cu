@@ -62,12 +62,14 @@ constexpr uint32_t kAlone = 0xFFFFFFFFu;
 template <typename K>
 __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ bank, const uint32_t *__restrict__ order,
                                                           const uint32_t *__restrict__ run, bool runs_contiguous,
+                                                          const uint32_t *__restrict__ seg_start, uint32_t onchip_max,
                                                           uint64_t n, unsigned long long *slots, uint64_t mask,
                                                           uint32_t *slot_of, int *status)
 {
     kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t r = run ? run[i] : 0u;
+        if (seg_start && seg_start[r + 1] - seg_start[r] <= onchip_max) continue;   // numbered on chip
         if (runs_contiguous && (i == 0 || run[i - 1] != r) && (i + 1 == n || run[i + 1] != r)) {
             slot_of[i] = kAlone;
             continue;
@@ -106,12 +108,86 @@ __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ 
     }
 }
 
+// slot_of of a row whose parent run was numbered in shared memory: its fpos
+// and first flag are written already.
+constexpr uint32_t kDoneOnChip = 0xFFFFFFFEu;
+
+// Parent runs of up to kRunOnChip rows are numbered by one CTA each in shared
+// memory (the reference's block-local tables, Hashing::calculate_hash_in_block,
+// src/hashing.h:178-287): the run's keys are staged in shared memory, every
+// row claims or finds its key's slot of an open-addressing table of positions
+// (at least twice as many slots as rows) and lowers the slot to its own
+// position with a shared atomicMin, so a slot ends at its key's first
+// appearance in the run.  Longer runs go through the global table.
+constexpr uint32_t kRunOnChip = 2048;
+constexpr uint32_t kRunOnChipSlots = 2 * kRunOnChip;
+
+template <typename K>
+__global__ void __launch_bounds__(256) hash_runs_onchip_kernel(const K *__restrict__ bank,
+                                                               const uint32_t *__restrict__ order,
+                                                               const uint32_t *__restrict__ seg_start,
+                                                               const uint32_t *d_nseg, uint32_t *slot_of,
+                                                               uint32_t *fpos, uint8_t *first)
+{
+    kernel_prologue();
+    __shared__ K keys[kRunOnChip];
+    __shared__ uint32_t table[kRunOnChipSlots];
+    __shared__ uint16_t slot_at[kRunOnChip];
+    const uint32_t nseg = *d_nseg;
+    for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
+        const uint32_t start = seg_start[s];
+        const uint32_t len = seg_start[s + 1] - start;
+        if (len > kRunOnChip) continue;   // the same for the whole block
+        if (len == 1) {
+            if (threadIdx.x == 0) {
+                fpos[start] = start;
+                first[start] = 1;
+                slot_of[start] = kDoneOnChip;
+            }
+            continue;
+        }
+        uint32_t ts = 64;
+        while (ts < 2 * len) ts <<= 1;
+        for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0xFFFFFFFFu;
+        for (uint32_t p = threadIdx.x; p < len; p += blockDim.x)
+            keys[p] = order ? bank[order[start + p]] : bank[start + p];
+        __syncthreads();
+        for (uint32_t p = threadIdx.x; p < len; p += blockDim.x) {
+            const K k = keys[p];
+            uint32_t h = (uint32_t)mix64((uint64_t)k) & (ts - 1);
+            for (uint32_t probe = 0; probe < ts; ++probe) {   // ts > len: a free or matching slot exists
+                uint32_t cur = table[h];
+                if (cur == 0xFFFFFFFFu) {
+                    const uint32_t prev = atomicCAS(&table[h], 0xFFFFFFFFu, p);
+                    if (prev == 0xFFFFFFFFu) break;
+                    cur = prev;
+                }
+                if (keys[cur] == k) {
+                    atomicMin(&table[h], p);
+                    break;
+                }
+                h = (h + 1) & (ts - 1);
+            }
+            slot_at[p] = (uint16_t)h;
+        }
+        __syncthreads();
+        for (uint32_t p = threadIdx.x; p < len; p += blockDim.x) {
+            const uint32_t f = table[slot_at[p]];
+            fpos[start + p] = start + f;
+            first[start + p] = f == p ? 1 : 0;
+            slot_of[start + p] = kDoneOnChip;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void first_flag_kernel(const uint32_t *__restrict__ slot_of, const unsigned long long *__restrict__ slots,
                                   uint8_t *__restrict__ first, uint32_t *__restrict__ fpos, uint64_t n)
 {
     kernel_prologue();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t so = slot_of[i];
+        if (so == kDoneOnChip) continue;
         const uint32_t f = so == kAlone ? (uint32_t)i : (uint32_t)slots[so];
         fpos[i] = f;
         first[i] = (f == (uint32_t)i) ? 1 : 0;
@@ -120,28 +196,48 @@ __global__ void first_flag_kernel(const uint32_t *__restrict__ slot_of, const un
 
 // id(i) = rank(f(i)); with `row_ids` also scatter the id to the row it
 // belongs to (row-indexed, the layout the segmented sort gathers from).
+// With `clustered` (a word that starts non-zero), a position whose id is
+// smaller than its predecessor's clears it: the ids of consecutive runs
+// ascend, so a word still set at the end says that every run's rows are in
+// id order already and the stable clustering moves nothing.  With
+// `key_bits`, the bits of the largest id (the group count less one).
 __global__ void assign_ids_kernel(const uint32_t *__restrict__ fpos, const uint32_t *__restrict__ rank,
                                   const uint32_t *__restrict__ order, uint32_t *__restrict__ ids,
-                                  uint32_t *__restrict__ row_ids, uint64_t n)
+                                  uint32_t *__restrict__ row_ids, uint64_t n, uint32_t *clustered,
+                                  const uint32_t *d_ngroups, uint32_t *key_bits)
 {
     kernel_prologue();
+    if (key_bits && blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t g = *d_ngroups;
+        *key_bits = g <= 1 ? 0u : 32u - (uint32_t)__clz(g - 1);
+    }
+    bool descent = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t g = rank[fpos[i]];
         if (ids) ids[i] = g;
         if (row_ids) row_ids[order ? order[i] : (uint32_t)i] = g;
+        if (clustered && i > 0 && rank[fpos[i - 1]] > g) descent = true;
     }
+    if (clustered && __any_sync(0xFFFFFFFFu, descent) && (threadIdx.x & 31) == 0) *clustered = 0u;
 }
 
+// The round's numbering: with parent-run starts (seg_start, *d_nseg runs),
+// runs of up to kRunOnChip rows in shared memory, the others in the global
+// table; without, every row in the global table.
 template <typename K>
 int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const uint32_t *run, bool runs_contiguous,
-                uint64_t n, unsigned long long *slots, uint64_t mask, uint32_t *slot_of)
+                const uint32_t *seg_start, const uint32_t *d_nseg, uint64_t n, unsigned long long *slots,
+                uint64_t mask, uint32_t *slot_of, uint32_t *fpos, uint8_t *first)
 {
     const unsigned grid = (unsigned)ctx->num_sms * 8;
+    if (seg_start) {
+        LaunchScope ls_(ctx, "hash_runs_onchip");
+        launch_k(hash_runs_onchip_kernel<K>, grid, 256, 0, ctx->stream, (const K *)bank, order, seg_start, d_nseg,
+                 slot_of, fpos, first);
+    }
     { LaunchScope ls_(ctx, "hash_insert");
-        launch_k(hash_insert_kernel<K>, grid, 256, 0, ctx->stream,
-                 (const K *)bank, order, run, runs_contiguous, n, slots, mask,
-                                                            slot_of,
-                                                            ctx->d_status);
+        launch_k(hash_insert_kernel<K>, grid, 256, 0, ctx->stream, (const K *)bank, order, run, runs_contiguous,
+                 seg_start, kRunOnChip, n, slots, mask, slot_of, ctx->d_status);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "hash insert launch");
@@ -151,7 +247,7 @@ int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const ui
 
 int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
                uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n, bool last_round,
-               uint32_t *d_ngroups, bool group_is_key)
+               uint32_t *d_ngroups, bool group_is_key, bool fixed_launches)
 {
     if (n == 0) return FMCS_OK;
     cudaStream_t st = ctx->stream;
@@ -181,15 +277,22 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     if (in_group && group_is_key) {
         keyrun = in_group;
     } else if (in_group) {
-        if ((rc = launch_group_ids(ctx, nullptr, 0, in_group, run, n, nullptr))) return rc;
+        // run ids and run starts in one boundary scan of in_group
+        if ((rc = ws_get(ctx, kSlotSegStart, (n + 2) * sizeof(uint32_t), &p))) return rc;
+        seg_start = (uint32_t *)p;
+        if ((rc = launch_group_ids_segments(ctx, nullptr, 0, in_group, run, seg_start, n, d_cnt))) return rc;
         keyrun = run;
         contiguous = true;
     }
     switch (bank_bytes) {
-    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
-    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
-    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
-    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, contiguous, n, slots, cap - 1, slot_of); break;
+    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
+                                      slot_of, fpos, first); break;
+    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
+                                       slot_of, fpos, first); break;
+    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
+                                       slot_of, fpos, first); break;
+    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
+                                       slot_of, fpos, first); break;
     default: return set_error(ctx, FMCS_E_INVAL, "hash round: bank_bytes must be 1, 2, 4 or 8");
     }
     if (rc) return rc;
@@ -201,7 +304,8 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     if ((rc = launch_flag_rank(ctx, first, rank, n, d_ngroups))) return rc;
     if (last_round) {
         { LaunchScope ls_(ctx, "assign_ids");
-            launch_k(assign_ids_kernel, grid, 256, 0, st, fpos, rank, nullptr, out_group, nullptr, n);
+            launch_k(assign_ids_kernel, grid, 256, 0, st, fpos, rank, nullptr, out_group, nullptr, n, nullptr,
+                     (const uint32_t *)d_ngroups, nullptr);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(ctx, e, "hash ids launch");
@@ -216,19 +320,21 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     // clustering: stable sort of (id, oid) inside each parent run; ids are
     // scattered to row order so that the sort's gather through order_in reads them.
     uint32_t *row_ids = run;   // run ids are dead after the insert
+    // the sort's key width (the bits of the largest id) and whether the ids
+    // are in order already are decided on the device: no read-back
+    uint32_t *d_clustered = d_cnt + 2, *d_kbits = d_cnt + 3;
+    cudaMemsetAsync(d_clustered, 0xFF, sizeof(uint32_t), st);
     { LaunchScope ls_(ctx, "assign_ids");
-        launch_k(assign_ids_kernel, grid, 256, 0, st, fpos, rank, order_in, nullptr, row_ids, n);
+        launch_k(assign_ids_kernel, grid, 256, 0, st, fpos, rank, order_in, nullptr, row_ids, n, d_clustered,
+                 (const uint32_t *)d_ngroups, d_kbits);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "hash ids launch");
-    // key width: read the group count back
-    cudaMemcpyAsync(ctx->h_small, d_ngroups, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "hash round sync");
-    const uint32_t G = ctx->h_small[0];
-    uint32_t bits = 1;
-    while (bits < 32 && (1ull << bits) < (uint64_t)G) bits++;
-    if (in_group) {
+    uint32_t bits = 1;   // ids < n: a bound on the key width, which sets the most radix levels
+    while (bits < 32 && (1ull << bits) < n) bits++;
+    if (in_group && !seg_start) {
+        // previous ids as the key (unclustered rows): the clustering's segments
+        // are still the runs of equal in_group
         if ((rc = ws_get(ctx, kSlotSegStart, (n + 2) * sizeof(uint32_t), &p))) return rc;
         seg_start = (uint32_t *)p;
         if ((rc = launch_segments(ctx, in_group, seg_start, d_cnt, n))) return rc;
@@ -244,6 +350,9 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     a.order_out = order_out;
     a.keys_out = out_group;
     a.n = n;
+    a.fixed_launches = fixed_launches;
+    a.d_key_bits = d_kbits;
+    a.d_in_order = d_clustered;
     return sort_segments(ctx, a);
 }
 

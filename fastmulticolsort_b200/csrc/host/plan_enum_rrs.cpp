@@ -14,7 +14,7 @@ PlanEnumRRS::PlanEnumRRS(uint64_t num_rows, uint32_t col_width_sum, uint32_t max
     : RRS<std::vector<uint32_t>, double>(0.99, 0.1, 0.99, 0.8, 0.5, 0.001), num_rows_(num_rows),
       col_width_sum_(col_width_sum), max_round_(std::max<uint32_t>(1, max_round)), columnOrder_(column_order),
       num_columns_(num_columns), bw_(bw), base_col_card_(base_col_card), time_limit_(time_limit),
-      start_(std::chrono::steady_clock::now()), tables_(GpuCostTables::Default()), rng_(0xF17C0001ull)
+      start_(std::chrono::steady_clock::now()), tables_(GpuCostTables::Cached()), rng_(0xF17C0001ull)
 {
 }
 

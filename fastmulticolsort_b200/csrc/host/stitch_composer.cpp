@@ -111,6 +111,12 @@ GpuCostTables GpuCostTables::Default()
     return t;
 }
 
+const GpuCostTables &GpuCostTables::Cached()
+{
+    static const GpuCostTables tables = Default();   // read once per process
+    return tables;
+}
+
 double GpuCostTables::SortGroupMs(double g, uint32_t bank_bytes, uint32_t key_bits) const
 {
     if (g <= 1.0) return 0.0;
@@ -139,7 +145,7 @@ double GpuCostTables::SortRoundMs(uint64_t n, double g, uint32_t bank_bytes, uin
 // ============================================================ StitchComposer
 StitchComposer::StitchComposer(setting_t setting, uint32_t ncolumns, uint64_t nrows, compose_params_t params,
                                Column **column_values)
-    : Composer(setting, ncolumns, nrows, params, column_values), tables_(GpuCostTables::Default())
+    : Composer(setting, ncolumns, nrows, params, column_values), tables_(GpuCostTables::Cached())
 {
     // cardinality carried by each bit of each column, and the shrink factor
     // (reference: src/stitch_composer.h:16-43)
@@ -161,15 +167,15 @@ StitchComposer::StitchComposer(setting_t setting, uint32_t ncolumns, uint64_t nr
 
 double StitchComposer::estimate_mergesort_uint16(double nitems)
 {
-    return GpuCostTables::Default().SortGroupMs(nitems, 2, 16);
+    return GpuCostTables::Cached().SortGroupMs(nitems, 2, 16);
 }
 double StitchComposer::estimate_mergesort_uint32(double nitems)
 {
-    return GpuCostTables::Default().SortGroupMs(nitems, 4, 32);
+    return GpuCostTables::Cached().SortGroupMs(nitems, 4, 32);
 }
 double StitchComposer::estimate_mergesort_uint64(double nitems)
 {
-    return GpuCostTables::Default().SortGroupMs(nitems, 8, 64);
+    return GpuCostTables::Cached().SortGroupMs(nitems, 8, 64);
 }
 
 double StitchComposer::estimate_stitch(uint32_t assembleStatistics[][3], uint32_t shiftStatistics[], uint32_t nitems)
@@ -181,13 +187,13 @@ double StitchComposer::estimate_stitch(uint32_t assembleStatistics[][3], uint32_
     for (int from = 0; from < 3; ++from)
         for (int to = 0; to < 3; ++to) moved += assembleStatistics[from][to] * bytes[from];
     for (int to = 0; to < 3; ++to) moved += (shiftStatistics[to] ? 1 : 0) * bytes[to];
-    return GpuCostTables::Default().stitch_per_byte * moved * (double)nitems / 1e6;
+    return GpuCostTables::Cached().stitch_per_byte * moved * (double)nitems / 1e6;
 }
 
 double StitchComposer::estimate_tuple_reconstruct(const uint32_t *bytewidths, const uint32_t column_num,
                                                   const uint64_t rows_num)
 {
-    const GpuCostTables t = GpuCostTables::Default();
+    const GpuCostTables &t = GpuCostTables::Cached();
     double ms = 0.0;
     for (uint32_t c = 1; c < column_num; ++c) ms += t.gather[GpuCostTables::BankIndex(bytewidths[c])] * rows_num / 1e6;
     return ms;

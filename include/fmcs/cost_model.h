@@ -42,8 +42,12 @@ struct FMCS_CXX_API GpuCostTables {
     /** Read a table written by the autotuner (JSON); false if absent/invalid. */
     bool Load(const std::string &path);
     /** The tables of the autotuner's last run next to libfmcs.so
-     *  (tuning/b200.json), or FMCS_TUNING, or the built-in defaults. */
+     *  (tuning/b200.json), or FMCS_TUNING, or the built-in defaults, read
+     *  from the file on every call. */
     static GpuCostTables Default();
+    /** Default() read once per process (on the first call) and kept: the
+     *  tables the composers and the static estimate_* functions use. */
+    static const GpuCostTables &Cached();
 
     /** Estimated ms to sort ONE group of g rows of the given bank width. */
     double SortGroupMs(double g, uint32_t bank_bytes, uint32_t key_bits) const;

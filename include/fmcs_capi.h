@@ -71,6 +71,14 @@ FMCS_API size_t fmcs_workspace_bytes(const fmcs_ctx *ctx);
  * where the launcher knows them (the MSD scatter passes), else 0. */
 FMCS_API int fmcs_profile(fmcs_ctx *ctx, int enable);
 FMCS_API int fmcs_profile_report(fmcs_ctx *ctx, char *buf, size_t len);
+/* Self-test of the bounded device waits (no reference counterpart; the
+ * reference has no device code).  Every device-side wait of the library (the
+ * decoupled look-backs) polls a bounded number of times, then records
+ * FMCS_E_TIMEOUT in the context's status word and lets its kernel finish.
+ * This call runs that same wait on a word that nothing writes, with a limit of
+ * `polls` polls (1..2^20), and returns what the host then reads:
+ * FMCS_E_TIMEOUT, with the status word cleared and the context usable. */
+FMCS_API int fmcs_selftest_wait(fmcs_ctx *ctx, uint32_t polls);
 /* Number of kernels this context has launched since it was created. */
 FMCS_API unsigned long long fmcs_launch_count(const fmcs_ctx *ctx);
 
@@ -239,14 +247,21 @@ FMCS_API int fmcs_write_columns_text(const char *path, int with_header, uint32_t
  * It runs in a private context (own stream and workspace, sized by one eager
  * run at creation); every radix level is part of the graph and exits on the
  * device when it has no work, so a replay needs no host round trip until its
- * final status check.  Sort plans only (hash rounds read a count back).
- * fmcs_graph_launch returns when the results are complete; fmcs_graph_stream
- * is the graph's stream. */
+ * final status check; the on-chip tiers that a replay's data leaves empty are
+ * skipped on the device.  fmcs_graph_create_hash captures the same plan
+ * through the hash-grouping rounds (run_single_plan_hash,
+ * src/stitch_composer.cpp:808-1079), whose key widths and clustering are also
+ * decided on the device.  fmcs_graph_launch returns when the results are
+ * complete; fmcs_graph_stream is the graph's stream. */
 typedef struct fmcs_graph fmcs_graph;
 FMCS_API int fmcs_graph_create(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes,
                                const uint32_t *bw, uint32_t ncols, const uint32_t *col_order, const uint32_t *split,
                                uint32_t nbanks, uint64_t n, uint32_t *order_out, uint32_t *group_out,
                                fmcs_graph **graph);
+FMCS_API int fmcs_graph_create_hash(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_bytes,
+                                    const uint32_t *bw, uint32_t ncols, const uint32_t *col_order,
+                                    const uint32_t *split, uint32_t nbanks, uint64_t n, uint32_t *order_out,
+                                    uint32_t *group_out, fmcs_graph **graph);
 FMCS_API int fmcs_graph_launch(fmcs_graph *graph, uint32_t *ngroups);
 FMCS_API void *fmcs_graph_stream(fmcs_graph *graph);
 /* Kernel nodes of the graph, each loop body (the radix levels of a sort round,

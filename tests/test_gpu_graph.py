@@ -73,3 +73,59 @@ def test_graph_level_loop_follows_the_data(ctx):
             assert np.array_equal(group.cpu().numpy().view(np.uint32), gr)
     finally:
         g.close()
+
+
+@pytest.mark.parametrize("widths,distinct,split,col_order", [
+    ([8, 12, 7], [16, 300, 0], [27], None),
+    ([8, 12, 7], [16, 300, 0], [8, 19], [0, 2, 1]),
+    ([2, 1, 12, 12, 32, 7], [3, 2, 2526, 2526, 0, 100], [58, 8], [0, 2, 3, 4, 1, 5]),
+    ([8, 8, 8], [4, 5, 6], [8, 8, 8], None),
+])
+def test_hash_graph_replays_match_oracle(ctx, widths, distinct, split, col_order):
+    """A hash-grouping plan captured as a graph (fmcs_graph_create_hash): its
+    key widths and its clustering are decided on the device, so replays on
+    new data match the oracle's hash plan (src/composer.cpp:137-227)."""
+    torch = pytest.importorskip("torch")
+    n = 300_000
+    cols, bw = W.cols_uniform(n, widths, seed_index=40, distinct=distinct)
+    dcols = [_dev(torch, c) for c in cols]
+    order = torch.zeros(n, dtype=torch.int32, device="cuda")
+    group = torch.zeros(n, dtype=torch.int32, device="cuda")
+    g = ctx.plan_graph(dcols, bw, split, order, group, col_order=col_order, hash=True)
+    try:
+        for seed in (40, 41, 40):
+            cols, _ = W.cols_uniform(n, widths, seed_index=seed, distinct=distinct)
+            for d, c in zip(dcols, cols):
+                d.copy_(_dev(torch, c))
+            torch.cuda.synchronize()
+            ng = g.launch()
+            o, gr, ng_ref = O.run_plan_hash(cols, bw, split, col_order=col_order)
+            assert ng == ng_ref
+            assert np.array_equal(order.cpu().numpy().view(np.uint32), o)
+            assert np.array_equal(group.cpu().numpy().view(np.uint32), gr)
+            # the same plan through the eager C ABI agrees
+            oe = np.zeros(n, np.uint32)
+            ge = np.zeros(n, np.uint32)
+            assert ctx.run_plan(cols, bw, split, oe, ge, col_order=col_order, hash=True) == ng_ref
+            assert np.array_equal(oe, o) and np.array_equal(ge, gr)
+    finally:
+        g.close()
+
+
+def test_eager_round_skips_empty_tiers(ctx):
+    """An eager sort round launches only the on-chip tiers its segments use:
+    a round-0 sort of 1,000 rows is one block sort (and the group ids)."""
+    rng = np.random.default_rng(5)
+    n = 1000
+    bank = rng.integers(0, 1 << 40, size=n, dtype=np.uint64)
+    order = np.zeros(n, np.uint32)
+    ctx.profile(True)
+    ctx.sort_round(bank, 40, order)
+    prof = ctx.profile_report()
+    ctx.profile(False)
+    ran = {k for k in prof if not k.startswith("_")}
+    assert "block_sort_1024" in ran
+    assert not ran & {"thread_sort", "warp_sort", "block_sort_512", "block_sort_2048", "block_sort_4096",
+                      "block_sort_8192", "copy", "copy_tiles"}
+    o_ref, _, _, _ = O.sort_round(bank)
+    assert np.array_equal(order, o_ref)
