@@ -156,6 +156,19 @@ def calibrate(ctx, quick: bool) -> dict:
     return out
 
 
+def write_tuning(path: str, knobs: dict, tables: dict, how: str, knob_search=None) -> dict:
+    """The tuning file both readers take: the library's context knobs
+    (rank_mode, local_max, msd_items) and the cost model's tables
+    (GpuCostTables::Load: stitch_per_byte, gather, boundary, msd_level, local,
+    round_fixed_ms), in ms per million rows."""
+    doc = {"device": "B200", "how": how, "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
+           **knobs, **tables, "knob_search": knob_search or []}
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        json.dump(doc, f, indent=1)
+    return doc
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_OUT)
@@ -165,12 +178,8 @@ def main():
         wl = Workloads(args.quick)
         best, table = search_knobs(ctx, wl)
         tables = calibrate(ctx, args.quick)
-    doc = {"device": "B200", "how": "python -m fastmulticolsort_b200.autotune"
-           + (" --quick" if args.quick else ""), "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
-           **best, **tables, "knob_search": table}
-    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
-    with open(args.out, "w") as f:
-        json.dump(doc, f, indent=1)
+    write_tuning(args.out, best, tables, "python -m fastmulticolsort_b200.autotune" + (" --quick" if args.quick else ""),
+                 table)
     print(json.dumps({"best": best, "out": args.out}))
 
 

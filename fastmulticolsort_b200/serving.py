@@ -102,11 +102,15 @@ def warm(torch, srv, pool, rounds=2):
             srv.wait(tk)
 
 
-def run_served(torch, srv, pool, trace, slots):
+def run_served(torch, srv, pool, trace, slots, keep=None):
     """The trace through the server.  Outputs come from a ring of buffers
     allocated before timing (a buffer is reused only after its request was
-    waited for), so no allocation sits inside the timed loop."""
+    waited for), so no allocation sits inside the timed loop.  Returns the
+    latencies (ms, in trace order), rows, wall seconds, the number of requests
+    that ran inside a shared launch, and, for the requests whose trace index
+    is in `keep`, a copy of their (order, group) and their batch size."""
     lat, rows, batched = [], 0, 0
+    kept = {}
     depth = 4 * slots
     maxn = max(d["n"] for d in pool)
     ring = [(torch.empty(maxn, dtype=torch.int32, device="cuda"), torch.empty(maxn, dtype=torch.int32, device="cuda"))
@@ -120,20 +124,27 @@ def run_served(torch, srv, pool, trace, slots):
             time.sleep(arrival - now)
         d = pool[k]
         o, g = ring[i % len(ring)]
-        pending.append((srv.submit(d["cols"], d["widths"], o[:d["n"]], g[:d["n"]], cardinality=d["card"]), d["n"]))
+        pending.append((srv.submit(d["cols"], d["widths"], o[:d["n"]], g[:d["n"]], cardinality=d["card"]), d["n"],
+                        i, o, g))
         # reap what finished, keeping the buffers in use bounded
         while len(pending) > depth:
-            tk, n = pending.pop(0)
+            tk, n, j, oo, gg = pending.pop(0)
             r = srv.wait(tk)
             lat.append(r["total_ms"])
             rows += n
             batched += r["batched_with"] > 1
-    for tk, n in pending:
+            if keep is not None and j in keep:
+                kept[j] = (oo[:n].clone(), gg[:n].clone(), r["batched_with"])
+    for tk, n, j, oo, gg in pending:
         r = srv.wait(tk)
         lat.append(r["total_ms"])
         rows += n
         batched += r["batched_with"] > 1
+        if keep is not None and j in keep:
+            kept[j] = (oo[:n].clone(), gg[:n].clone(), r["batched_with"])
     wall = time.perf_counter() - t0
+    if keep is not None:
+        return lat, rows, wall, batched, kept
     return lat, rows, wall, batched
 
 
@@ -165,6 +176,69 @@ def run_serial_plain(torch, ctx, pool, trace):
     return lat, rows, clock
 
 
+def burst_trace(rng, bursts, per_burst, gap_s, pool_size):
+    """Bursts of `per_burst` requests arriving together every `gap_s` seconds
+    (requests that co-arrive while the slots are busy: the case continuous
+    batching is for)."""
+    trace = []
+    for b in range(bursts):
+        for _ in range(per_burst):
+            trace.append((b * gap_s, int(rng.integers(0, pool_size))))
+    return trace
+
+
+def burst_benchmark(torch, slots=4, budget=150 << 30, batch_rows_max=1 << 20, seed=0xF17C0006, bursts=40,
+                    per_burst=48, gap_s=0.025, pool_size=48):
+    """Small requests (65,536 to 1,048,576 rows, log-uniform) of ONE layout
+    (8/24/40-bit uniform columns, the many-instances shape) in bursts, served
+    with continuous batching (batch_rows_max) and without it (0); a sample of
+    the requests' results from the batched run is compared with the same
+    requests' results from the unbatched run."""
+    rng = np.random.default_rng(seed)
+    widths = [8, 24, 40]
+    pool = []
+    for _ in range(pool_size):
+        n = int(math.exp(rng.uniform(math.log(MIN_ROWS), math.log(1 << 20))))
+        cols = [_store(torch, _uniform_codes(torch, rng, n, w), w) for w in widths]
+        pool.append(dict(n=n, widths=widths, cols=cols, card=[min(n, 1 << w) for w in widths], zipf=False))
+    trace = burst_trace(rng, bursts, per_burst, gap_s, pool_size)
+    keep = set(range(0, len(trace), max(1, len(trace) // 16)))
+    out = {"requests": len(trace), "bursts": bursts, "per_burst": per_burst, "gap_ms": gap_s * 1e3,
+           "rows": "log-uniform [65536, 1048576]", "columns": widths}
+    results = {}
+    for name, brm in (("batched", batch_rows_max), ("unbatched", 0)):
+        with capi.Server(0, hbm_budget_bytes=budget, slots=slots, batch_rows_max=brm) as srv:
+            warm(torch, srv, pool)
+            torch.cuda.synchronize()
+            lat, rows, wall, nb, kept = run_served(torch, srv, pool, trace, slots, keep=keep)
+        results[name] = kept
+        out[name] = {"p50_ms": round(float(np.percentile(lat, 50)), 3),
+                     "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                     "rows_per_s_M": round(rows / wall / 1e6, 1), "batched_requests": nb,
+                     "batch_rows_max": brm}
+    same = all(torch.equal(results["batched"][j][0], results["unbatched"][j][0])
+               and torch.equal(results["batched"][j][1], results["unbatched"][j][1]) for j in keep)
+    out["check"] = {"sampled": len(keep),
+                    "sampled_in_shared_launch": int(sum(results["batched"][j][2] > 1 for j in keep)),
+                    "batched_equals_unbatched": bool(same)}
+    out["checked"] = bool(same)
+    return out
+
+
+def tail_of(lat, trace, pool, q=99):
+    """The requests at or above the q-th latency percentile: how many, and
+    their mean rows and key bits, beside the trace's mean rows (what the
+    tail is made of)."""
+    lat = np.asarray(lat)
+    cut = np.percentile(lat, q)
+    ds = [pool[trace[i][1]] for i, v in enumerate(lat) if v >= cut and i < len(trace)]
+    if not ds:
+        return {}
+    return {"count": len(ds), "mean_rows": round(float(np.mean([d["n"] for d in ds])), 1),
+            "mean_key_bits": round(float(np.mean([sum(d["widths"]) for d in ds])), 1),
+            "trace_mean_rows": round(float(np.mean([pool[k]["n"] for _, k in trace])), 1)}
+
+
 def benchmark(rate=200.0, duration=5.0, pool_size=32, slots=4, budget=150 << 30, batch_rows_max=1 << 20,
               seed=0xF17C0005):
     import torch
@@ -177,6 +251,7 @@ def benchmark(rate=200.0, duration=5.0, pool_size=32, slots=4, budget=150 << 30,
         lat, rows, wall, batched = run_served(torch, srv, pool, trace, slots)
     with capi.Context(0) as ctx:
         plat, prows, pwall = run_serial_plain(torch, ctx, pool, trace)
+    burst = burst_benchmark(torch, slots=slots, budget=budget, batch_rows_max=batch_rows_max)
     return {
         "requests": len(trace), "rate_req_s": rate, "duration_s": duration, "slots": slots,
         "hbm_budget_gb": budget / 2**30, "batch_rows_max": batch_rows_max,
@@ -186,4 +261,6 @@ def benchmark(rate=200.0, duration=5.0, pool_size=32, slots=4, budget=150 << 30,
         "serial_plain": {"p50_ms": round(float(np.percentile(plat, 50)), 3),
                          "p99_ms": round(float(np.percentile(plat, 99)), 3),
                          "rows_per_s_M": round(prows / pwall / 1e6, 1)},
+        "p99_tail": tail_of(lat, trace, pool),
+        "burst": burst,
     }

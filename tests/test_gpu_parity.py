@@ -328,3 +328,27 @@ def test_run_plan_descending_columns(ctx, desc, split):
     v0 = cols[0][order].astype(np.int64)
     d0 = np.diff(v0)
     assert (d0 <= 0).all() if desc[0] else (d0 >= 0).all()
+
+
+@pytest.mark.parametrize("hash_path", [False, True])
+def test_group_by_column_order_matches_oracle(ctx, hash_path):
+    """GROUP BY may reorder the columns (the optimizer's ordered=0 search,
+    src/stitch_composer.cpp:15-35, 3877-3882): the column order it picks for
+    the wide shape is not the identity, and the plan run with that order
+    (sort or hash rounds) matches the oracle given the same order."""
+    from fastmulticolsort_b200 import capi
+    n = 400_000
+    widths, distinct = [2, 1, 12, 12, 32, 7], [3, 2, 2526, 2526, 0, 100]
+    cols, bw = W.cols_uniform(n, widths, seed_index=17, distinct=distinct)
+    # the search on the 60,000,000-row table's statistics (at this row count
+    # the identity order is already the cheapest)
+    card = [k if k else 60_000_000 for k in distinct]
+    split, corder, _ = capi.optimize_plan(bw, card, [c.dtype.itemsize for c in cols], 60_000_000, ordered=False)
+    assert corder != sorted(corder)
+    order = np.zeros(n, np.uint32)
+    group = np.zeros(n, np.uint32)
+    ng = ctx.run_plan(cols, bw, split, order, group, col_order=corder, hash=hash_path)
+    run = O.run_plan_hash if hash_path else O.run_plan_sort
+    o, g, ng_ref = run(cols, bw, split, col_order=corder)
+    assert ng == ng_ref
+    assert np.array_equal(order, o) and np.array_equal(group, g)
