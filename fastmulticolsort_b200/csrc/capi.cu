@@ -181,8 +181,7 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
             top_hist = (uint32_t *)p;
             uint32_t *tdst;
             uint4 *tinfo;
-            unsigned long long *clb;
-            if ((rc = level_tile_arrays(ctx, n, sort_tile_rows(ctx), &tile_cnt, &tdst, &tinfo, &clb))) return rc;
+            if ((rc = level_tile_arrays(ctx, n, sort_tile_rows(ctx), &tile_cnt, &tdst, &tinfo))) return rc;
         }
         if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits, tile_cnt,
                                 sort_tile_rows(ctx))))

@@ -238,10 +238,8 @@ int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
 uint32_t sort_tile_rows(const fmcs_ctx *ctx);
 uint64_t sort_level_tiles(const fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows);
 // The per-tile arrays of the radix levels (workspace slots kSlotTileCnt,
-// kSlotTileDst, kSlotLookback), sized for a sort of n rows in tiles of
-// tile_rows rows.
-int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo,
-                      unsigned long long **clb);
+// kSlotTileDst), sized for a sort of n rows in tiles of tile_rows rows.
+int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo);
 // Stable full-array LSD radix sort of (keys, vals) in place by key bits
 // [0, bits): the plain, unsegmented comparator path.
 int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits);

@@ -9,19 +9,20 @@
 //
 // B200 design.  Every group is a segment [start, start+len) that is sorted in
 // place (segments never move).  Segments are binned by size:
-//   tier A  len <= 128   one warp per segment, LSD radix in registers/smem
-//   tier B  len <= 1024  one 128-thread CTA per segment, LSD radix in smem
-//   tier C  len <= 4096  one 256-thread CTA per segment, LSD radix in smem
-//   large   len >  4096  MSD radix levels: per-segment digit histogram, then a
-//                        onesweep-style stable scatter with a decoupled
-//                        look-back chained over the segment's tiles; every
-//                        non-empty bucket becomes a child segment with 8 bits
-//                        fewer, re-binned into the tiers above.
-// Each key is ranked by warp-level multi-split (match.any + popc) so every
-// pass is stable; the MSD scatter is stable too, so the whole sort is stable:
+//   thread   len <= 16 (32)   one thread, an odd-even transposition network
+//   warp     len <= 128       one warp, LSD radix in registers/smem
+//   block    len <= 8192      one CTA, in six tiers of 512 to 8192 rows:
+//                             compound-key buckets in shared memory
+//   large    len > local_max  HBM radix levels: per-tile digit counts, a
+//                             column scan of them into per-tile destinations,
+//                             and a stable scatter of TMA-fed tiles; every
+//                             non-empty bucket becomes a child segment with 8
+//                             bits fewer, re-binned into the tiers above.
+// Each key is ranked by warp-level multi-split (match.any / ballots / shared
+// OR words + popc) so every pass is stable, and the whole sort is stable:
 // ties keep the oid order of the input, which is what the reference gives once
-// its ties are canonicalised to ascending oid.  Rows move only through HBM in
-// the large tier; a tier-A/B/C segment is read once and written once.
+// its ties are canonicalised to ascending oid.  A row moves through HBM only in
+// the large tier; a thread/warp/block segment is read once and written once.
 //
 // Data sources of a segment: BUF0 (final buffer: the caller's order array and
 // the sorted-key array), BUF1 (work buffer), EXT (the round's input: the bank
@@ -49,8 +50,9 @@ constexpr int kCapT32 = 32;  // the same up to 32 rows, for 2- and 4-byte keys (
 constexpr int kCapA = 128;   // warp per segment: 32 lanes x 4 items
 constexpr int kItemsA = 4;
 constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
-constexpr int kNtB2 = 128, kItB2 = 8, kCapB2 = kNtB2 * kItB2;   // 1024
-constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
+constexpr int kNtB2 = 256, kItB2 = 4, kCapB2 = kNtB2 * kItB2;   // 1024
+constexpr int kNtC1 = 512, kItC1 = 4, kCapC1 = kNtC1 * kItC1;   // 2048
+constexpr int kNtC1b = 512, kItC1b = 5, kCapC1b = kNtC1b * kItC1b;   // 2560
 constexpr int kNtC2 = 512, kItC2 = 8, kCapC2 = kNtC2 * kItC2;   // 4096
 constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
 constexpr int kCapLocal = kCapC3;   // largest segment a local tier can take; larger: MSD levels
@@ -74,9 +76,8 @@ constexpr int kCtrCopyTile = 13;
 constexpr uint32_t kCopySplit = 4096;
 constexpr int kCtrLevel = 15;      // MSD levels started so far (device-side level index)
 constexpr int kCtrLocalC3 = 16;
-constexpr int kCtrChunk = 17;      // chunks of the tile scan claimed so far (current level)
+constexpr int kCtrLocalC1b = 18;
 constexpr int kCtrWords = 32;
-constexpr int kScanChunk = 16;     // tiles per chunk of the tile scan
 
 struct LargeSeg {
     uint32_t start, len, shift, src;
@@ -94,8 +95,7 @@ struct LargeSeg {
 // 4,096 rows); tdst[t][d] the global position of the tile's first row of
 // digit d (segment start + the digit's offset in the segment + the rows of
 // digit d in the segment's earlier tiles); tinfo[t] = (first row, rows,
-// lo | width << 8 | src << 16, 0); clb the chunk look-back words of the tile
-// scan.
+// lo | width << 8 | src << 16, 0).
 struct LevelRefs {
     LargeSeg *large[2];
     uint32_t *hist[2];
@@ -105,7 +105,6 @@ struct LevelRefs {
     uint16_t *tcnt;
     uint32_t *tdst;
     uint4 *tinfo;
-    unsigned long long *clb;
 };
 
 // Index of the level whose launches are running (level_prefix_kernel has
@@ -197,7 +196,7 @@ __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32
 }
 
 struct Lists {
-    uint2 *t, *t32, *a, *b1, *b2, *c1, *c2, *c3;
+    uint2 *t, *t32, *a, *b1, *b2, *c1, *c1b, *c2, *c3;
     uint32_t cap_t32;      // kCapT32 for keys of <= 4 bytes, else 0 (17..32 rows go to the warp tier)
     LargeSeg *copy;        // segments that only need to reach BUF0, <= kCopySplit rows (warp each)
     LargeSeg *copy_large;  // the same, larger: copied by tiles across the grid
@@ -246,6 +245,8 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
         which = kCtrLocalB2;
     } else if (len <= (uint32_t)kCapC1) {
         which = kCtrLocalC1;
+    } else if (len <= (uint32_t)kCapC1b) {
+        which = kCtrLocalC1b;
     } else if (len <= (uint32_t)kCapC2) {
         which = kCtrLocalC2;
     } else if (len <= (uint32_t)kCapC3) {
@@ -264,6 +265,7 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
     case kCtrLocalB1: L.b1[slot] = e; break;
     case kCtrLocalB2: L.b2[slot] = e; break;
     case kCtrLocalC1: L.c1[slot] = e; break;
+    case kCtrLocalC1b: L.c1b[slot] = e; break;
     case kCtrLocalC2: L.c2[slot] = e; break;
     case kCtrLocalC3: L.c3[slot] = e; break;
     default: {
@@ -381,7 +383,6 @@ __global__ void __launch_bounds__(1024) level_prefix_kernel(LevelRefs r, uint32_
         r.ctr[kCtrLarge0 + nxt] = 0;
         r.ctr[kCtrMsdTile] = 0;
         r.ctr[kCtrMoved] = 0;
-        r.ctr[kCtrChunk] = 0;
         if (r.dev_level) r.ctr[kCtrLevel] = lvl + 1;
     }
     tile_prefix_body((cur ? r.large[1] : r.large[0]), nseg, tile_prefix, tile_rows);
@@ -527,94 +528,141 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lis
 // Tile scan: for every tile of the level, the global position of its first
 // row of each digit (tdst: segment start + the digit's offset in the segment
 // + the rows of that digit in the segment's earlier tiles) and its descriptor
-// (tinfo).  Thread d owns digit d.  Chunks of kScanChunk consecutive tiles are
-// claimed in order through a counter; a chunk whose first segment began in an
-// earlier chunk takes that segment's running counts by a decoupled look-back
-// over the chunks before it (bounded waits, words tagged with the level's
-// epoch).  Runs after msd_plan, whose offsets and skip marks it reads.
+// (tinfo).  A column scan with no waits: CTA c takes digits [4c, 4c + 4), its
+// thread i a contiguous run of tiles; each thread sums its run's counts from
+// the run's last segment start, one block-wide segmented scan (the sums reset
+// where a segment starts) gives every run the counts of its segment's earlier
+// tiles, and a second walk over the run writes the destinations.  Runs after
+// msd_plan, whose offsets and skip marks it reads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kRadix) tile_scan_kernel(LevelRefs r, const uint32_t *tile_prefix, uint32_t tile_rows,
-                                                          uint32_t epoch_base, int *status)
+constexpr int kScanDigits = 4;     // digits per CTA of the tile scan (one 8-byte count load per tile)
+constexpr int kScanThreads = 256;
+
+struct SegSum {
+    uint32_t head;                 // a segment starts inside the run
+    uint32_t s[kScanDigits];       // counts since the run's last segment start (or its first tile)
+};
+
+// left (earlier tiles) then right: a start in the right part resets the sums
+__device__ __forceinline__ SegSum seg_combine(const SegSum &l, const SegSum &r)
+{
+    SegSum o;
+    o.head = l.head | r.head;
+#pragma unroll
+    for (int j = 0; j < kScanDigits; ++j) o.s[j] = r.head ? r.s[j] : l.s[j] + r.s[j];
+    return o;
+}
+
+__device__ __forceinline__ SegSum seg_shfl_up(const SegSum &v, int o)
+{
+    SegSum w;
+    w.head = __shfl_up_sync(0xFFFFFFFFu, v.head, o);
+#pragma unroll
+    for (int j = 0; j < kScanDigits; ++j) w.s[j] = __shfl_up_sync(0xFFFFFFFFu, v.s[j], o);
+    return w;
+}
+
+// the large segment holding tile t: tile_prefix[s] <= t < tile_prefix[s + 1]
+__device__ __forceinline__ uint32_t segment_of_tile(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
+{
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (tile_prefix[m] <= t) lo = m;
+        else hi = m;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(LevelRefs r, const uint32_t *tile_prefix,
+                                                                uint32_t tile_rows)
 {
     kernel_prologue();
-    __shared__ uint32_t s_chunk;
+    constexpr int NW = kScanThreads / 32;
+    __shared__ SegSum wsum[NW];
     const uint32_t lvl = running_level(r);
     const uint32_t cur = lvl & 1u;
     const LargeSeg *segs = cur ? r.large[1] : r.large[0];
     const uint32_t *offs = cur ? r.hist[1] : r.hist[0];
     const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
     if (nseg == 0) return;
-    const uint32_t epoch = epoch_base + lvl;
     const uint32_t T = tile_prefix[nseg];
-    const uint32_t chunks = (T + kScanChunk - 1) / kScanChunk;
-    const uint32_t d = threadIdx.x;
-    for (;;) {
-        __syncthreads();   // every thread has read the previous chunk index
-        if (d == 0) s_chunk = atomicAdd(&r.ctr[kCtrChunk], 1u);
-        __syncthreads();
-        const uint32_t c = s_chunk;
-        if (c >= chunks) break;
-        const uint32_t t0 = c * kScanChunk;
-        const uint32_t t1 = min(T, t0 + kScanChunk);
-        const uint32_t s0 = find_segment_warp(tile_prefix, nseg, t0);
-        const bool before = tile_prefix[s0] < t0;   // s0 began in an earlier chunk
-        uint32_t pre[kScanChunk];
-        uint32_t s = s0, snext = tile_prefix[s0 + 1], run = 0;
+    const uint32_t d0 = blockIdx.x * kScanDigits;
+    const uint32_t per = (T + kScanThreads - 1) / kScanThreads;
+    const uint32_t a = threadIdx.x * per;
+    const uint32_t b = min(T, a + per);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // pass 1: the run's sums since its last segment start
+    SegSum mine{};
+    uint32_t s0 = 0;
+    if (a < b) {
+        s0 = segment_of_tile(tile_prefix, nseg, a);
+        uint32_t s = s0, snext = tile_prefix[s0 + 1];
+        mine.head = tile_prefix[s0] == a;
+        for (uint32_t t = a; t < b; ++t) {
+            if (t >= snext) {   // a segment starts at t (every large segment has a tile)
+                ++s;
+                snext = tile_prefix[s + 1];
+                mine.head = 1;
 #pragma unroll
-        for (int i = 0; i < kScanChunk; ++i) {
-            const uint32_t t = t0 + i;
-            pre[i] = 0;
-            if (t < t1) {
-                if (t >= snext) {   // a segment starts at t (every large segment has a tile)
-                    ++s;
-                    snext = tile_prefix[s + 1];
-                    run = 0;
-                }
-                pre[i] = run;
-                run += r.tcnt[(uint64_t)t * kRadix + d];
+                for (int j = 0; j < kScanDigits; ++j) mine.s[j] = 0;
+            }
+            const ushort4 c = *reinterpret_cast<const ushort4 *>(r.tcnt + (uint64_t)t * kRadix + d0);
+            mine.s[0] += c.x;
+            mine.s[1] += c.y;
+            mine.s[2] += c.z;
+            mine.s[3] += c.w;
+        }
+    }
+    // block-wide exclusive segmented scan of the runs' sums
+    SegSum incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const SegSum up = seg_shfl_up(incl, o);
+        if (lane >= o) incl = seg_combine(up, incl);
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    SegSum before{};   // everything before this warp
+    for (int w = 0; w < warp; ++w) before = seg_combine(before, wsum[w]);
+    SegSum lane_excl = seg_shfl_up(incl, 1);
+    if (lane == 0) lane_excl = SegSum{};
+    const SegSum excl = seg_combine(before, lane_excl);
+    if (a >= b) return;
+    // pass 2: destinations and descriptors
+    uint32_t s = s0, snext = tile_prefix[s0 + 1], sfirst = tile_prefix[s0];
+    LargeSeg sg = segs[s0];
+    uint32_t run[kScanDigits], base[kScanDigits];
+    const bool carried = sfirst < a;   // the run's first segment began in an earlier run
+#pragma unroll
+    for (int j = 0; j < kScanDigits; ++j) {
+        run[j] = carried ? excl.s[j] : 0u;
+        base[j] = sg.start + offs[(uint64_t)s0 * kRadix + d0 + j];
+    }
+    for (uint32_t t = a; t < b; ++t) {
+        if (t >= snext) {
+            ++s;
+            sfirst = snext;
+            snext = tile_prefix[s + 1];
+            sg = segs[s];
+#pragma unroll
+            for (int j = 0; j < kScanDigits; ++j) {
+                run[j] = 0;
+                base[j] = sg.start + offs[(uint64_t)s * kRadix + d0 + j];
             }
         }
-        // the chunk's word describes its last segment: inclusive when that
-        // segment began inside the chunk, else an aggregate until the carry
-        // is known
-        const bool last_inside = (s != s0) || !before;
-        unsigned long long *mine = &r.clb[(uint64_t)c * kRadix + d];
-        st_volatile_u64(mine, lb_word(epoch, last_inside ? kFlagInclusive : kFlagAggregate, run));
-        uint32_t carry = 0;
-        if (before) {
-            uint32_t p = c;
-            while (p > 0) {
-                --p;
-                const unsigned long long w = lb_wait(&r.clb[(uint64_t)p * kRadix + d], epoch, status);
-                carry += (uint32_t)w;
-                if (((uint32_t)(w >> 32) & 3u) == kFlagInclusive) break;
-            }
-            if (!last_inside) st_volatile_u64(mine, lb_word(epoch, kFlagInclusive, carry + run));
-        }
-        s = s0;
-        snext = tile_prefix[s0 + 1];
-        uint32_t sfirst = tile_prefix[s0];
-        LargeSeg sg = segs[s0];
-        uint32_t base = sg.start + offs[(uint64_t)s0 * kRadix + d] + carry;   // carry: 0 unless s0 began earlier
-#pragma unroll
-        for (int i = 0; i < kScanChunk; ++i) {
-            const uint32_t t = t0 + i;
-            if (t < t1) {
-                if (t >= snext) {
-                    ++s;
-                    sfirst = snext;
-                    snext = tile_prefix[s + 1];
-                    sg = segs[s];
-                    base = sg.start + offs[(uint64_t)s * kRadix + d];
-                }
-                r.tdst[(uint64_t)t * kRadix + d] = base + pre[i];
-                if (d == 0) {
-                    const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
-                    const uint32_t rb = sg.start + (t - sfirst) * tile_rows;
-                    const uint32_t cnt = min(tile_rows, sg.start + sg.len - rb);
-                    r.tinfo[t] = make_uint4(rb, cnt, (sg.shift - width) | (width << 8) | (sg.src << 16), 0u);
-                }
-            }
+        const ushort4 c = *reinterpret_cast<const ushort4 *>(r.tcnt + (uint64_t)t * kRadix + d0);
+        *reinterpret_cast<uint4 *>(r.tdst + (uint64_t)t * kRadix + d0) =
+            make_uint4(base[0] + run[0], base[1] + run[1], base[2] + run[2], base[3] + run[3]);
+        run[0] += c.x;
+        run[1] += c.y;
+        run[2] += c.z;
+        run[3] += c.w;
+        if (blockIdx.x == 0) {
+            const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
+            const uint32_t rb = sg.start + (t - sfirst) * tile_rows;
+            const uint32_t cnt = min(tile_rows, sg.start + sg.len - rb);
+            r.tinfo[t] = make_uint4(rb, cnt, (sg.shift - width) | (width << 8) | (sg.src << 16), 0u);
         }
     }
 }
@@ -963,11 +1011,18 @@ __global__ void __launch_bounds__(kNtM, scatter_ctas_per_sm(IT)) msd_scatter_ker
 constexpr uint32_t kCountRankMax = 64;
 constexpr uint32_t kBucketMax = 64;
 
+constexpr int pow2_ceil(int x)
+{
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
 template <typename K, int NT, int IT>
 struct BucketSmem {
     unsigned long long cs[NT * IT];   // compound keys, bucketed
     uint32_t vals[NT * IT];
-    uint32_t off[NT * IT + 1];        // per bucket: count -> start
+    uint32_t off[pow2_ceil(NT * IT) + 1];   // per bucket: count -> start (up to 2^ceil(log2 len) buckets)
     uint16_t orig[NT * IT];           // position in the segment, when the compound key has no room for it
     uint32_t tmp[NT / 32 + 1];
     unsigned long long any, all;      // OR and AND of the segment's keys
@@ -1673,14 +1728,11 @@ uint64_t sort_level_tiles(const fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows)
 }
 
 // The per-tile arrays of the HBM radix levels, in their workspace slots: the
-// counts (which the stitch may fill for level 0 before the sort starts), the
-// destinations and descriptors, and the chunk look-back words of the tile scan
-// (zeroed when first allocated).
-int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo,
-                      unsigned long long **clb)
+// counts (which the stitch may fill for level 0 before the sort starts), and
+// the destinations and descriptors.
+int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo)
 {
     const uint64_t tiles = sort_level_tiles(ctx, n, tile_rows);
-    const uint64_t chunks = tiles / kScanChunk + 1;
     void *p;
     int rc;
     if ((rc = ws_get(ctx, kSlotTileCnt, tiles * kRadix * sizeof(uint16_t), &p))) return rc;
@@ -1690,8 +1742,6 @@ int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **
     Carver cv(p);
     *tdst = cv.take<uint32_t>(tiles * kRadix);
     *tinfo = cv.take<uint4>(tiles);
-    if ((rc = ws_get(ctx, kSlotLookback, chunks * kRadix * sizeof(unsigned long long), &p, true))) return rc;
-    *clb = (unsigned long long *)p;
     return FMCS_OK;
 }
 
@@ -1727,7 +1777,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const uint64_t cap_t = n / 2 + 2, cap_t32 = n / (kCapT + 1) + 2, cap_a = n / (kCapT + 1) + 2;
     const uint64_t cap_b1 = n / (kCapA + 1) + 2;
     const uint64_t cap_b2 = n / (kCapB1 + 1) + 2;
-    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2, cap_c3 = n / (kCapC2 + 1) + 2;
+    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c1b = n / (kCapC1 + 1) + 2, cap_c2 = n / (kCapC1b + 1) + 2;
+    const uint64_t cap_c3 = n / (kCapC2 + 1) + 2;
     // copy entries: disjoint ranges; at most 256 children per large segment per
     // level, so bounded by both n and (levels + 1) * 256 * cap_large
     const uint64_t levels_max = (a.key_bits + kRadixBits - 1) / kRadixBits;
@@ -1742,7 +1793,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         const size_t e = sizeof(uint2);
         if ((rc = ws_get(ctx, kSlotLocalA,
                          carve_total({cap_t * e, cap_t32 * e, cap_a * e, cap_b1 * e, cap_b2 * e, cap_c1 * e,
-                                      cap_c2 * e, cap_c3 * e}),
+                                      cap_c1b * e, cap_c2 * e, cap_c3 * e}),
                          &p)))
             return rc;
         Carver cv(p);
@@ -1753,6 +1804,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         lists.b1 = cv.take<uint2>(cap_b1);
         lists.b2 = cv.take<uint2>(cap_b2);
         lists.c1 = cv.take<uint2>(cap_c1);
+        lists.c1b = cv.take<uint2>(cap_c1b);
         lists.c2 = cv.take<uint2>(cap_c2);
         lists.c3 = cv.take<uint2>(cap_c3);
         if ((rc = ws_get(ctx, kSlotLocalC, carve_total({cap_copy * sizeof(LargeSeg), cap_large * sizeof(LargeSeg)}),
@@ -1775,8 +1827,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     uint16_t *tcnt;
     uint32_t *tdst;
     uint4 *tinfo;
-    unsigned long long *clb;
-    if ((rc = level_tile_arrays(ctx, n, tile_rows, &tcnt, &tdst, &tinfo, &clb))) return rc;
+    if ((rc = level_tile_arrays(ctx, n, tile_rows, &tcnt, &tdst, &tinfo))) return rc;
     uint32_t *ctr;
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     ctr = (uint32_t *)p + 64;   // words 0..63 belong to other kernels
@@ -1812,6 +1863,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                               : len <= (uint32_t)kCapB1 ? kCtrLocalB1
                               : len <= (uint32_t)kCapB2 ? kCtrLocalB2
                               : len <= (uint32_t)kCapC1 ? kCtrLocalC1
+                              : len <= (uint32_t)kCapC1b ? kCtrLocalC1b
                               : len <= (uint32_t)kCapC2 ? kCtrLocalC2 : kCtrLocalC3;
             w[which] = 1;
         }
@@ -1835,9 +1887,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             tiers_known = true;
         }
         const int hist0_ready = (a.top_hist && !a.seg_start) ? 1 : 0;
-        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready, tcnt, tdst, tinfo, clb};
-        const uint32_t epoch_base = ctx->epoch;
-        ctx->epoch += (uint32_t)levels;
+        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready, tcnt, tdst, tinfo};
         const unsigned scatter_grid = sms * scatter_ctas_per_sm(IT);
         int host_lvl = 0;   // the level being launched, for the eager read-back
         // one level: the same five launches for every level (the level index
@@ -1855,8 +1905,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                 launch_k(msd_plan_kernel, sms * 8, kRadix, 0, s, lr, lists, true);
             }
             { LaunchScope ls_(ctx, "tile_scan");
-                launch_k(tile_scan_kernel, sms * 2, kRadix, 0, s, lr, tile_prefix, tile_rows, epoch_base,
-                         ctx->d_status);
+                launch_k(tile_scan_kernel, kRadix / kScanDigits, kScanThreads, 0, s, lr, tile_prefix, tile_rows);
             }
             if (read_back) {
                 // read the counters (the next level's count, the rows moved,
@@ -1907,11 +1956,13 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const size_t smem_b1 = std::max(sizeof(BlockSmem<K, kNtB1, kItB1>), sizeof(BucketSmem<K, kNtB1, kItB1>));
     const size_t smem_b2 = std::max(sizeof(BlockSmem<K, kNtB2, kItB2>), sizeof(BucketSmem<K, kNtB2, kItB2>));
     const size_t smem_c1 = std::max(sizeof(BlockSmem<K, kNtC1, kItC1>), sizeof(BucketSmem<K, kNtC1, kItC1>));
+    const size_t smem_c1b = std::max(sizeof(BlockSmem<K, kNtC1b, kItC1b>), sizeof(BucketSmem<K, kNtC1b, kItC1b>));
     const size_t smem_c2 = std::max(sizeof(BlockSmem<K, kNtC2, kItC2>), sizeof(BucketSmem<K, kNtC2, kItC2>));
     const size_t smem_c3 = std::max(sizeof(BlockSmem<K, kNtC3, kItC3>), sizeof(BucketSmem<K, kNtC3, kItC3>));
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB1, kItB1, RANK>, smem_b1))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB2, kItB2, RANK>, smem_b2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1, kItC1, RANK>, smem_c1))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1b, kItC1b, RANK>, smem_c1b))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC3, kItC3, RANK>, smem_c3))) return rc;
     // Each tier's launch, with the counter word of its list.  A tier whose
@@ -1951,6 +2002,11 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         LaunchScope ls_(ctx, "block_sort_2048");
         launch_k(block_sort_kernel<K, kNtC1, kItC1, RANK>, sms * (1024 / kNtC1), kNtC1, smem_c1, s, b, lists.c1,
                  &ctr[kCtrLocalC1]);
+    }});
+    tiers.push_back({kCtrLocalC1b, [&](cudaStream_t s) {
+        LaunchScope ls_(ctx, "block_sort_2560");
+        launch_k(block_sort_kernel<K, kNtC1b, kItC1b, RANK>, sms * (1024 / kNtC1b), kNtC1b, smem_c1b, s, b, lists.c1b,
+                 &ctr[kCtrLocalC1b]);
     }});
     tiers.push_back({kCtrLocalC2, [&](cudaStream_t s) {
         LaunchScope ls_(ctx, "block_sort_4096");
@@ -2069,8 +2125,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
     uint16_t *tcnt;
     uint32_t *tdst;
     uint4 *tinfo;
-    unsigned long long *clb;
-    if ((rc = level_tile_arrays(ctx, n, tile_rows, &tcnt, &tdst, &tinfo, &clb))) return rc;
+    if ((rc = level_tile_arrays(ctx, n, tile_rows, &tcnt, &tdst, &tinfo))) return rc;
     uint32_t *ctr;
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     ctr = (uint32_t *)p + 64;
@@ -2079,7 +2134,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
     const int sms = ctx->num_sms;
     Lists none{};
     // one segment [0, n), re-set before every pass; level buffers of set 0
-    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0, 0, tcnt, tdst, tinfo, clb};
+    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0, 0, tcnt, tdst, tinfo};
     int pass = 0;
     for (uint32_t lo = 0; lo < bits; lo += kRadixBits, ++pass) {
         const uint32_t shift = std::min(bits, lo + kRadixBits);
@@ -2096,8 +2151,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
             launch_k(msd_plan_kernel, 1, kRadix, 0, st, lr, none, false);
         }
         { LaunchScope ls_(ctx, "tile_scan");
-            launch_k(tile_scan_kernel, sms * 2, kRadix, 0, st, lr, tile_prefix, tile_rows, ctx->epoch++,
-                     ctx->d_status);
+            launch_k(tile_scan_kernel, kRadix / kScanDigits, kScanThreads, 0, st, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_scatter");
             launch_k(msd_scatter_kernel<K, RANK, IT>, sms * scatter_ctas_per_sm(IT), kNtM, msd_smem, st, b, lr,

@@ -116,30 +116,34 @@ __device__ __forceinline__ void fold_groups(const StitchParams &p, uint64_t row0
 }
 
 // The stitch of a round-0 sort bank, by tiles of the first radix level
-// (tile_rows = 256 threads x 8 or 16 rows): besides the bank it writes every
-// tile's top-digit counts (tile_cnt, 256 u16 per tile) and adds the CTA's
-// totals to top_hist once at its end.
+// (tile_rows = 2048 or 4096): besides the bank it writes every tile's
+// top-digit counts (tile_cnt, 256 u16 per tile) and adds the CTA's totals to
+// top_hist once at its end.  512 threads take a tile's groups of 4 rows, one
+// or two each (the loads of both in flight together); CTAs of 512 threads
+// hold a tile at a time, so the tiles spread over the resident CTAs in many
+// rounds and the last, partial round is short.
+constexpr int kStitchTileThreads = 512;
+
 template <typename B>
-__global__ void __launch_bounds__(256) stitch_tiles_kernel(const __grid_constant__ StitchParams p, B *bank,
-                                                           uint64_t n, bool aligned, uint32_t *top_hist,
-                                                           uint16_t *tile_cnt, uint32_t tile_rows,
-                                                           uint32_t hist_lo, uint32_t hist_mask)
+__global__ void __launch_bounds__(kStitchTileThreads) stitch_tiles_kernel(const __grid_constant__ StitchParams p,
+                                                                         B *bank, uint64_t n, bool aligned,
+                                                                         uint32_t *top_hist, uint16_t *tile_cnt,
+                                                                         uint32_t tile_rows, uint32_t hist_lo,
+                                                                         uint32_t hist_mask)
 {
     kernel_prologue();
     __shared__ uint32_t sh[256];
     const uint32_t d = threadIdx.x;
-    sh[d] = 0;
+    if (d < 256) sh[d] = 0;
     uint32_t total = 0;
     __syncthreads();
     const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
-    const uint32_t pairs = tile_rows / (2 * 4 * 256);   // two groups of 4 rows per thread per step
+    const bool two_groups = tile_rows == 8 * kStitchTileThreads;   // 4096-row tiles
     for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint64_t tbeg = t * tile_rows;
-        for (uint32_t q = 0; q < pairs; ++q) {
-            const uint64_t row0 = tbeg + ((uint64_t)(2 * q) * 256 + d) * 4;
-            const uint64_t row1 = row0 + 256 * 4;
-            if (row0 >= n) break;
-            const bool two = row1 < n;
+        const uint64_t row0 = t * tile_rows + (uint64_t)d * 4;
+        const uint64_t row1 = row0 + (uint64_t)kStitchTileThreads * 4;
+        if (row0 < n) {
+            const bool two = two_groups && row1 < n;
             const bool vec0 = aligned && row0 + 4 <= n;
             const bool vec1 = aligned && row1 + 4 <= n;
             uint64_t acc0[4], acc1[4];
@@ -153,13 +157,15 @@ __global__ void __launch_bounds__(256) stitch_tiles_kernel(const __grid_constant
             }
         }
         __syncthreads();
-        const uint32_t c = sh[d];
-        sh[d] = 0;
-        tile_cnt[t * 256 + d] = (uint16_t)c;
-        total += c;
+        if (d < 256) {
+            const uint32_t c = sh[d];
+            sh[d] = 0;
+            tile_cnt[t * 256 + d] = (uint16_t)c;
+            total += c;
+        }
         __syncthreads();
     }
-    if (total) atomicAdd(&top_hist[d], total);
+    if (d < 256 && total) atomicAdd(&top_hist[d], total);
 }
 
 template <typename B>
@@ -292,18 +298,18 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
     if (top_hist && tile_cnt) {
         if (tile_rows != 2048 && tile_rows != 4096) return set_error(ctx, FMCS_E_INVAL, "stitch: tile rows");
         const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
-        const unsigned tgrid = (unsigned)std::min<uint64_t>(tiles, cap);
+        const unsigned tgrid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctx->num_sms * (2048 / kStitchTileThreads));
         switch (bank_bytes) {
         case 2:
-            launch_k(stitch_tiles_kernel<uint16_t>, tgrid, 256, 0, st, p, (uint16_t *)bank, n, aligned, top_hist,
+            launch_k(stitch_tiles_kernel<uint16_t>, tgrid, kStitchTileThreads, 0, st, p, (uint16_t *)bank, n, aligned, top_hist,
                      tile_cnt, tile_rows, hist_lo, hist_mask);
             break;
         case 4:
-            launch_k(stitch_tiles_kernel<uint32_t>, tgrid, 256, 0, st, p, (uint32_t *)bank, n, aligned, top_hist,
+            launch_k(stitch_tiles_kernel<uint32_t>, tgrid, kStitchTileThreads, 0, st, p, (uint32_t *)bank, n, aligned, top_hist,
                      tile_cnt, tile_rows, hist_lo, hist_mask);
             break;
         case 8:
-            launch_k(stitch_tiles_kernel<uint64_t>, tgrid, 256, 0, st, p, (uint64_t *)bank, n, aligned, top_hist,
+            launch_k(stitch_tiles_kernel<uint64_t>, tgrid, kStitchTileThreads, 0, st, p, (uint64_t *)bank, n, aligned, top_hist,
                      tile_cnt, tile_rows, hist_lo, hist_mask);
             break;
         default: return set_error(ctx, FMCS_E_INVAL, "stitch: a sort bank has 2, 4 or 8 bytes");
