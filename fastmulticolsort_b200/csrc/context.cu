@@ -77,55 +77,6 @@ int ws_get(fmcs_ctx *ctx, int slot, size_t bytes, void **out, bool zero_new)
     return FMCS_OK;
 }
 
-int cond_handle(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle *h)
-{
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "cond_handle: capture info");
-    if (cs != cudaStreamCaptureStatusActive) return set_error(ctx, FMCS_E_INVAL, "cond_handle: stream not capturing");
-    e = cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault);
-    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "cond_handle: create");
-}
-
-int capture_if(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle h,
-               const std::function<int(cudaStream_t)> &body)
-{
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t g = nullptr;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: capture info");
-    if (cs != cudaStreamCaptureStatusActive) return set_error(ctx, FMCS_E_INVAL, "capture_if: stream not capturing");
-    if (!ctx->side) {
-        e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: stream");
-    }
-    cudaGraphNodeParams np = {};
-    np.type = cudaGraphNodeTypeConditional;
-    np.conditional.handle = h;
-    np.conditional.type = cudaGraphCondTypeIf;
-    np.conditional.size = 1;
-    cudaGraphNode_t node;
-    e = cudaGraphAddNode(&node, g, deps, ndeps, &np);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: node");
-    cudaGraph_t bodyg = np.conditional.phGraph_out[0];
-    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: dependencies");
-    e = cudaStreamBeginCaptureToGraph(ctx->side, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: body capture");
-    cudaStream_t saved = ctx->stream;
-    ctx->stream = ctx->side;
-    int rc = body(ctx->side);
-    ctx->stream = saved;
-    cudaGraph_t out = nullptr;
-    e = cudaStreamEndCapture(ctx->side, &out);
-    if (rc) return rc;
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture_if: body end");
-    return FMCS_OK;
-}
-
 int capture_while(fmcs_ctx *ctx, cudaStream_t st,
                   const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body)
 {
@@ -275,7 +226,7 @@ static void load_tuning(fmcs_ctx *ctx)
     ss << f.rdbuf();
     const std::string txt = ss.str();
     double v;
-    if (json_number(txt, "rank_mode", &v) && v >= 0 && v <= 2) ctx->rank_mode = (int)v;
+    if (json_number(txt, "rank_mode", &v) && v >= 0 && v <= 3) ctx->rank_mode = (int)v;
     if (json_number(txt, "local_max", &v) && v >= 128 && v <= 8192) ctx->local_max = (uint32_t)v;
     if (json_number(txt, "msd_items", &v)) ctx->msd_items = v >= 16 ? 16 : 8;
 }
@@ -313,7 +264,8 @@ extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
     }
     *ctx->h_status = 0;
     load_tuning(ctx);
-    if (const char *m = getenv("FMCS_RANK_MODE")) ctx->rank_mode = (m[0] == 'b' || m[0] == '1') ? 1 : (m[0] == 'o' || m[0] == '2') ? 2 : 0;
+    if (const char *m = getenv("FMCS_RANK_MODE"))
+        ctx->rank_mode = (m[0] == 'b' || m[0] == '1') ? 1 : (m[0] == 'o' || m[0] == '2') ? 2 : (m[0] == '3') ? 3 : 0;
     *out = ctx;
     return FMCS_OK;
 }
@@ -428,7 +380,7 @@ extern "C" int fmcs_set_tuning(fmcs_ctx *ctx, const char *key, long long value)
     if (!ctx || !key) return FMCS_E_INVAL;
     const std::string k(key);
     if (k == "rank_mode") {
-        if (value < 0 || value > 2) return set_error(ctx, FMCS_E_INVAL, "rank_mode must be 0, 1 or 2");
+        if (value < 0 || value > 3) return set_error(ctx, FMCS_E_INVAL, "rank_mode must be 0, 1, 2 or 3");
         ctx->rank_mode = (int)value;
     } else if (k == "local_max") {
         if (value < 128 || value > 8192) return set_error(ctx, FMCS_E_INVAL, "local_max must be in 128..8192");

@@ -155,14 +155,6 @@ class LaunchScope {
 int capture_while(fmcs_ctx *ctx, cudaStream_t st,
                   const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body);
 
-// A conditional handle of the graph being captured on `st` (default 0 at
-// every graph launch), and an IF node on it whose body is captured from
-// body(stream): the body runs when a kernel earlier in the graph has set the
-// handle to non-zero (cudaGraphSetConditional).
-int cond_handle(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle *h);
-int capture_if(fmcs_ctx *ctx, cudaStream_t st, cudaGraphConditionalHandle h,
-               const std::function<int(cudaStream_t)> &body);
-
 // Launches a library kernel with programmatic stream serialization: it may
 // begin launching while the stream's previous kernel finishes (its prologue
 // waits for that kernel's completion).  Every kernel launched this way starts

@@ -50,8 +50,8 @@ constexpr int kCapT32 = 32;  // the same up to 32 rows, for 2- and 4-byte keys (
 constexpr int kCapA = 128;   // warp per segment: 32 lanes x 4 items
 constexpr int kItemsA = 4;
 constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
-constexpr int kNtB2 = 256, kItB2 = 4, kCapB2 = kNtB2 * kItB2;   // 1024
-constexpr int kNtC1 = 512, kItC1 = 4, kCapC1 = kNtC1 * kItC1;   // 2048
+constexpr int kNtB2 = 128, kItB2 = 8, kCapB2 = kNtB2 * kItB2;   // 1024
+constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
 constexpr int kNtC1b = 512, kItC1b = 5, kCapC1b = kNtC1b * kItC1b;   // 2560
 constexpr int kNtC2 = 512, kItC2 = 8, kCapC2 = kNtC2 * kItC2;   // 4096
 constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
@@ -536,7 +536,8 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lis
 // msd_plan, whose offsets and skip marks it reads.
 // ---------------------------------------------------------------------------
 constexpr int kScanDigits = 4;     // digits per CTA of the tile scan (one 8-byte count load per tile)
-constexpr int kScanThreads = 256;
+constexpr int kScanThreads = 512;
+constexpr int kScanBatch = 8;      // count loads of a run in flight together
 
 struct SegSum {
     uint32_t head;                 // a segment starts inside the run
@@ -592,6 +593,13 @@ __global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(LevelRefs r, co
     const uint32_t a = threadIdx.x * per;
     const uint32_t b = min(T, a + per);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the counts of tiles [t, t + kScanBatch) of the run, loaded together
+    auto load_batch = [&](uint32_t t, ushort4 (&c)[kScanBatch]) {
+#pragma unroll
+        for (int i = 0; i < kScanBatch; ++i)
+            c[i] = t + i < b ? *reinterpret_cast<const ushort4 *>(r.tcnt + (uint64_t)(t + i) * kRadix + d0)
+                             : make_ushort4(0, 0, 0, 0);
+    };
     // pass 1: the run's sums since its last segment start
     SegSum mine{};
     uint32_t s0 = 0;
@@ -599,19 +607,24 @@ __global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(LevelRefs r, co
         s0 = segment_of_tile(tile_prefix, nseg, a);
         uint32_t s = s0, snext = tile_prefix[s0 + 1];
         mine.head = tile_prefix[s0] == a;
-        for (uint32_t t = a; t < b; ++t) {
-            if (t >= snext) {   // a segment starts at t (every large segment has a tile)
-                ++s;
-                snext = tile_prefix[s + 1];
-                mine.head = 1;
+        for (uint32_t t = a; t < b; t += kScanBatch) {
+            ushort4 c[kScanBatch];
+            load_batch(t, c);
 #pragma unroll
-                for (int j = 0; j < kScanDigits; ++j) mine.s[j] = 0;
+            for (int i = 0; i < kScanBatch; ++i) {
+                if (t + i >= b) break;
+                if (t + i >= snext) {   // a segment starts here (every large segment has a tile)
+                    ++s;
+                    snext = tile_prefix[s + 1];
+                    mine.head = 1;
+#pragma unroll
+                    for (int j = 0; j < kScanDigits; ++j) mine.s[j] = 0;
+                }
+                mine.s[0] += c[i].x;
+                mine.s[1] += c[i].y;
+                mine.s[2] += c[i].z;
+                mine.s[3] += c[i].w;
             }
-            const ushort4 c = *reinterpret_cast<const ushort4 *>(r.tcnt + (uint64_t)t * kRadix + d0);
-            mine.s[0] += c.x;
-            mine.s[1] += c.y;
-            mine.s[2] += c.z;
-            mine.s[3] += c.w;
         }
     }
     // block-wide exclusive segmented scan of the runs' sums
@@ -639,30 +652,36 @@ __global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(LevelRefs r, co
         run[j] = carried ? excl.s[j] : 0u;
         base[j] = sg.start + offs[(uint64_t)s0 * kRadix + d0 + j];
     }
-    for (uint32_t t = a; t < b; ++t) {
-        if (t >= snext) {
-            ++s;
-            sfirst = snext;
-            snext = tile_prefix[s + 1];
-            sg = segs[s];
+    for (uint32_t t0 = a; t0 < b; t0 += kScanBatch) {
+        ushort4 c[kScanBatch];
+        load_batch(t0, c);
 #pragma unroll
-            for (int j = 0; j < kScanDigits; ++j) {
-                run[j] = 0;
-                base[j] = sg.start + offs[(uint64_t)s * kRadix + d0 + j];
+        for (int i = 0; i < kScanBatch; ++i) {
+            const uint32_t t = t0 + i;
+            if (t >= b) break;
+            if (t >= snext) {
+                ++s;
+                sfirst = snext;
+                snext = tile_prefix[s + 1];
+                sg = segs[s];
+#pragma unroll
+                for (int j = 0; j < kScanDigits; ++j) {
+                    run[j] = 0;
+                    base[j] = sg.start + offs[(uint64_t)s * kRadix + d0 + j];
+                }
             }
-        }
-        const ushort4 c = *reinterpret_cast<const ushort4 *>(r.tcnt + (uint64_t)t * kRadix + d0);
-        *reinterpret_cast<uint4 *>(r.tdst + (uint64_t)t * kRadix + d0) =
-            make_uint4(base[0] + run[0], base[1] + run[1], base[2] + run[2], base[3] + run[3]);
-        run[0] += c.x;
-        run[1] += c.y;
-        run[2] += c.z;
-        run[3] += c.w;
-        if (blockIdx.x == 0) {
-            const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
-            const uint32_t rb = sg.start + (t - sfirst) * tile_rows;
-            const uint32_t cnt = min(tile_rows, sg.start + sg.len - rb);
-            r.tinfo[t] = make_uint4(rb, cnt, (sg.shift - width) | (width << 8) | (sg.src << 16), 0u);
+            *reinterpret_cast<uint4 *>(r.tdst + (uint64_t)t * kRadix + d0) =
+                make_uint4(base[0] + run[0], base[1] + run[1], base[2] + run[2], base[3] + run[3]);
+            run[0] += c[i].x;
+            run[1] += c[i].y;
+            run[2] += c[i].z;
+            run[3] += c[i].w;
+            if (blockIdx.x == 0) {
+                const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
+                const uint32_t rb = sg.start + (t - sfirst) * tile_rows;
+                const uint32_t cnt = min(tile_rows, sg.start + sg.len - rb);
+                r.tinfo[t] = make_uint4(rb, cnt, (sg.shift - width) | (width << 8) | (sg.src << 16), 0u);
+            }
         }
     }
 }
@@ -895,30 +914,48 @@ __global__ void __launch_bounds__(kNtM, scatter_ctas_per_sm(IT)) msd_scatter_ker
                     if (wbase + j * 32 + lane < cnt) key[j] = b.ext_bank[val[j]];
             }
             __syncthreads();   // the buffer's rows are in registers: its words are free
-            // kRankOr's per-warp peer words live in this tile's oid buffer
+            // the OR-word ranks' per-warp peer words live in this tile's oid
+            // buffer (a second array for the two-step rounds where it fits)
+            constexpr bool kOrWords = RANK == kRankOr || RANK == kRankOr2;
+            constexpr bool kTwoSteps = RANK == kRankOr2 && IT % 2 == 0 && kNtM * IT >= 2 * (kNtM / 32) * kRadix;
             uint32_t *const peerw = &sm.vals[Q][warp * kRadix];
+            uint32_t *const peerb = &sm.vals[Q][(kNtM / 32 + (kTwoSteps ? warp : 0)) * kRadix];
             for (int d = lane; d < kRadix; d += 32) {
                 sm.whist[warp][d] = 0;
-                if constexpr (RANK == kRankOr) peerw[d] = 0;
+                if constexpr (kOrWords) peerw[d] = 0;
+                if constexpr (kTwoSteps) peerb[d] = 0;
             }
             (void)peerw;
+            (void)peerb;
             __syncwarp();
             if (cnt == kTileM && width == (uint32_t)kRadixBits) {
                 // a whole tile and a whole digit (the common case): no lane checks
+                if constexpr (kTwoSteps) {
 #pragma unroll
-                for (int j = 0; j < IT; ++j) {
-                    const uint32_t d = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
-                    if constexpr (RANK == kRankOr)
-                        rd[j] = wlms_rank_or(d, true, sm.whist[warp], peerw) | (d << 16);
-                    else
-                        rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
+                    for (int j = 0; j < IT; j += 2) {
+                        const uint32_t d0 = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
+                        const uint32_t d1 = (uint32_t)((uint64_t)key[j + 1] >> lo) & (uint32_t)(kRadix - 1);
+                        uint32_t r0, r1;
+                        wlms_rank_or2(d0, d1, sm.whist[warp], peerw, peerb, r0, r1);
+                        rd[j] = r0 | (d0 << 16);
+                        rd[j + 1] = r1 | (d1 << 16);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < IT; ++j) {
+                        const uint32_t d = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
+                        if constexpr (kOrWords)
+                            rd[j] = wlms_rank_or(d, true, sm.whist[warp], peerw) | (d << 16);
+                        else
+                            rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
+                    }
                 }
             } else {
 #pragma unroll
                 for (int j = 0; j < IT; ++j) {
                     const uint32_t p = wbase + j * 32 + lane;
                     const uint32_t d = digit_of(key[j], lo, width);
-                    if constexpr (RANK == kRankOr)
+                    if constexpr (kOrWords)
                         rd[j] = wlms_rank_or(d, p < cnt, sm.whist[warp], peerw) | (d << 16);
                     else
                         rd[j] = wlms_rank<RANK>(d, p < cnt, sm.whist[warp], width) | (d << 16);
@@ -1682,20 +1719,6 @@ __global__ void __launch_bounds__(256) copy_tiles_kernel(Bufs<K> b, const LargeS
     }
 }
 
-// The IF nodes of a captured round's on-chip tiers: node i runs when the
-// counter word[i] (a tier's list size) is non-zero.
-struct TierGate {
-    cudaGraphConditionalHandle h[12];
-    uint32_t word[12];
-    int n;
-};
-
-__global__ void tier_gate_kernel(TierGate g, const uint32_t *ctr)
-{
-    kernel_prologue();
-    if ((int)threadIdx.x < g.n) cudaGraphSetConditional(g.h[threadIdx.x], ctr[g.word[threadIdx.x]] ? 1u : 0u);
-}
-
 template <typename F>
 int set_smem(fmcs_ctx *ctx, F *f, size_t bytes)
 {
@@ -1965,10 +1988,11 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1b, kItC1b, RANK>, smem_c1b))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC3, kItC3, RANK>, smem_c3))) return rc;
-    // Each tier's launch, with the counter word of its list.  A tier whose
-    // list is empty is not launched: eager calls know the lists' sizes from
-    // their last read-back (tiers_known), a captured graph puts each tier in
-    // an IF node that a gate kernel sets from the counters.
+    // Each tier's launch, with the counter word of its list.  An eager call
+    // that knows the lists' sizes from its last read-back (tiers_known) does
+    // not launch a tier whose list is empty.  A captured graph launches every
+    // tier (an empty one returns at once): one conditional node per tier cost
+    // more on replay than the empty launches it saved.
     struct Tier {
         int word;
         std::function<void(cudaStream_t)> launch;
@@ -2031,32 +2055,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         LaunchScope ls_(ctx, "copy_tiles");
         launch_k(copy_tiles_kernel<K>, sms * 8, 256, 0, s, b, lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix);
     }});
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    const bool capturing = a.fixed_launches && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
-                           cap == cudaStreamCaptureStatusActive;
-    if (capturing) {
-        TierGate gate{};
-        gate.n = (int)tiers.size();
-        for (size_t i = 0; i < tiers.size(); ++i) {
-            if ((rc = cond_handle(ctx, st, &gate.h[i]))) return rc;
-            gate.word[i] = (uint32_t)tiers[i].word;
-        }
-        {
-            LaunchScope ls_(ctx, "tier_gate");
-            launch_k(tier_gate_kernel, 1, 32, 0, st, gate, (const uint32_t *)ctr);
-        }
-        FMCS_LAUNCH_CHECK("tier gate");
-        for (size_t i = 0; i < tiers.size(); ++i) {
-            if ((rc = capture_if(ctx, st, gate.h[i], [&](cudaStream_t s) {
-                     tiers[i].launch(s);
-                     return FMCS_OK;
-                 })))
-                return rc;
-        }
-    } else {
-        for (const Tier &t : tiers)
-            if (!tiers_known || hctr[t.word] > 0) t.launch(st);
-    }
+    for (const Tier &t : tiers)
+        if (!tiers_known || hctr[t.word] > 0) t.launch(st);
     FMCS_LAUNCH_CHECK("local tiers");
     return FMCS_OK;
 }
@@ -2184,6 +2184,8 @@ template <typename K>
 static int sort_dispatch(fmcs_ctx *ctx, const SortArgs &a)
 {
     const bool big = ctx->msd_items >= 16;
+    if (ctx->rank_mode == 3)
+        return big ? sort_segments_t<K, kRankOr2, 16>(ctx, a) : sort_segments_t<K, kRankOr2, 8>(ctx, a);
     if (ctx->rank_mode == 2)
         return big ? sort_segments_t<K, kRankOr, 16>(ctx, a) : sort_segments_t<K, kRankOr, 8>(ctx, a);
     if (ctx->rank_mode)

@@ -87,7 +87,9 @@ FMCS_API unsigned long long fmcs_launch_count(const fmcs_ctx *ctx);
  * starts from the autotuner's file (tuning/b200.json next to the library, or
  * the file FMCS_TUNING names), else the built-in defaults.  Keys:
  *   "rank_mode"  0: match.any multi-split ranking, 1: ballot multi-split,
- *                2: shared-memory OR peer words (HBM radix levels; ballot elsewhere);
+ *                2: shared-memory OR peer words (HBM radix levels; ballot elsewhere),
+ *                3: as 2, two steps of a warp ranked per round where the radix
+ *                   tile has room for a second peer array (4,096-row tiles);
  *   "local_max"  128..8192: segments with more rows take the HBM radix levels;
  *   "msd_items"  8 or 16: items per thread of an HBM radix tile.
  * fmcs_get_tuning returns -1 for an unknown key. */
@@ -247,8 +249,7 @@ FMCS_API int fmcs_write_columns_text(const char *path, int with_header, uint32_t
  * It runs in a private context (own stream and workspace, sized by one eager
  * run at creation); every radix level is part of the graph and exits on the
  * device when it has no work, so a replay needs no host round trip until its
- * final status check; the on-chip tiers that a replay's data leaves empty are
- * skipped on the device.  fmcs_graph_create_hash captures the same plan
+ * final status check.  fmcs_graph_create_hash captures the same plan
  * through the hash-grouping rounds (run_single_plan_hash,
  * src/stitch_composer.cpp:808-1079), whose key widths and clustering are also
  * decided on the device.  fmcs_graph_launch returns when the results are
