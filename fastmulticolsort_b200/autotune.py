@@ -31,7 +31,7 @@ from . import workloads as W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "tuning", "b200.json")
-KNOBS = {"rank_mode": (0, 1, 2, 3), "local_max": (2048, 4096, 8192), "msd_items": (8, 16)}
+KNOBS = {"rank_mode": (0, 1, 2), "local_max": (2048, 4096, 8192), "msd_items": (8, 16)}
 
 
 def _dev(a):

@@ -226,7 +226,7 @@ static void load_tuning(fmcs_ctx *ctx)
     ss << f.rdbuf();
     const std::string txt = ss.str();
     double v;
-    if (json_number(txt, "rank_mode", &v) && v >= 0 && v <= 3) ctx->rank_mode = (int)v;
+    if (json_number(txt, "rank_mode", &v) && v >= 0 && v <= 2) ctx->rank_mode = (int)v;
     if (json_number(txt, "local_max", &v) && v >= 128 && v <= 8192) ctx->local_max = (uint32_t)v;
     if (json_number(txt, "msd_items", &v)) ctx->msd_items = v >= 16 ? 16 : 8;
 }
@@ -265,7 +265,7 @@ extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
     *ctx->h_status = 0;
     load_tuning(ctx);
     if (const char *m = getenv("FMCS_RANK_MODE"))
-        ctx->rank_mode = (m[0] == 'b' || m[0] == '1') ? 1 : (m[0] == 'o' || m[0] == '2') ? 2 : (m[0] == '3') ? 3 : 0;
+        ctx->rank_mode = (m[0] == 'b' || m[0] == '1') ? 1 : (m[0] == 'o' || m[0] == '2') ? 2 : 0;
     *out = ctx;
     return FMCS_OK;
 }
@@ -380,7 +380,7 @@ extern "C" int fmcs_set_tuning(fmcs_ctx *ctx, const char *key, long long value)
     if (!ctx || !key) return FMCS_E_INVAL;
     const std::string k(key);
     if (k == "rank_mode") {
-        if (value < 0 || value > 3) return set_error(ctx, FMCS_E_INVAL, "rank_mode must be 0, 1, 2 or 3");
+        if (value < 0 || value > 2) return set_error(ctx, FMCS_E_INVAL, "rank_mode must be 0, 1 or 2");
         ctx->rank_mode = (int)value;
     } else if (k == "local_max") {
         if (value < 128 || value > 8192) return set_error(ctx, FMCS_E_INVAL, "local_max must be in 128..8192");

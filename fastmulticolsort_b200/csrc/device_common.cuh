@@ -86,7 +86,6 @@ __device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, uint32_t f
 constexpr int kRankMatch = 0;
 constexpr int kRankBallot = 1;
 constexpr int kRankOr = 2;
-constexpr int kRankOr2 = 3;   // kRankOr, two steps ranked per round where the scatter has room (else kRankOr)
 
 template <int MODE>
 __device__ __forceinline__ uint32_t peers_of(uint32_t digit, bool valid, uint32_t width)
@@ -171,37 +170,6 @@ __device__ __forceinline__ uint32_t wlms_rank_or(uint32_t digit, bool valid, uin
     }
     __syncwarp();
     return base + below;
-}
-
-// Two consecutive steps (j and j + 1) of a warp's full, valid items ranked in
-// one round by shared-memory OR words: `pa` and `pb` are the warp's peer
-// arrays of step j and step j + 1 (all zero on entry and on exit).  A step
-// j + 1 item's rank adds the step j items of its digit (pa[d1]).  The digit
-// counters are written in order: step j's leaders first, then step j + 1's,
-// whose total includes step j's items of the same digit.
-__device__ __forceinline__ void wlms_rank_or2(uint32_t d0, uint32_t d1, uint32_t *whist, uint32_t *pa, uint32_t *pb,
-                                              uint32_t &r0, uint32_t &r1)
-{
-    const uint32_t bit = 1u << lane_id();
-    const uint32_t lt = lanemask_lt();
-    atomicOr(&pa[d0], bit);
-    atomicOr(&pb[d1], bit);
-    __syncwarp();
-    const uint32_t p0 = pa[d0];   // step j lanes of digit d0
-    const uint32_t p1 = pb[d1];   // step j + 1 lanes of digit d1
-    const uint32_t x1 = pa[d1];   // step j lanes of digit d1
-    const uint32_t b0 = whist[d0];
-    const uint32_t b1 = whist[d1];
-    __syncwarp();
-    const uint32_t below0 = __popc(p0 & lt), below1 = __popc(p1 & lt);
-    r0 = b0 + below0;
-    r1 = b1 + __popc(x1) + below1;
-    if (below0 == 0) whist[d0] = b0 + __popc(p0);
-    __syncwarp();
-    if (below1 == 0) whist[d1] = b1 + __popc(x1) + __popc(p1);
-    if (below0 == 0) pa[d0] = 0;
-    if (below1 == 0) pb[d1] = 0;
-    __syncwarp();
 }
 
 // Exclusive scan of kRadix counters in shared memory by a block of NT threads.

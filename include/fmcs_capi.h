@@ -87,9 +87,7 @@ FMCS_API unsigned long long fmcs_launch_count(const fmcs_ctx *ctx);
  * starts from the autotuner's file (tuning/b200.json next to the library, or
  * the file FMCS_TUNING names), else the built-in defaults.  Keys:
  *   "rank_mode"  0: match.any multi-split ranking, 1: ballot multi-split,
- *                2: shared-memory OR peer words (HBM radix levels; ballot elsewhere),
- *                3: as 2, two steps of a warp ranked per round where the radix
- *                   tile has room for a second peer array (4,096-row tiles);
+ *                2: shared-memory OR peer words (HBM radix levels; ballot elsewhere);
  *   "local_max"  128..8192: segments with more rows take the HBM radix levels;
  *   "msd_items"  8 or 16: items per thread of an HBM radix tile.
  * fmcs_get_tuning returns -1 for an unknown key. */
