@@ -236,73 +236,4 @@ __device__ __forceinline__ unsigned long long lb_wait(const unsigned long long *
     return lb_word(epoch, kFlagInclusive, 0);
 }
 
-// ---------------------------------------------------------------------------
-// Bulk copies global -> shared memory (cp.async.bulk, the TMA engine's 1-D
-// form) completing on a shared-memory mbarrier.  Source and destination must
-// be 16-byte aligned and the size a multiple of 16 bytes; the copies read this
-// GPU's own memory only and never multicast.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t arrivals)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(arrivals) : "memory");
-}
-
-// Makes mbarrier initialisation visible to the async proxy (the bulk copies).
-__device__ __forceinline__ void fence_mbar_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-// Orders this thread's earlier generic-proxy shared-memory accesses (made
-// visible to it by a barrier) before its later async-proxy ones: needed before
-// a bulk copy overwrites shared memory that threads have just read or written.
-__device__ __forceinline__ void fence_proxy_async_smem()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// One arrival that also expects `bytes` of copies to complete on the barrier.
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_copy_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes,
-                                              unsigned long long *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst_smem)),
-                 "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for the phase of parity `parity` of a bulk-copy barrier.
-// Returns false after recording FMCS_E_TIMEOUT in *status (the caller then
-// skips the tile's work; the copies it waited for target only its own
-// shared memory).
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity, int *status,
-                                          uint32_t limit = kSpinLimit)
-{
-    for (uint32_t it = 0; it < limit; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    atomicCAS(status, kDevOk, kDevTimeout);
-    return false;
-}
-
 }  // namespace fmcs

@@ -50,8 +50,6 @@ enum Slot : int {
     kSlotGroupB,      // run_plan group pong
     kSlotColStage,    // run_plan host column staging (several columns)
     kSlotTopHist,     // level-0 digit histogram of a round-0 bank, counted by the stitch
-    kSlotTileCnt,     // per-tile digit counts of an HBM radix level (level 0's from the stitch)
-    kSlotTileDst,     // per-tile digit destinations and tile descriptors of an HBM radix level
     kSlotMisc,
     kSlotCount
 };
@@ -189,11 +187,9 @@ struct StitchSlice {
 constexpr int kMaxSlices = 32;
 // With top_hist (device, 256 words), the stitch also counts the top digit
 // (bits [key_bits - min(8, key_bits), key_bits)) of every bank value: the
-// first radix level's histogram of a round-0 sort of the bank, in all
-// (top_hist) and per tile of tile_rows rows (tile_cnt, 256 u16 per tile).
+// first radix level's histogram of a round-0 sort of the bank.
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0, uint16_t *tile_cnt = nullptr,
-                  uint32_t tile_rows = 0);
+                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0);
 
 // bank[i] <<= lshift (src == NULL) or bank[i] |= (src[i] >> rshift) & mask(width)
 int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,
@@ -225,13 +221,6 @@ struct SortArgs {
     const uint32_t *d_in_order = nullptr;
 };
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
-// Rows of an HBM radix tile (the context's msd_items x 256 threads), and the
-// most tiles one radix level of a sort of n rows can have.
-uint32_t sort_tile_rows(const fmcs_ctx *ctx);
-uint64_t sort_level_tiles(const fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows);
-// The per-tile arrays of the radix levels (workspace slots kSlotTileCnt,
-// kSlotTileDst), sized for a sort of n rows in tiles of tile_rows rows.
-int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo);
 // Stable full-array LSD radix sort of (keys, vals) in place by key bits
 // [0, bits): the plain, unsegmented comparator path.
 int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits);

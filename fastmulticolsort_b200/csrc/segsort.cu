@@ -9,20 +9,19 @@
 //
 // B200 design.  Every group is a segment [start, start+len) that is sorted in
 // place (segments never move).  Segments are binned by size:
-//   thread   len <= 16 (32)   one thread, an odd-even transposition network
-//   warp     len <= 128       one warp, LSD radix in registers/smem
-//   block    len <= 8192      one CTA, in six tiers of 512 to 8192 rows:
-//                             compound-key buckets in shared memory
-//   large    len > local_max  HBM radix levels: per-tile digit counts, a
-//                             column scan of them into per-tile destinations,
-//                             and a stable scatter of TMA-fed tiles; every
-//                             non-empty bucket becomes a child segment with 8
-//                             bits fewer, re-binned into the tiers above.
-// Each key is ranked by warp-level multi-split (match.any / ballots / shared
-// OR words + popc) so every pass is stable, and the whole sort is stable:
+//   tier A  len <= 128   one warp per segment, LSD radix in registers/smem
+//   tier B  len <= 1024  one 128-thread CTA per segment, LSD radix in smem
+//   tier C  len <= 4096  one 256-thread CTA per segment, LSD radix in smem
+//   large   len >  4096  MSD radix levels: per-segment digit histogram, then a
+//                        onesweep-style stable scatter with a decoupled
+//                        look-back chained over the segment's tiles; every
+//                        non-empty bucket becomes a child segment with 8 bits
+//                        fewer, re-binned into the tiers above.
+// Each key is ranked by warp-level multi-split (match.any + popc) so every
+// pass is stable; the MSD scatter is stable too, so the whole sort is stable:
 // ties keep the oid order of the input, which is what the reference gives once
-// its ties are canonicalised to ascending oid.  A row moves through HBM only in
-// the large tier; a thread/warp/block segment is read once and written once.
+// its ties are canonicalised to ascending oid.  Rows move only through HBM in
+// the large tier; a tier-A/B/C segment is read once and written once.
 //
 // Data sources of a segment: BUF0 (final buffer: the caller's order array and
 // the sorted-key array), BUF1 (work buffer), EXT (the round's input: the bank
@@ -32,7 +31,8 @@
 #include "fmcs_internal.h"
 
 #include <algorithm>
-#include <type_traits>
+#include <functional>
+#include <vector>
 
 namespace fmcs {
 
@@ -57,6 +57,7 @@ constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
 constexpr int kCapLocal = kCapC3;   // largest segment a local tier can take; larger: MSD levels
 constexpr int kNtM = 256;           // MSD tile: 256 threads x IT items (IT = 8 or 16, tuned)
 constexpr int kHistCtas = 4;         // resident histogram CTAs per SM (the grid is one wave)
+constexpr int kMsdCtas16 = 3;       // resident scatter CTAs per SM with 16 rows per thread
 
 // counters slot words
 constexpr int kCtrMsdTile = 1;
@@ -88,21 +89,12 @@ struct LargeSeg {
 // otherwise every launch works on set 0.
 // (Kernels select a set with a conditional, not by indexing with the level
 // parity: a parameter array indexed at run time is copied to local memory.)
-// Per-tile arrays of a level (tiles of the level's large segments, in tile
-// prefix order): tcnt[t][d] the tile's digit counts (u16: a tile has at most
-// 4,096 rows); tdst[t][d] the global position of the tile's first row of
-// digit d (segment start + the digit's offset in the segment + the rows of
-// digit d in the segment's earlier tiles); tinfo[t] = (first row, rows,
-// lo | width << 8 | src << 16, 0).
 struct LevelRefs {
     LargeSeg *large[2];
     uint32_t *hist[2];
     uint32_t *ctr;
     int dev_level;
-    int hist0_ready;   // level 0's counts were made before the sort (by the stitch)
-    uint16_t *tcnt;
-    uint32_t *tdst;
-    uint4 *tinfo;
+    int hist0_ready;   // level 0's histogram was counted before the sort (by the stitch)
 };
 
 // Index of the level whose launches are running (level_prefix_kernel has
@@ -405,19 +397,15 @@ __device__ __forceinline__ uint32_t find_segment_warp(const uint32_t *tile_prefi
     return lo;
 }
 
-// Top-digit counts of every tile of every large segment (tcnt) and of every
-// large segment (hist).  A block takes a contiguous run of tiles; each thread
-// issues all of a tile's loads before counting (up to 16 in flight), and each
-// warp counts into its own shared sub-histogram so that skewed digits do not
-// serialize the whole block on one counter.  Thread d keeps the running total
-// of digit d over the run's part of the current segment and adds it to the
-// segment's row once per segment.
+// Top-digit histogram of every large segment.  A block takes a contiguous run
+// of tiles; each thread issues all of a tile's loads before counting (up to 16
+// in flight), and each warp counts into its own shared sub-histogram so that
+// skewed digits do not serialize the whole block on one counter.
 template <typename K>
 __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, LevelRefs r, const uint32_t *tile_prefix,
                                                         uint32_t tile_rows)
 {
     kernel_prologue();
-    static_assert(kNtM == kRadix, "thread d owns digit d");
     constexpr int NW = kNtM / 32;
     constexpr int MAXJ = 16;   // tile_rows <= 16 * kNtM
     __shared__ uint32_t sh[NW][kRadix];
@@ -430,21 +418,34 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
     const int warp = threadIdx.x >> 5;
-    const uint32_t d = threadIdx.x;
+    // a contiguous run of tiles per block; the per-warp counts are added to
+    // the segment's histogram when the run moves to the next segment (every
+    // large segment has at least one tile) and at its end
     const uint32_t per = (T + gridDim.x - 1) / gridDim.x;
     const uint32_t t0 = blockIdx.x * per;
     const uint32_t t1 = min(T, t0 + per);
     if (t0 >= T) return;
-    for (int i = threadIdx.x; i < NW * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+    for (int d = threadIdx.x; d < NW * kRadix; d += blockDim.x) (&sh[0][0])[d] = 0;
     uint32_t s = find_segment_warp(tile_prefix, nseg, t0);
     LargeSeg sg = segs[s];
     uint32_t sfirst = tile_prefix[s], snext = tile_prefix[s + 1];
-    uint32_t segacc = 0;
+    auto flush = [&]() {
+        __syncthreads();
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+            uint32_t c = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                c += sh[w][d];
+                sh[w][d] = 0;
+            }
+            if (c) atomicAdd(&hist[(uint64_t)s * kRadix + d], c);
+        }
+        __syncthreads();
+    };
     __syncthreads();
     for (uint32_t t = t0; t < t1; ++t) {
         if (t >= snext) {
-            if (segacc) atomicAdd(&hist[(uint64_t)s * kRadix + d], segacc);
-            segacc = 0;
+            flush();
             ++s;
             sg = segs[s];
             sfirst = snext;
@@ -466,18 +467,8 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
             const uint64_t i = beg + threadIdx.x + (uint64_t)j * kNtM;
             if (i < end) atomicAdd(&sh[warp][digit_of(key[j], lo, width)], 1u);
         }
-        __syncthreads();
-        uint32_t c = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            c += sh[w][d];
-            sh[w][d] = 0;
-        }
-        r.tcnt[(uint64_t)t * kRadix + d] = (uint16_t)c;
-        segacc += c;
-        __syncthreads();
     }
-    if (segacc) atomicAdd(&hist[(uint64_t)s * kRadix + d], segacc);
+    flush();
 }
 
 // Per large segment: exclusive digit offsets, skip detection, children.
@@ -519,245 +510,38 @@ __global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lis
     }
 }
 
-// ---------------------------------------------------------------------------
-// Tile scan: for every tile of the level, the global position of its first
-// row of each digit (tdst: segment start + the digit's offset in the segment
-// + the rows of that digit in the segment's earlier tiles) and its descriptor
-// (tinfo).  A column scan with no waits: CTA c takes digits [4c, 4c + 4), its
-// thread i a contiguous run of tiles; each thread sums its run's counts from
-// the run's last segment start, one block-wide segmented scan (the sums reset
-// where a segment starts) gives every run the counts of its segment's earlier
-// tiles, and a second walk over the run writes the destinations.  Runs after
-// msd_plan, whose offsets and skip marks it reads.
-// ---------------------------------------------------------------------------
-constexpr int kScanDigits = 4;     // digits per CTA of the tile scan (one 8-byte count load per tile)
-constexpr int kScanThreads = 512;
-constexpr int kScanBatch = 8;      // count loads of a run in flight together
-
-struct SegSum {
-    uint32_t head;                 // a segment starts inside the run
-    uint32_t s[kScanDigits];       // counts since the run's last segment start (or its first tile)
-};
-
-// left (earlier tiles) then right: a start in the right part resets the sums
-__device__ __forceinline__ SegSum seg_combine(const SegSum &l, const SegSum &r)
-{
-    SegSum o;
-    o.head = l.head | r.head;
-#pragma unroll
-    for (int j = 0; j < kScanDigits; ++j) o.s[j] = r.head ? r.s[j] : l.s[j] + r.s[j];
-    return o;
-}
-
-__device__ __forceinline__ SegSum seg_shfl_up(const SegSum &v, int o)
-{
-    SegSum w;
-    w.head = __shfl_up_sync(0xFFFFFFFFu, v.head, o);
-#pragma unroll
-    for (int j = 0; j < kScanDigits; ++j) w.s[j] = __shfl_up_sync(0xFFFFFFFFu, v.s[j], o);
-    return w;
-}
-
-// the large segment holding tile t: tile_prefix[s] <= t < tile_prefix[s + 1]
-__device__ __forceinline__ uint32_t segment_of_tile(const uint32_t *tile_prefix, uint32_t nseg, uint32_t t)
-{
-    uint32_t lo = 0, hi = nseg;
-    while (hi - lo > 1) {
-        const uint32_t m = (lo + hi) >> 1;
-        if (tile_prefix[m] <= t) lo = m;
-        else hi = m;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(LevelRefs r, const uint32_t *tile_prefix,
-                                                                uint32_t tile_rows)
-{
-    kernel_prologue();
-    constexpr int NW = kScanThreads / 32;
-    __shared__ SegSum wsum[NW];
-    const uint32_t lvl = running_level(r);
-    const uint32_t cur = lvl & 1u;
-    const LargeSeg *segs = cur ? r.large[1] : r.large[0];
-    const uint32_t *offs = cur ? r.hist[1] : r.hist[0];
-    const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
-    if (nseg == 0) return;
-    const uint32_t T = tile_prefix[nseg];
-    const uint32_t d0 = blockIdx.x * kScanDigits;
-    const uint32_t per = (T + kScanThreads - 1) / kScanThreads;
-    const uint32_t a = threadIdx.x * per;
-    const uint32_t b = min(T, a + per);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // the counts of tiles [t, t + kScanBatch) of the run, loaded together
-    auto load_batch = [&](uint32_t t, ushort4 (&c)[kScanBatch]) {
-#pragma unroll
-        for (int i = 0; i < kScanBatch; ++i)
-            c[i] = t + i < b ? *reinterpret_cast<const ushort4 *>(r.tcnt + (uint64_t)(t + i) * kRadix + d0)
-                             : make_ushort4(0, 0, 0, 0);
-    };
-    // pass 1: the run's sums since its last segment start
-    SegSum mine{};
-    uint32_t s0 = 0;
-    if (a < b) {
-        s0 = segment_of_tile(tile_prefix, nseg, a);
-        uint32_t s = s0, snext = tile_prefix[s0 + 1];
-        mine.head = tile_prefix[s0] == a;
-        for (uint32_t t = a; t < b; t += kScanBatch) {
-            ushort4 c[kScanBatch];
-            load_batch(t, c);
-#pragma unroll
-            for (int i = 0; i < kScanBatch; ++i) {
-                if (t + i >= b) break;
-                if (t + i >= snext) {   // a segment starts here (every large segment has a tile)
-                    ++s;
-                    snext = tile_prefix[s + 1];
-                    mine.head = 1;
-#pragma unroll
-                    for (int j = 0; j < kScanDigits; ++j) mine.s[j] = 0;
-                }
-                mine.s[0] += c[i].x;
-                mine.s[1] += c[i].y;
-                mine.s[2] += c[i].z;
-                mine.s[3] += c[i].w;
-            }
-        }
-    }
-    // block-wide exclusive segmented scan of the runs' sums
-    SegSum incl = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const SegSum up = seg_shfl_up(incl, o);
-        if (lane >= o) incl = seg_combine(up, incl);
-    }
-    if (lane == 31) wsum[warp] = incl;
-    __syncthreads();
-    SegSum before{};   // everything before this warp
-    for (int w = 0; w < warp; ++w) before = seg_combine(before, wsum[w]);
-    SegSum lane_excl = seg_shfl_up(incl, 1);
-    if (lane == 0) lane_excl = SegSum{};
-    const SegSum excl = seg_combine(before, lane_excl);
-    if (a >= b) return;
-    // pass 2: destinations and descriptors
-    uint32_t s = s0, snext = tile_prefix[s0 + 1], sfirst = tile_prefix[s0];
-    LargeSeg sg = segs[s0];
-    uint32_t run[kScanDigits], base[kScanDigits];
-    const bool carried = sfirst < a;   // the run's first segment began in an earlier run
-#pragma unroll
-    for (int j = 0; j < kScanDigits; ++j) {
-        run[j] = carried ? excl.s[j] : 0u;
-        base[j] = sg.start + offs[(uint64_t)s0 * kRadix + d0 + j];
-    }
-    for (uint32_t t0 = a; t0 < b; t0 += kScanBatch) {
-        ushort4 c[kScanBatch];
-        load_batch(t0, c);
-#pragma unroll
-        for (int i = 0; i < kScanBatch; ++i) {
-            const uint32_t t = t0 + i;
-            if (t >= b) break;
-            if (t >= snext) {
-                ++s;
-                sfirst = snext;
-                snext = tile_prefix[s + 1];
-                sg = segs[s];
-#pragma unroll
-                for (int j = 0; j < kScanDigits; ++j) {
-                    run[j] = 0;
-                    base[j] = sg.start + offs[(uint64_t)s * kRadix + d0 + j];
-                }
-            }
-            *reinterpret_cast<uint4 *>(r.tdst + (uint64_t)t * kRadix + d0) =
-                make_uint4(base[0] + run[0], base[1] + run[1], base[2] + run[2], base[3] + run[3]);
-            run[0] += c[i].x;
-            run[1] += c[i].y;
-            run[2] += c[i].z;
-            run[3] += c[i].w;
-            if (blockIdx.x == 0) {
-                const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
-                const uint32_t rb = sg.start + (t - sfirst) * tile_rows;
-                const uint32_t cnt = min(tile_rows, sg.start + sg.len - rb);
-                r.tinfo[t] = make_uint4(rb, cnt, (sg.shift - width) | (width << 8) | (sg.src << 16), 0u);
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// MSD scatter: every tile's rows move to their bucket in the level's other
-// buffer, stably.  The positions come from the tile scan, so no tile waits
-// for another: each CTA takes tiles blockIdx.x, blockIdx.x + grid, ... and
-// keeps the next one streaming into shared memory while it works on the
-// current one.  Per tile, one thread issues bulk copies (TMA) of the 16-byte
-// aligned interior of the tile's keys and oids and of its tdst row into one of
-// two buffers, completing on that buffer's mbarrier; the lanes of warp 0 load
-// the unaligned rows at either end into registers at the same time and store
-// them into the buffer when the tile's turn comes.  Then the rows are ranked
-// by warp-level multi-split (stable), laid out in digit order in the same
-// buffer and written out in runs of equal digit.
-// ---------------------------------------------------------------------------
-constexpr int scatter_ctas_per_sm(int it) { return it >= 16 ? 2 : 3; }
+// Resident CTAs of the scatter per SM (the launch bound and the grid).
+constexpr int msd_ctas_per_sm(int it) { return it >= 16 ? kMsdCtas16 : 4; }
 
 template <typename K, int IT>
-struct ScatterSmem {
-    K keys[2][kNtM * IT + 16 / sizeof(K)];   // room for the tile's misalignment inside 16 bytes
-    uint32_t vals[2][kNtM * IT + 4];
-    uint32_t gdst[2][kRadix];                // the tile's tdst row, then its per-digit bases
+struct MsdSmem {
     uint32_t whist[kNtM / 32][kRadix];
-    uint32_t doff[kRadix];
-    uint4 info[2];
-    unsigned long long bar[2];
+    uint32_t total[kRadix];
+    uint32_t doff[kRadix];       // tile-local exclusive digit offsets
+    uint32_t gdst[kRadix];       // global destination base per digit (mod 2^32; rows < 2^32)
     uint32_t tmp[kNtM / 32 + 1];
-    static_assert((sizeof(K) * (kNtM * IT + 16 / sizeof(K))) % 16 == 0, "16-byte aligned buffers");
-    static_assert(kNtM * IT >= (kNtM / 32) * kRadix, "the peer words of kRankOr fit in a vals buffer");
+    uint32_t tile, seg;
+    K keys[kNtM * IT];
+    uint32_t vals[kNtM * IT];
+    static_assert(kNtM * IT >= (kNtM / 32) * kRadix, "the peer words of kRankOr fit in vals");
 };
-
-// The unaligned rows of one tile held by a lane of warp 0 until the tile's
-// turn: at most one key row and one oid row per lane.
-template <typename K>
-struct EdgeRows {
-    K key;
-    uint32_t val;
-    int ki, vi;   // row of the tile, -1: none
-};
-
-// The aligned interior [a0, a1) of the bytes of rows [rb, rb + cnt) of `base`
-// and the unaligned rows at either end.
-struct CopyPlan {
-    uintptr_t a0, a1;   // copy when a1 > a0
-    uint32_t sh;        // the tile's first row sits at element `sh` of its buffer
-    uint32_t nhead, tail0, ntail;
-};
-
-template <int EB>
-__device__ __forceinline__ CopyPlan copy_plan(const void *base, uint32_t rb, uint32_t cnt)
-{
-    CopyPlan c;
-    const uintptr_t gb = (uintptr_t)base + (uintptr_t)rb * EB;
-    const uintptr_t ge = gb + (uintptr_t)cnt * EB;
-    c.a0 = (gb + 15) & ~(uintptr_t)15;
-    c.a1 = ge & ~(uintptr_t)15;
-    c.sh = (uint32_t)(gb & 15) / EB;
-    if (c.a1 > c.a0) {
-        c.nhead = (uint32_t)((c.a0 - gb) / EB);
-        c.tail0 = (uint32_t)((c.a1 - gb) / EB);
-        c.ntail = cnt - c.tail0;
-    } else {
-        c.nhead = cnt;   // fewer than 31 bytes: every row is an edge row
-        c.tail0 = cnt;
-        c.ntail = 0;
-    }
-    return c;
-}
 
 template <typename K, int RANK, int IT>
-__global__ void __launch_bounds__(kNtM, scatter_ctas_per_sm(IT)) msd_scatter_kernel(
-    Bufs<K> b, LevelRefs r, const uint32_t *tile_prefix, int *status, cudaGraphConditionalHandle more, uint32_t levels)
+__global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(Bufs<K> b, LevelRefs r,
+                                                           const uint32_t *tile_prefix, unsigned long long *lookback,
+                                                           uint32_t epoch_base, int *status,
+                                                           cudaGraphConditionalHandle more, uint32_t levels)
 {
     kernel_prologue();
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    ScatterSmem<K, IT> &sm = *reinterpret_cast<ScatterSmem<K, IT> *>(smem_raw);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MsdSmem<K, IT> &sm = *reinterpret_cast<MsdSmem<K, IT> *>(smem_raw);
     constexpr uint32_t kTileM = kNtM * IT;
     const uint32_t lvl = running_level(r);
     const uint32_t cur = lvl & 1u;
+    const LargeSeg *segs = (cur ? r.large[1] : r.large[0]);
+    const uint32_t *offs = (cur ? r.hist[1] : r.hist[0]);
+    uint32_t *tile_counter = &r.ctr[kCtrMsdTile];
+    const uint32_t epoch = epoch_base + lvl;
     const uint32_t nseg = r.ctr[kCtrLarge0 + cur];
     // Inside a graph, the level loop goes on while the next level has large
     // segments (msd_plan has counted them before this launch).
@@ -776,225 +560,119 @@ __global__ void __launch_bounds__(kNtM, scatter_ctas_per_sm(IT)) msd_scatter_ker
     }
     if (nseg == 0) return;
     const uint32_t T = tile_prefix[nseg];
-    const uint32_t G = gridDim.x;
-    if (blockIdx.x >= T) return;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        mbar_init(&sm.bar[0], 1);
-        mbar_init(&sm.bar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    auto keys_of = [&](uint32_t src) -> const K * {
-        return src == kSrcExt ? (b.ext_order ? nullptr : b.ext_bank) : (src == kSrcBuf1 ? b.k1 : b.k0);
-    };
-    auto vals_of = [&](uint32_t src) -> const uint32_t * {
-        return src == kSrcExt ? b.ext_order : (src == kSrcBuf1 ? b.v1 : b.v0);
-    };
-
-    // Start tile t streaming into buffer Q (warp 0; every other warp skips).
-    // Returns true in the thread that issued bulk copies.
-    auto prefetch = [&](auto qc, uint32_t t, EdgeRows<K> &e) -> bool {
-        constexpr int Q = decltype(qc)::value;
-        if (warp != 0) return false;
-        uint4 info = make_uint4(0u, 0u, 1u << 24, 0u);   // past the last tile: a skipped tile
-        if (t < T) {
-            if (lane == 0) info = r.tinfo[t];
-            info.x = __shfl_sync(0xFFFFFFFFu, info.x, 0);
-            info.y = __shfl_sync(0xFFFFFFFFu, info.y, 0);
-            info.z = __shfl_sync(0xFFFFFFFFu, info.z, 0);
-        }
-        if (lane == 0) sm.info[Q] = info;
-        e.ki = -1;
-        e.vi = -1;
-        if ((info.z >> 24) & 1u) return false;   // skipped tile: nothing to copy
-        const uint32_t rb = info.x, cnt = info.y, src = (info.z >> 16) & 3u;
-        const K *kp = keys_of(src);
-        const uint32_t *vp = vals_of(src);
-        CopyPlan kc{}, vc{};
-        uint32_t bytes = kRadix * sizeof(uint32_t);
-        if (kp) {
-            kc = copy_plan<sizeof(K)>(kp, rb, cnt);
-            if (kc.a1 > kc.a0) bytes += (uint32_t)(kc.a1 - kc.a0);
-        }
-        if (vp) {
-            vc = copy_plan<4>(vp, rb, cnt);
-            if (vc.a1 > vc.a0) bytes += (uint32_t)(vc.a1 - vc.a0);
-        }
-        if (lane == 0) {
-            // the buffer's earlier contents were read and written by every
-            // thread before the barrier that preceded this call
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&sm.bar[Q], bytes);
-            bulk_copy_g2s(&sm.gdst[Q][0], r.tdst + (uint64_t)t * kRadix, kRadix * sizeof(uint32_t), &sm.bar[Q]);
-            if (kp && kc.a1 > kc.a0)
-                bulk_copy_g2s(reinterpret_cast<char *>(&sm.keys[Q][0]) + (kc.a0 - (((uintptr_t)kp + (uintptr_t)rb * sizeof(K)) & ~(uintptr_t)15)),
-                              (const void *)kc.a0, (uint32_t)(kc.a1 - kc.a0), &sm.bar[Q]);
-            if (vp && vc.a1 > vc.a0)
-                bulk_copy_g2s(reinterpret_cast<char *>(&sm.vals[Q][0]) + (vc.a0 - (((uintptr_t)vp + (uintptr_t)rb * 4u) & ~(uintptr_t)15)),
-                              (const void *)vc.a0, (uint32_t)(vc.a1 - vc.a0), &sm.bar[Q]);
-        }
-        // unaligned rows: lane l takes the l-th edge row of the keys and of the oids
-        if (kp && (uint32_t)lane < kc.nhead + kc.ntail) {
-            const uint32_t i = (uint32_t)lane < kc.nhead ? (uint32_t)lane : kc.tail0 + ((uint32_t)lane - kc.nhead);
-            e.key = kp[(uint64_t)rb + i];
-            e.ki = (int)i;
-        }
-        if (vp && (uint32_t)lane < vc.nhead + vc.ntail) {
-            const uint32_t i = (uint32_t)lane < vc.nhead ? (uint32_t)lane : vc.tail0 + ((uint32_t)lane - vc.nhead);
-            e.val = vp[(uint64_t)rb + i];
-            e.vi = (int)i;
-        }
-        return lane == 0;
-    };
-
-    EdgeRows<K> e0, e1;
-    uint32_t ph0 = 0, ph1 = 0;   // parity of each buffer's next phase
-    // in the issuing thread: a buffer's copies are in flight and not yet
-    // waited for, and the parity of the phase they complete
-    bool pend0 = prefetch(std::integral_constant<int, 0>{}, blockIdx.x, e0);
-    uint32_t wpar0 = 0;
-    bool pend1 = prefetch(std::integral_constant<int, 1>{}, blockIdx.x + G, e1);
-    uint32_t wpar1 = 0;
-    __syncthreads();
-
-    // One tile from buffer Q, then the tile 2 * grid further on into Q.
-    // Returns false when the CTA is done (or a wait gave up).
-    auto step = [&](auto qc, uint32_t t) -> bool {
-        constexpr int Q = decltype(qc)::value;
-        EdgeRows<K> &e = Q ? e1 : e0;
-        uint32_t &ph = Q ? ph1 : ph0;
-        bool &pend = Q ? pend1 : pend0;
-        uint32_t &wpar = Q ? wpar1 : wpar0;
-        if (t >= T) return false;
-        const uint4 info = sm.info[Q];
-        const bool skip = (info.z >> 24) & 1u;
-        if (!skip) {
-            const bool ok = __syncthreads_and(mbar_wait(&sm.bar[Q], ph, status));
-            ph ^= 1u;
-            if (!ok) return false;   // the copies stay pending
-            pend = false;
-        }
-        const uint32_t rb = info.x, cnt = info.y;
-        const uint32_t lo = info.z & 0xFFu, width = (info.z >> 8) & 0xFFu, src = (info.z >> 16) & 3u;
-        const K *kp = keys_of(src);
-        const uint32_t *vp = vals_of(src);
-        const uint32_t ksh = kp ? (uint32_t)(((uintptr_t)kp + (uintptr_t)rb * sizeof(K)) & 15) / sizeof(K) : 0u;
-        const uint32_t vsh = vp ? (uint32_t)(((uintptr_t)vp + (uintptr_t)rb * 4u) & 15) / 4u : 0u;
-        if (!skip) {
-            if (warp == 0) {
-                if (e.ki >= 0) sm.keys[Q][ksh + (uint32_t)e.ki] = e.key;
-                if (e.vi >= 0) sm.vals[Q][vsh + (uint32_t)e.vi] = e.val;
-            }
+    for (;;) {
+        if (threadIdx.x == 0) sm.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const uint32_t t = sm.tile;
+        if (t >= T) break;
+        const uint32_t s = find_segment_warp(tile_prefix, nseg, t);
+        const LargeSeg sg = segs[s];
+        if (sg.src & kSkipBit) {
             __syncthreads();
-            const uint32_t wbase = warp * (IT * 32);
-            K key[IT];
-            uint32_t val[IT];
-            uint32_t rd[IT];   // rank in the warp (low 16 bits) | digit << 16
+            continue;
+        }
+        const uint32_t k = t - tile_prefix[s];
+        const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
+        const uint32_t lo = sg.shift - width;
+        const uint64_t tbeg = (uint64_t)sg.start + (uint64_t)k * kTileM;
+        const uint64_t send = (uint64_t)sg.start + sg.len;
+        const uint32_t cnt = (uint32_t)min((uint64_t)kTileM, send - tbeg);
+        // kRankOr's per-warp peer words live in the vals staging area, which
+        // is free until the ranks are known
+        uint32_t *peerw = &sm.vals[warp * kRadix];
+        for (int d = lane; d < kRadix; d += 32) {
+            sm.whist[warp][d] = 0;
+            if constexpr (RANK == kRankOr) peerw[d] = 0;
+        }
+        __syncwarp();
+
+        K key[IT];
+        uint32_t val[IT];
+        uint32_t rd[IT];   // rank in the warp (low 16 bits) | digit << 16
+        const uint32_t wbase = warp * (IT * 32);
+        load_rows<K, IT>(b, sg.src, (uint32_t)tbeg, cnt, IT, wbase, key, val);
+        if (cnt == kTileM && width == (uint32_t)kRadixBits) {
+            // a whole tile and a whole digit (the common case): no lane checks
+#pragma unroll
+            for (int j = 0; j < IT; ++j) {
+                const uint32_t d = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
+                if constexpr (RANK == kRankOr)
+                    rd[j] = wlms_rank_or(d, true, sm.whist[warp], peerw) | (d << 16);
+                else
+                    rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
+            }
+        } else {
 #pragma unroll
             for (int j = 0; j < IT; ++j) {
                 const uint32_t p = wbase + j * 32 + lane;
-                key[j] = K(0);
-                val[j] = 0u;
-                if (p < cnt) {
-                    val[j] = vp ? sm.vals[Q][vsh + p] : rb + p;
-                    if (kp) key[j] = sm.keys[Q][ksh + p];
-                }
-            }
-            if (!kp) {   // through the previous order: gather the bank's keys
-#pragma unroll
-                for (int j = 0; j < IT; ++j)
-                    if (wbase + j * 32 + lane < cnt) key[j] = b.ext_bank[val[j]];
-            }
-            __syncthreads();   // the buffer's rows are in registers: its words are free
-            // kRankOr's per-warp peer words live in this tile's oid buffer
-            uint32_t *const peerw = &sm.vals[Q][warp * kRadix];
-            for (int d = lane; d < kRadix; d += 32) {
-                sm.whist[warp][d] = 0;
-                if constexpr (RANK == kRankOr) peerw[d] = 0;
-            }
-            (void)peerw;
-            __syncwarp();
-            if (cnt == kTileM && width == (uint32_t)kRadixBits) {
-                // a whole tile and a whole digit (the common case): no lane checks
-#pragma unroll
-                for (int j = 0; j < IT; ++j) {
-                    const uint32_t d = (uint32_t)((uint64_t)key[j] >> lo) & (uint32_t)(kRadix - 1);
-                    if constexpr (RANK == kRankOr)
-                        rd[j] = wlms_rank_or(d, true, sm.whist[warp], peerw) | (d << 16);
-                    else
-                        rd[j] = wlms_rank_full<RANK>(d, sm.whist[warp]) | (d << 16);
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < IT; ++j) {
-                    const uint32_t p = wbase + j * 32 + lane;
-                    const uint32_t d = digit_of(key[j], lo, width);
-                    if constexpr (RANK == kRankOr)
-                        rd[j] = wlms_rank_or(d, p < cnt, sm.whist[warp], peerw) | (d << 16);
-                    else
-                        rd[j] = wlms_rank<RANK>(d, p < cnt, sm.whist[warp], width) | (d << 16);
-                }
-            }
-            __syncthreads();
-            // per digit: exclusive over warps, tile total
-            for (int d = threadIdx.x; d < kRadix; d += kNtM) {
-                uint32_t run = 0;
-#pragma unroll
-                for (int w = 0; w < kNtM / 32; ++w) {
-                    const uint32_t c = sm.whist[w][d];
-                    sm.whist[w][d] = run;
-                    run += c;
-                }
-                sm.doff[d] = run;
-            }
-            __syncthreads();
-            uint32_t tot;
-            block_exclusive_scan_radix<kNtM>(sm.doff, sm.tmp, &tot);
-            for (int d = threadIdx.x; d < kRadix; d += kNtM) {
-                const uint32_t dof = sm.doff[d];
-                sm.gdst[Q][d] -= dof;   // wraps; + the row's place in the tile is in range
-#pragma unroll
-                for (int w = 0; w < kNtM / 32; ++w) sm.whist[w][d] += dof;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < IT; ++j) {
-                const uint32_t p = wbase + j * 32 + lane;
-                if (p < cnt) {
-                    const uint32_t pos = sm.whist[warp][rd[j] >> 16] + (rd[j] & 0xFFFFu);
-                    sm.keys[Q][pos] = key[j];
-                    sm.vals[Q][pos] = val[j];
-                }
-            }
-            __syncthreads();
-            K *dk = (src == kSrcBuf1) ? b.k0 : b.k1;
-            uint32_t *dv = (src == kSrcBuf1) ? b.v0 : b.v1;
-            for (uint32_t i = threadIdx.x; i < cnt; i += kNtM) {
-                const K kk = sm.keys[Q][i];
-                const uint32_t o = sm.gdst[Q][digit_of(kk, lo, width)] + i;
-                dk[o] = kk;
-                dv[o] = sm.vals[Q][i];
+                const uint32_t d = digit_of(key[j], lo, width);
+                if constexpr (RANK == kRankOr)
+                    rd[j] = wlms_rank_or(d, p < cnt, sm.whist[warp], peerw) | (d << 16);
+                else
+                    rd[j] = wlms_rank<RANK>(d, p < cnt, sm.whist[warp], width) | (d << 16);
             }
         }
-        __syncthreads();   // every read and write of buffer Q is done
-        if (prefetch(qc, t + 2 * G, e)) {
-            pend = true;
-            wpar = ph;
+        __syncthreads();
+        // per digit: exclusive over warps, tile total
+        for (int d = threadIdx.x; d < kRadix; d += kNtM) {
+            uint32_t run = 0;
+#pragma unroll
+            for (int w = 0; w < kNtM / 32; ++w) {
+                const uint32_t c = sm.whist[w][d];
+                sm.whist[w][d] = run;
+                run += c;
+            }
+            sm.total[d] = run;
+            sm.doff[d] = run;
+            unsigned long long *mine = &lookback[(uint64_t)t * kRadix + d];
+            st_volatile_u64(mine, lb_word(epoch, k == 0 ? kFlagInclusive : kFlagAggregate, run));
         }
-        return true;
-    };
-
-    for (uint32_t t = blockIdx.x;; t += 2 * G) {
-        if (!step(std::integral_constant<int, 0>{}, t)) break;
-        if (!step(std::integral_constant<int, 1>{}, t + G)) break;
+        __syncthreads();
+        uint32_t tot;
+        block_exclusive_scan_radix<kNtM>(sm.doff, sm.tmp, &tot);
+        // decoupled look-back along the segment's tiles
+        for (int d = threadIdx.x; d < kRadix; d += kNtM) {
+            uint32_t excl = 0;
+            if (k > 0) {
+                int64_t p = (int64_t)t - 1;
+                for (;;) {
+                    const unsigned long long w = lb_wait(&lookback[(uint64_t)p * kRadix + d], epoch, status);
+                    excl += (uint32_t)w;
+                    if (((uint32_t)(w >> 32) & 3u) == kFlagInclusive) break;
+                    --p;
+                }
+                st_volatile_u64(&lookback[(uint64_t)t * kRadix + d],
+                                lb_word(epoch, kFlagInclusive, excl + sm.total[d]));
+            }
+            const uint32_t dof = sm.doff[d];
+            sm.gdst[d] = sg.start + offs[(uint64_t)s * kRadix + d] + excl - dof;   // wraps; + slot is in range
+            // the warps' exclusive counts become tile positions
+#pragma unroll
+            for (int w = 0; w < kNtM / 32; ++w) sm.whist[w][d] += dof;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t p = wbase + j * 32 + lane;
+            if (p < cnt) {
+                const uint32_t pos = sm.whist[warp][rd[j] >> 16] + (rd[j] & 0xFFFFu);
+                sm.keys[pos] = key[j];
+                sm.vals[pos] = val[j];
+            }
+        }
+        __syncthreads();
+        K *dk = (sg.src == kSrcBuf1) ? b.k0 : b.k1;
+        uint32_t *dv = (sg.src == kSrcBuf1) ? b.v0 : b.v1;
+        for (uint32_t i = threadIdx.x; i < cnt; i += kNtM) {
+            const K kk = sm.keys[i];
+            const uint32_t o = sm.gdst[digit_of(kk, lo, width)] + i;
+            dk[o] = kk;
+            dv[o] = sm.vals[i];
+        }
+        __syncthreads();
     }
-    // copies still in flight after a wait gave up: wait for them once more
-    // (bounded) before the CTA's shared memory is released
-    if (pend0) mbar_wait(&sm.bar[0], wpar0, status);
-    if (pend1) mbar_wait(&sm.bar[1], wpar1, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -1025,18 +703,11 @@ __global__ void __launch_bounds__(kNtM, scatter_ctas_per_sm(IT)) msd_scatter_ker
 constexpr uint32_t kCountRankMax = 64;
 constexpr uint32_t kBucketMax = 64;
 
-constexpr int pow2_ceil(int x)
-{
-    int p = 1;
-    while (p < x) p <<= 1;
-    return p;
-}
-
 template <typename K, int NT, int IT>
 struct BucketSmem {
     unsigned long long cs[NT * IT];   // compound keys, bucketed
     uint32_t vals[NT * IT];
-    uint32_t off[pow2_ceil(NT * IT) + 1];   // per bucket: count -> start (up to 2^ceil(log2 len) buckets)
+    uint32_t off[NT * IT + 1];        // per bucket: count -> start
     uint16_t orig[NT * IT];           // position in the segment, when the compound key has no room for it
     uint32_t tmp[NT / 32 + 1];
     unsigned long long any, all;      // OR and AND of the segment's keys
@@ -1466,7 +1137,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
 block_sort_kernel(Bufs<K> b, const uint2 *list, const uint32_t *d_count)
 {
     kernel_prologue();
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NW = NT / 32;
     const uint32_t count = *d_count;
     const int warp = threadIdx.x >> 5;
@@ -1709,44 +1380,6 @@ int set_smem(fmcs_ctx *ctx, F *f, size_t bytes)
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what);          \
     } while (0)
 
-}  // namespace
-
-// Rows of an HBM radix tile, the largest segment an on-chip tier takes, and
-// the most tiles one level of a sort of n rows can have (every large segment
-// adds at most one partial tile).
-uint32_t sort_tile_rows(const fmcs_ctx *ctx) { return (uint32_t)kNtM * (ctx->msd_items >= 16 ? 16u : 8u); }
-
-static uint32_t sort_local_max(const fmcs_ctx *ctx)
-{
-    return std::max<uint32_t>(kCapA, std::min<uint32_t>(ctx->local_max, kCapLocal));
-}
-
-uint64_t sort_level_tiles(const fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows)
-{
-    const uint64_t cap_large = n / (sort_local_max(ctx) + 1) + 2;
-    return n / tile_rows + cap_large + 1;
-}
-
-// The per-tile arrays of the HBM radix levels, in their workspace slots: the
-// counts (which the stitch may fill for level 0 before the sort starts), and
-// the destinations and descriptors.
-int level_tile_arrays(fmcs_ctx *ctx, uint64_t n, uint32_t tile_rows, uint16_t **tcnt, uint32_t **tdst, uint4 **tinfo)
-{
-    const uint64_t tiles = sort_level_tiles(ctx, n, tile_rows);
-    void *p;
-    int rc;
-    if ((rc = ws_get(ctx, kSlotTileCnt, tiles * kRadix * sizeof(uint16_t), &p))) return rc;
-    *tcnt = (uint16_t *)p;
-    if ((rc = ws_get(ctx, kSlotTileDst, carve_total({tiles * kRadix * sizeof(uint32_t), tiles * sizeof(uint4)}), &p)))
-        return rc;
-    Carver cv(p);
-    *tdst = cv.take<uint32_t>(tiles * kRadix);
-    *tinfo = cv.take<uint4>(tiles);
-    return FMCS_OK;
-}
-
-namespace {
-
 template <typename K, int RANK, int IT>
 int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
 {
@@ -1771,7 +1404,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     b.v1 = (uint32_t *)p;
 
     // lists (capacities are bounds on disjoint segments of each tier's minimum size)
-    const uint32_t local_max = sort_local_max(ctx);
+    const uint32_t local_max = std::max<uint32_t>(kCapA, std::min<uint32_t>(ctx->local_max, kCapLocal));
     const uint32_t tile_rows = kNtM * IT;
     const uint64_t cap_large = n / (local_max + 1) + 2;
     const uint64_t cap_t = n / 2 + 2, cap_t32 = n / (kCapT + 1) + 2, cap_a = n / (kCapT + 1) + 2;
@@ -1822,10 +1455,10 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     }
     if ((rc = ws_get(ctx, kSlotTilePrefix, (cap_large + 1) * sizeof(uint32_t), &p))) return rc;
     tile_prefix = (uint32_t *)p;
-    uint16_t *tcnt;
-    uint32_t *tdst;
-    uint4 *tinfo;
-    if ((rc = level_tile_arrays(ctx, n, tile_rows, &tcnt, &tdst, &tinfo))) return rc;
+    const uint64_t max_tiles = n / tile_rows + cap_large + 1;
+    unsigned long long *lookback;
+    if ((rc = ws_get(ctx, kSlotLookback, max_tiles * kRadix * sizeof(unsigned long long), &p, true))) return rc;
+    lookback = (unsigned long long *)p;
     uint32_t *ctr;
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     ctr = (uint32_t *)p + 64;   // words 0..63 belong to other kernels
@@ -1868,7 +1501,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     }
     // MSD levels
     const int levels = (int)((a.key_bits + kRadixBits - 1) / kRadixBits);
-    const size_t msd_smem = sizeof(ScatterSmem<K, IT>);
+    const size_t msd_smem = sizeof(MsdSmem<K, IT>);
     if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK, IT>, msd_smem))) return rc;
     if (n > (uint64_t)local_max) {
         // Host-known count of the level's large segments (exact unless the
@@ -1884,10 +1517,12 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             tiers_known = true;
         }
         const int hist0_ready = (a.top_hist && !a.seg_start) ? 1 : 0;
-        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready, tcnt, tdst, tinfo};
-        const unsigned scatter_grid = sms * scatter_ctas_per_sm(IT);
+        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready};
+        const uint32_t epoch_base = ctx->epoch;
+        ctx->epoch += (uint32_t)levels;
+        const unsigned scatter_grid = sms * msd_ctas_per_sm(IT);
         int host_lvl = 0;   // the level being launched, for the eager read-back
-        // one level: the same five launches for every level (the level index
+        // one level: the same four launches for every level (the level index
         // lives on the device)
         auto level = [&](cudaStream_t s, cudaGraphConditionalHandle more, bool read_back) -> int {
             { LaunchScope ls_(ctx, "tile_prefix");
@@ -1901,9 +1536,6 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             { LaunchScope ls_(ctx, "msd_plan");
                 launch_k(msd_plan_kernel, sms * 8, kRadix, 0, s, lr, lists, true);
             }
-            { LaunchScope ls_(ctx, "tile_scan");
-                launch_k(tile_scan_kernel, kRadix / kScanDigits, kScanThreads, 0, s, lr, tile_prefix, tile_rows);
-            }
             if (read_back) {
                 // read the counters (the next level's count, the rows moved,
                 // the tiers' list sizes) while the scatter runs
@@ -1912,8 +1544,9 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             }
             {
                 LaunchScope ls_(ctx, "msd_scatter");
-                launch_k(msd_scatter_kernel<K, RANK, IT>, scatter_grid, kNtM, msd_smem, s, b, lr, tile_prefix,
-                         ctx->d_status, more, (uint32_t)levels);
+                launch_k(msd_scatter_kernel<K, RANK, IT>, scatter_grid, kNtM, msd_smem, s, b, lr, tile_prefix, lookback,
+                                                                                   epoch_base, ctx->d_status, more,
+                                                                                   (uint32_t)levels);
                 if (read_back) {
                     cudaError_t e = cudaEventSynchronize(ctx->ev_level);
                     if (e != cudaSuccess) return cuda_fail(ctx, e, "sort: level event");
@@ -2089,19 +1722,19 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
     if ((rc = ws_get(ctx, kSlotTilePrefix, 4 * sizeof(uint32_t), &p))) return rc;
     tile_prefix = (uint32_t *)p;
     const uint32_t tile_rows = kNtM * IT;
-    uint16_t *tcnt;
-    uint32_t *tdst;
-    uint4 *tinfo;
-    if ((rc = level_tile_arrays(ctx, n, tile_rows, &tcnt, &tdst, &tinfo))) return rc;
+    const uint64_t max_tiles = n / tile_rows + 2;
+    unsigned long long *lookback;
+    if ((rc = ws_get(ctx, kSlotLookback, max_tiles * kRadix * sizeof(unsigned long long), &p, true))) return rc;
+    lookback = (unsigned long long *)p;
     uint32_t *ctr;
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     ctr = (uint32_t *)p + 64;
-    const size_t msd_smem = sizeof(ScatterSmem<K, IT>);
+    const size_t msd_smem = sizeof(MsdSmem<K, IT>);
     if ((rc = set_smem(ctx, msd_scatter_kernel<K, RANK, IT>, msd_smem))) return rc;
     const int sms = ctx->num_sms;
     Lists none{};
     // one segment [0, n), re-set before every pass; level buffers of set 0
-    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0, 0, tcnt, tdst, tinfo};
+    const LevelRefs lr{{seg, seg + 1}, {hist, hist + kRadix}, ctr, 0, 0};
     int pass = 0;
     for (uint32_t lo = 0; lo < bits; lo += kRadixBits, ++pass) {
         const uint32_t shift = std::min(bits, lo + kRadixBits);
@@ -2117,12 +1750,9 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
         { LaunchScope ls_(ctx, "msd_plan");
             launch_k(msd_plan_kernel, 1, kRadix, 0, st, lr, none, false);
         }
-        { LaunchScope ls_(ctx, "tile_scan");
-            launch_k(tile_scan_kernel, kRadix / kScanDigits, kScanThreads, 0, st, lr, tile_prefix, tile_rows);
-        }
         { LaunchScope ls_(ctx, "msd_scatter");
-            launch_k(msd_scatter_kernel<K, RANK, IT>, sms * scatter_ctas_per_sm(IT), kNtM, msd_smem, st, b, lr,
-                     tile_prefix, ctx->d_status, 0, 1u);
+            launch_k(msd_scatter_kernel<K, RANK, IT>, sms * msd_ctas_per_sm(IT), kNtM, msd_smem, st, 
+                b, lr, tile_prefix, lookback, ctx->epoch++, ctx->d_status, 0, 1u);
         }
         FMCS_LAUNCH_CHECK("lsd pass");
     }

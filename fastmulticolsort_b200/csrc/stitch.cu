@@ -91,83 +91,6 @@ __device__ __forceinline__ void store4(B *bank, uint64_t row, bool vec, uint64_t
         if (row + k < n) bank[row + k] = (B)a[k];
 }
 
-// Every slice of one group of 4 rows (or two groups, a stride apart, whose
-// loads are then in flight together) folded into the bank values.
-__device__ __forceinline__ void fold_groups(const StitchParams &p, uint64_t row0, uint64_t row1, bool two, bool vec0,
-                                            bool vec1, uint64_t n, uint64_t (&acc0)[4], uint64_t (&acc1)[4])
-{
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc0[k] = acc1[k] = 0;
-    for (int s = 0; s < p.ns; ++s) {
-        const StitchSlice sl = p.s[s];
-        uint64_t v0[4], v1[4] = {0, 0, 0, 0};
-        load4(sl.src, sl.src_bytes, row0, vec0, n, v0);
-        if (two) load4(sl.src, sl.src_bytes, row1, vec1, n, v1);
-        const uint64_t mask = sl.width >= 64 ? ~0ull : ((1ull << sl.width) - 1);
-        const uint64_t flip = sl.invert ? mask : 0ull;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint64_t x0 = ((v0[k] >> sl.rshift) & mask) ^ flip;
-            const uint64_t x1 = ((v1[k] >> sl.rshift) & mask) ^ flip;
-            acc0[k] = (s == 0 || sl.width >= 64) ? x0 : ((acc0[k] << sl.width) | x0);
-            acc1[k] = (s == 0 || sl.width >= 64) ? x1 : ((acc1[k] << sl.width) | x1);
-        }
-    }
-}
-
-// The stitch of a round-0 sort bank, by tiles of the first radix level
-// (tile_rows = 2048 or 4096): besides the bank it writes every tile's
-// top-digit counts (tile_cnt, 256 u16 per tile) and adds the CTA's totals to
-// top_hist once at its end.  512 threads take a tile's groups of 4 rows, one
-// or two each (the loads of both in flight together); CTAs of 512 threads
-// hold a tile at a time, so the tiles spread over the resident CTAs in many
-// rounds and the last, partial round is short.
-constexpr int kStitchTileThreads = 512;
-
-template <typename B>
-__global__ void __launch_bounds__(kStitchTileThreads) stitch_tiles_kernel(const __grid_constant__ StitchParams p,
-                                                                         B *bank, uint64_t n, bool aligned,
-                                                                         uint32_t *top_hist, uint16_t *tile_cnt,
-                                                                         uint32_t tile_rows, uint32_t hist_lo,
-                                                                         uint32_t hist_mask)
-{
-    kernel_prologue();
-    __shared__ uint32_t sh[256];
-    const uint32_t d = threadIdx.x;
-    if (d < 256) sh[d] = 0;
-    uint32_t total = 0;
-    __syncthreads();
-    const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
-    const bool two_groups = tile_rows == 8 * kStitchTileThreads;   // 4096-row tiles
-    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint64_t row0 = t * tile_rows + (uint64_t)d * 4;
-        const uint64_t row1 = row0 + (uint64_t)kStitchTileThreads * 4;
-        if (row0 < n) {
-            const bool two = two_groups && row1 < n;
-            const bool vec0 = aligned && row0 + 4 <= n;
-            const bool vec1 = aligned && row1 + 4 <= n;
-            uint64_t acc0[4], acc1[4];
-            fold_groups(p, row0, row1, two, vec0, vec1, n, acc0, acc1);
-            store4<B>(bank, row0, vec0, n, acc0);
-            if (two) store4<B>(bank, row1, vec1, n, acc1);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (row0 + k < n) atomicAdd(&sh[(uint32_t)(acc0[k] >> hist_lo) & hist_mask], 1u);
-                if (two && row1 + k < n) atomicAdd(&sh[(uint32_t)(acc1[k] >> hist_lo) & hist_mask], 1u);
-            }
-        }
-        __syncthreads();
-        if (d < 256) {
-            const uint32_t c = sh[d];
-            sh[d] = 0;
-            tile_cnt[t * 256 + d] = (uint16_t)c;
-            total += c;
-        }
-        __syncthreads();
-    }
-    if (d < 256 && total) atomicAdd(&top_hist[d], total);
-}
-
 template <typename B>
 __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ StitchParams p, B *bank,
                                                      uint64_t n, bool aligned, uint32_t *top_hist,
@@ -268,7 +191,7 @@ int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t 
 }
 
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist, uint32_t key_bits, uint16_t *tile_cnt, uint32_t tile_rows)
+                  uint64_t n, uint32_t *top_hist, uint32_t key_bits)
 {
     if (ns < 1 || ns > kMaxSlices) return set_error(ctx, FMCS_E_INVAL, "stitch: 1..32 slices");
     if (!(bank_bytes == 1 || bank_bytes == 2 || bank_bytes == 4 || bank_bytes == 8))
@@ -295,28 +218,6 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
     const unsigned grid = (unsigned)blocks;
     cudaStream_t st = ctx->stream;
     LaunchScope ls_(ctx, "stitch");
-    if (top_hist && tile_cnt) {
-        if (tile_rows != 2048 && tile_rows != 4096) return set_error(ctx, FMCS_E_INVAL, "stitch: tile rows");
-        const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
-        const unsigned tgrid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctx->num_sms * (2048 / kStitchTileThreads));
-        switch (bank_bytes) {
-        case 2:
-            launch_k(stitch_tiles_kernel<uint16_t>, tgrid, kStitchTileThreads, 0, st, p, (uint16_t *)bank, n, aligned, top_hist,
-                     tile_cnt, tile_rows, hist_lo, hist_mask);
-            break;
-        case 4:
-            launch_k(stitch_tiles_kernel<uint32_t>, tgrid, kStitchTileThreads, 0, st, p, (uint32_t *)bank, n, aligned, top_hist,
-                     tile_cnt, tile_rows, hist_lo, hist_mask);
-            break;
-        case 8:
-            launch_k(stitch_tiles_kernel<uint64_t>, tgrid, kStitchTileThreads, 0, st, p, (uint64_t *)bank, n, aligned, top_hist,
-                     tile_cnt, tile_rows, hist_lo, hist_mask);
-            break;
-        default: return set_error(ctx, FMCS_E_INVAL, "stitch: a sort bank has 2, 4 or 8 bytes");
-        }
-        cudaError_t e = cudaGetLastError();
-        return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "stitch launch");
-    }
     switch (bank_bytes) {
     case 1:
         launch_k(stitch_kernel<uint8_t>, grid, 256, 0, st,
