@@ -561,12 +561,16 @@ def run_serving(args):
 def run_batch_workloads(args):
     """Many independent instances and the wide table: one JSON line of their own."""
     from fastmulticolsort_b200 import batch_bench
-    res = batch_bench.benchmark(reps=max(1, min(args.steps, 5)))
-    inst = res["instances"]
-    line = {"metric": METRIC, "workload": "batch", "value": inst["batched_mrows_s"], "unit": "M rows/s",
+    res = batch_bench.benchmark(reps=max(1, min(args.steps, 5)), with_instances=not args.no_instances,
+                                wide_rows=args.wide_rows)
+    inst = res.get("instances")
+    wd = res["wide"]
+    line = {"metric": METRIC, "workload": "batch",
+            "value": inst["batched_mrows_s"] if inst else wd["order_by_mrows_s"], "unit": "M rows/s",
             "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded; generated on the device)",
-            "config": {"workload": f"{inst['instances']} instances, {inst['rows']:,} rows in all (8/24/40-bit "
-                                   "columns), one fmcs_run_batch call; plus a 60M-row 6-column wide table"},
+            "config": {"workload": (f"{inst['instances']} instances, {inst['rows']:,} rows in all (8/24/40-bit "
+                                    "columns), one fmcs_run_batch call; plus " if inst else "")
+                       + f"a {args.wide_rows:,}-row 6-column wide table"},
             **res}
     print(json.dumps(line), flush=True)
     return 0
@@ -583,6 +587,8 @@ def main():
     ap.add_argument("--no-zipf", action="store_true", help="skip the Zipf segmented comparison")
     ap.add_argument("--zipf-rows", type=int, default=67_108_864)
     ap.add_argument("--workload", default="massaged", choices=["massaged", "serving", "batch"])
+    ap.add_argument("--no-instances", action="store_true", help="batch workload: the wide table only")
+    ap.add_argument("--wide-rows", type=int, default=60_000_000, help="batch workload: rows of the wide table")
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--duration", type=float, default=5.0)
     ap.add_argument("--only-steps", action="store_true",

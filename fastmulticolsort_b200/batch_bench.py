@@ -97,18 +97,18 @@ def instance_workload(torch, count=INSTANCE_COUNT):
     return cols, sizes, bw, split, est
 
 
-def wide_workload(torch):
-    """The wide table on the device: (cols, card, ORDER BY split, GROUP BY
-    (split, column order))."""
+def wide_workload(torch, n=WIDE_ROWS):
+    """The wide table on the device (n rows, 60,000,000 by default): (cols,
+    card, ORDER BY split, GROUP BY (split, column order)).  The plans are the
+    cost model's for the 60,000,000-row table."""
     rng = W.rng_for(4, salt=1)
-    n = WIDE_ROWS
     cols = []
     for w, k in zip(WIDE_BITS, WIDE_CARD):
         cols.append(_uniform_column(torch, rng, n, w) if k >= (1 << w) else _pool_column(torch, rng, n, w, k))
     col_bytes = [c.element_size() for c in cols]
-    card = [min(k, n) for k in WIDE_CARD]
-    split, _, _ = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=True)
-    gsplit, gorder, _ = capi.optimize_plan(WIDE_BITS, card, col_bytes, n, ordered=False)
+    card = [min(k, WIDE_ROWS) for k in WIDE_CARD]
+    split, _, _ = capi.optimize_plan(WIDE_BITS, card, col_bytes, WIDE_ROWS, ordered=True)
+    gsplit, gorder, _ = capi.optimize_plan(WIDE_BITS, card, col_bytes, WIDE_ROWS, ordered=False)
     return cols, card, split, (gsplit, gorder)
 
 
@@ -202,9 +202,8 @@ def instances(torch, ctx, stream, reps=3, plain=True):
     return out
 
 
-def wide(torch, ctx, stream, reps=3):
-    n = WIDE_ROWS
-    cols, card, split, (gsplit, gorder) = wide_workload(torch)
+def wide(torch, ctx, stream, reps=3, n=WIDE_ROWS):
+    cols, card, split, (gsplit, gorder) = wide_workload(torch, n)
     order = torch.empty(n, dtype=torch.int32, device="cuda")
     group = torch.empty(n, dtype=torch.int32, device="cuda")
     g2 = torch.empty_like(group)
@@ -310,10 +309,12 @@ def same_grouping(torch, sort_res, hash_res, n):
     return bool(na == nb == pairs)
 
 
-def benchmark(reps=3, plain=True):
+def benchmark(reps=3, plain=True, with_instances=True, wide_rows=WIDE_ROWS):
     import torch
+    out = {}
     with capi.Context(0) as ctx:
         stream = torch.cuda.ExternalStream(ctx.stream)
-        inst = instances(torch, ctx, stream, reps=reps, plain=plain)
-        wd = wide(torch, ctx, stream, reps=reps)
-    return {"instances": inst, "wide": wd}
+        if with_instances:
+            out["instances"] = instances(torch, ctx, stream, reps=reps, plain=plain)
+        out["wide"] = wide(torch, ctx, stream, reps=reps, n=wide_rows)
+    return out

@@ -52,6 +52,7 @@ constexpr int kItemsA = 4;
 constexpr int kNtB1 = 128, kItB1 = 4, kCapB1 = kNtB1 * kItB1;   // 512
 constexpr int kNtB2 = 128, kItB2 = 8, kCapB2 = kNtB2 * kItB2;   // 1024
 constexpr int kNtC1 = 256, kItC1 = 8, kCapC1 = kNtC1 * kItC1;   // 2048
+constexpr int kNtC1b = 256, kItC1b = 9, kCapC1b = kNtC1b * kItC1b;   // 2304
 constexpr int kNtC2 = 512, kItC2 = 8, kCapC2 = kNtC2 * kItC2;   // 4096
 constexpr int kNtC3 = 1024, kItC3 = 8, kCapC3 = kNtC3 * kItC3;  // 8192
 constexpr int kCapLocal = kCapC3;   // largest segment a local tier can take; larger: MSD levels
@@ -76,6 +77,7 @@ constexpr int kCtrCopyTile = 13;
 constexpr uint32_t kCopySplit = 4096;
 constexpr int kCtrLevel = 15;      // MSD levels started so far (device-side level index)
 constexpr int kCtrLocalC3 = 16;
+constexpr int kCtrLocalC1b = 17;
 constexpr int kCtrWords = 32;
 
 struct LargeSeg {
@@ -186,7 +188,7 @@ __device__ __forceinline__ uint2 pack_local(uint32_t start, uint32_t len, uint32
 }
 
 struct Lists {
-    uint2 *t, *t32, *a, *b1, *b2, *c1, *c2, *c3;
+    uint2 *t, *t32, *a, *b1, *b2, *c1, *c1b, *c2, *c3;
     uint32_t cap_t32;      // kCapT32 for keys of <= 4 bytes, else 0 (17..32 rows go to the warp tier)
     LargeSeg *copy;        // segments that only need to reach BUF0, <= kCopySplit rows (warp each)
     LargeSeg *copy_large;  // the same, larger: copied by tiles across the grid
@@ -235,6 +237,8 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
         which = kCtrLocalB2;
     } else if (len <= (uint32_t)kCapC1) {
         which = kCtrLocalC1;
+    } else if (len <= (uint32_t)kCapC1b) {
+        which = kCtrLocalC1b;
     } else if (len <= (uint32_t)kCapC2) {
         which = kCtrLocalC2;
     } else if (len <= (uint32_t)kCapC3) {
@@ -253,6 +257,7 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
     case kCtrLocalB1: L.b1[slot] = e; break;
     case kCtrLocalB2: L.b2[slot] = e; break;
     case kCtrLocalC1: L.c1[slot] = e; break;
+    case kCtrLocalC1b: L.c1b[slot] = e; break;
     case kCtrLocalC2: L.c2[slot] = e; break;
     case kCtrLocalC3: L.c3[slot] = e; break;
     default: {
@@ -703,11 +708,18 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
 constexpr uint32_t kCountRankMax = 64;
 constexpr uint32_t kBucketMax = 64;
 
+constexpr int pow2_ceil(int x)
+{
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
 template <typename K, int NT, int IT>
 struct BucketSmem {
     unsigned long long cs[NT * IT];   // compound keys, bucketed
     uint32_t vals[NT * IT];
-    uint32_t off[NT * IT + 1];        // per bucket: count -> start
+    uint32_t off[pow2_ceil(NT * IT) + 1];   // per bucket: count -> start (up to 2^ceil(log2 len) buckets)
     uint16_t orig[NT * IT];           // position in the segment, when the compound key has no room for it
     uint32_t tmp[NT / 32 + 1];
     unsigned long long any, all;      // OR and AND of the segment's keys
@@ -1410,7 +1422,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const uint64_t cap_t = n / 2 + 2, cap_t32 = n / (kCapT + 1) + 2, cap_a = n / (kCapT + 1) + 2;
     const uint64_t cap_b1 = n / (kCapA + 1) + 2;
     const uint64_t cap_b2 = n / (kCapB1 + 1) + 2;
-    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c2 = n / (kCapC1 + 1) + 2, cap_c3 = n / (kCapC2 + 1) + 2;
+    const uint64_t cap_c1 = n / (kCapB2 + 1) + 2, cap_c1b = n / (kCapC1 + 1) + 2, cap_c2 = n / (kCapC1b + 1) + 2;
+    const uint64_t cap_c3 = n / (kCapC2 + 1) + 2;
     // copy entries: disjoint ranges; at most 256 children per large segment per
     // level, so bounded by both n and (levels + 1) * 256 * cap_large
     const uint64_t levels_max = (a.key_bits + kRadixBits - 1) / kRadixBits;
@@ -1425,7 +1438,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         const size_t e = sizeof(uint2);
         if ((rc = ws_get(ctx, kSlotLocalA,
                          carve_total({cap_t * e, cap_t32 * e, cap_a * e, cap_b1 * e, cap_b2 * e, cap_c1 * e,
-                                      cap_c2 * e, cap_c3 * e}),
+                                      cap_c1b * e, cap_c2 * e, cap_c3 * e}),
                          &p)))
             return rc;
         Carver cv(p);
@@ -1436,6 +1449,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         lists.b1 = cv.take<uint2>(cap_b1);
         lists.b2 = cv.take<uint2>(cap_b2);
         lists.c1 = cv.take<uint2>(cap_c1);
+        lists.c1b = cv.take<uint2>(cap_c1b);
         lists.c2 = cv.take<uint2>(cap_c2);
         lists.c3 = cv.take<uint2>(cap_c3);
         if ((rc = ws_get(ctx, kSlotLocalC, carve_total({cap_copy * sizeof(LargeSeg), cap_large * sizeof(LargeSeg)}),
@@ -1494,6 +1508,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                               : len <= (uint32_t)kCapB1 ? kCtrLocalB1
                               : len <= (uint32_t)kCapB2 ? kCtrLocalB2
                               : len <= (uint32_t)kCapC1 ? kCtrLocalC1
+                              : len <= (uint32_t)kCapC1b ? kCtrLocalC1b
                               : len <= (uint32_t)kCapC2 ? kCtrLocalC2 : kCtrLocalC3;
             w[which] = 1;
         }
@@ -1586,11 +1601,13 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
     const size_t smem_b1 = std::max(sizeof(BlockSmem<K, kNtB1, kItB1>), sizeof(BucketSmem<K, kNtB1, kItB1>));
     const size_t smem_b2 = std::max(sizeof(BlockSmem<K, kNtB2, kItB2>), sizeof(BucketSmem<K, kNtB2, kItB2>));
     const size_t smem_c1 = std::max(sizeof(BlockSmem<K, kNtC1, kItC1>), sizeof(BucketSmem<K, kNtC1, kItC1>));
+    const size_t smem_c1b = std::max(sizeof(BlockSmem<K, kNtC1b, kItC1b>), sizeof(BucketSmem<K, kNtC1b, kItC1b>));
     const size_t smem_c2 = std::max(sizeof(BlockSmem<K, kNtC2, kItC2>), sizeof(BucketSmem<K, kNtC2, kItC2>));
     const size_t smem_c3 = std::max(sizeof(BlockSmem<K, kNtC3, kItC3>), sizeof(BucketSmem<K, kNtC3, kItC3>));
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB1, kItB1, RANK>, smem_b1))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtB2, kItB2, RANK>, smem_b2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1, kItC1, RANK>, smem_c1))) return rc;
+    if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC1b, kItC1b, RANK>, smem_c1b))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC2, kItC2, RANK>, smem_c2))) return rc;
     if ((rc = set_smem(ctx, block_sort_kernel<K, kNtC3, kItC3, RANK>, smem_c3))) return rc;
     // Each tier's launch, with the counter word of its list.  An eager call
@@ -1631,6 +1648,11 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         LaunchScope ls_(ctx, "block_sort_2048");
         launch_k(block_sort_kernel<K, kNtC1, kItC1, RANK>, sms * (1024 / kNtC1), kNtC1, smem_c1, s, b, lists.c1,
                  &ctr[kCtrLocalC1]);
+    }});
+    tiers.push_back({kCtrLocalC1b, [&](cudaStream_t s) {
+        LaunchScope ls_(ctx, "block_sort_2304");
+        launch_k(block_sort_kernel<K, kNtC1b, kItC1b, RANK>, sms * (1024 / kNtC1b), kNtC1b, smem_c1b, s, b, lists.c1b,
+                 &ctr[kCtrLocalC1b]);
     }});
     tiers.push_back({kCtrLocalC2, [&](cudaStream_t s) {
         LaunchScope ls_(ctx, "block_sort_4096");
