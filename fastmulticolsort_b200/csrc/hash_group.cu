@@ -112,40 +112,73 @@ __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ 
 // and first flag are written already.
 constexpr uint32_t kDoneOnChip = 0xFFFFFFFEu;
 
-// Parent runs of up to kRunOnChip rows are numbered by one CTA each in shared
-// memory (the reference's block-local tables, Hashing::calculate_hash_in_block,
-// src/hashing.h:178-287): the run's keys are staged in shared memory, every
-// row claims or finds its key's slot of an open-addressing table of positions
-// (at least twice as many slots as rows) and lowers the slot to its own
-// position with a shared atomicMin, so a slot ends at its key's first
-// appearance in the run.  Longer runs go through the global table.
+// Parent runs of up to kRunOnChip rows are numbered on chip (the reference's
+// block-local tables, Hashing::calculate_hash_in_block, src/hashing.h:178-287),
+// longer runs in the global table.  A classification pass (one thread per run)
+// settles one-row runs at once and queues the others by size: runs of up to
+// 32 rows are numbered by one warp each (match.any on the key: a lane's first
+// appearance is the lowest lane holding its key), runs of 33 to kRunOnChip rows
+// by one CTA each: the run's keys are staged in shared memory, every row claims
+// or finds its key's slot of an open-addressing table of positions (at least
+// twice as many slots as rows) and lowers the slot to its own position with a
+// shared atomicMin, so a slot ends at its key's first appearance in the run.
 constexpr uint32_t kRunOnChip = 2048;
 constexpr uint32_t kRunOnChipSlots = 2 * kRunOnChip;
+constexpr uint32_t kRunWarp = 32;
+
+__global__ void hash_runs_classify_kernel(const uint32_t *__restrict__ seg_start, const uint32_t *d_nseg,
+                                          uint32_t *slot_of, uint32_t *fpos, uint8_t *first, uint32_t *warp_runs,
+                                          uint32_t *cta_runs, uint32_t *counts)
+{
+    kernel_prologue();
+    const uint32_t nseg = *d_nseg;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // every lane of a warp takes the same number of steps (the queue appends
+    // below are warp-wide)
+    const uint32_t steps = (nseg + stride - 1) / stride;
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t k = 0; k < steps; ++k, s += stride) {
+        uint32_t start = 0, len = 0;
+        if (s < nseg) {
+            start = seg_start[s];
+            len = seg_start[s + 1] - start;
+        }
+        if (len == 1) {
+            fpos[start] = start;
+            first[start] = 1;
+            slot_of[start] = kDoneOnChip;
+        }
+        const int which = (len >= 2 && len <= kRunWarp) ? 0 : (len > kRunWarp && len <= kRunOnChip) ? 1 : 2;
+        const uint32_t lane = threadIdx.x & 31;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, which);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (which < 2 && lane == leader) base = atomicAdd(&counts[which], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        const uint32_t slot = base + __popc(peers & lanemask_lt());
+        if (which == 0) warp_runs[slot] = s;
+        else if (which == 1) cta_runs[slot] = s;
+    }
+}
 
 template <typename K>
 __global__ void __launch_bounds__(256) hash_runs_onchip_kernel(const K *__restrict__ bank,
                                                                const uint32_t *__restrict__ order,
                                                                const uint32_t *__restrict__ seg_start,
-                                                               const uint32_t *d_nseg, uint32_t *slot_of,
+                                                               const uint32_t *warp_runs, const uint32_t *cta_runs,
+                                                               const uint32_t *counts, uint32_t *slot_of,
                                                                uint32_t *fpos, uint8_t *first)
 {
     kernel_prologue();
     __shared__ K keys[kRunOnChip];
     __shared__ uint32_t table[kRunOnChipSlots];
     __shared__ uint16_t slot_at[kRunOnChip];
-    const uint32_t nseg = *d_nseg;
-    for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
-        const uint32_t start = seg_start[s];
-        const uint32_t len = seg_start[s + 1] - start;
-        if (len > kRunOnChip) continue;   // the same for the whole block
-        if (len == 1) {
-            if (threadIdx.x == 0) {
-                fpos[start] = start;
-                first[start] = 1;
-                slot_of[start] = kDoneOnChip;
-            }
-            continue;
-        }
+    // runs of 33..kRunOnChip rows: one CTA each
+    const uint32_t ncta = counts[1];
+    for (uint32_t q = blockIdx.x; q < ncta; q += gridDim.x) {
+        const uint32_t sidx = cta_runs[q];
+        const uint32_t start = seg_start[sidx];
+        const uint32_t len = seg_start[sidx + 1] - start;
         uint32_t ts = 64;
         while (ts < 2 * len) ts <<= 1;
         for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0xFFFFFFFFu;
@@ -178,6 +211,25 @@ __global__ void __launch_bounds__(256) hash_runs_onchip_kernel(const K *__restri
             slot_of[start + p] = kDoneOnChip;
         }
         __syncthreads();
+    }
+    // runs of 2..32 rows: one warp each, lane i holding row i
+    const uint32_t nwarp = counts[0];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x / 32;
+    for (uint32_t q = blockIdx.x * wpb + (threadIdx.x >> 5); q < nwarp; q += gridDim.x * wpb) {
+        const uint32_t sidx = warp_runs[q];
+        const uint32_t start = seg_start[sidx];
+        const uint32_t len = seg_start[sidx + 1] - start;
+        const bool mine = lane < len;
+        const uint32_t valid = __ballot_sync(0xFFFFFFFFu, mine);
+        if (mine) {
+            const K k = order ? bank[order[start + lane]] : bank[start + lane];
+            const uint32_t peers = __match_any_sync(valid, (unsigned long long)k);
+            const uint32_t f = __ffs(peers) - 1;
+            fpos[start + lane] = start + f;
+            first[start + lane] = f == lane ? 1 : 0;
+            slot_of[start + lane] = kDoneOnChip;
+        }
     }
 }
 
@@ -227,13 +279,21 @@ __global__ void assign_ids_kernel(const uint32_t *__restrict__ fpos, const uint3
 template <typename K>
 int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const uint32_t *run, bool runs_contiguous,
                 const uint32_t *seg_start, const uint32_t *d_nseg, uint64_t n, unsigned long long *slots,
-                uint64_t mask, uint32_t *slot_of, uint32_t *fpos, uint8_t *first)
+                uint64_t mask, uint32_t *slot_of, uint32_t *fpos, uint8_t *first, uint32_t *warp_runs,
+                uint32_t *cta_runs, uint32_t *counts)
 {
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     if (seg_start) {
+        cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), ctx->stream);
+        {
+            LaunchScope ls_(ctx, "hash_runs_classify");
+            launch_k(hash_runs_classify_kernel, grid, 256, 0, ctx->stream, seg_start, d_nseg, slot_of, fpos, first,
+                     warp_runs, cta_runs, counts);
+        }
         LaunchScope ls_(ctx, "hash_runs_onchip");
-        launch_k(hash_runs_onchip_kernel<K>, grid, 256, 0, ctx->stream, (const K *)bank, order, seg_start, d_nseg,
-                 slot_of, fpos, first);
+        launch_k(hash_runs_onchip_kernel<K>, grid, 256, 0, ctx->stream, (const K *)bank, order, seg_start,
+                 (const uint32_t *)warp_runs, (const uint32_t *)cta_runs, (const uint32_t *)counts, slot_of, fpos,
+                 first);
     }
     { LaunchScope ls_(ctx, "hash_insert");
         launch_k(hash_insert_kernel<K>, grid, 256, 0, ctx->stream, (const K *)bank, order, run, runs_contiguous,
@@ -260,12 +320,22 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     unsigned long long *slots = (unsigned long long *)p;
     cudaMemsetAsync(slots, 0xFF, cap * sizeof(unsigned long long), st);
     // per-row scratch: slot_of / rank (n), fpos (n), run ids (n), first flags (n bytes)
-    if ((rc = ws_get(ctx, kSlotHashIdx, 3 * carve_round(n * sizeof(uint32_t)) + carve_round(n), &p))) return rc;
+    // per-row scratch: slot_of / rank, fpos, run ids, first flags; and the
+    // queues of parent runs numbered on chip (a warp each: at most n / 2 runs
+    // of 2..32 rows; a CTA each: at most n / 33)
+    const uint64_t nq_warp = n / 2 + 1, nq_cta = n / (kRunWarp + 1) + 1;
+    if ((rc = ws_get(ctx, kSlotHashIdx,
+                     carve_total({n * sizeof(uint32_t), n * sizeof(uint32_t), n * sizeof(uint32_t), n,
+                                  nq_warp * sizeof(uint32_t), nq_cta * sizeof(uint32_t)}),
+                     &p)))
+        return rc;
     Carver cv(p);
     uint32_t *slot_of = cv.take<uint32_t>(n);
     uint32_t *fpos = cv.take<uint32_t>(n);
     uint32_t *run = cv.take<uint32_t>(n);
     uint8_t *first = cv.take<uint8_t>(n);
+    uint32_t *warp_runs = cv.take<uint32_t>(nq_warp);
+    uint32_t *cta_runs = cv.take<uint32_t>(nq_cta);
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
     uint32_t *d_cnt = (uint32_t *)p + 32;   // words 32..39 belong to the hash round
     uint32_t *seg_start = nullptr;
@@ -286,13 +356,13 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     }
     switch (bank_bytes) {
     case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                      slot_of, fpos, first); break;
+                                      slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
     case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                       slot_of, fpos, first); break;
+                                       slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
     case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                       slot_of, fpos, first); break;
+                                       slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
     case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                       slot_of, fpos, first); break;
+                                       slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
     default: return set_error(ctx, FMCS_E_INVAL, "hash round: bank_bytes must be 1, 2, 4 or 8");
     }
     if (rc) return rc;
