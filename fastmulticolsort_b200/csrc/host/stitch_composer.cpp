@@ -142,6 +142,38 @@ double GpuCostTables::SortRoundMs(uint64_t n, double g, uint32_t bank_bytes, uin
     return ((double)n / g) * SortGroupMs(g, bank_bytes, key_bits);
 }
 
+double GpuCostTables::SortGroupMs(double g, uint32_t bank_bytes, uint32_t key_bits, const double *split,
+                                  int nsplit) const
+{
+    if (g <= 1.0) return 0.0;
+    const int b = BankIndex(bank_bytes);
+    double per_mrow = 0.0;
+    double rest = g;
+    int levels = 0;
+    const int max_levels = (int)((key_bits + 7) / 8);
+    while (rest > (double)local_max && levels < max_levels) {
+        levels++;
+        per_mrow += msd_level[b];
+        // after `levels` levels a group holds the rows of one value of its
+        // top 8 * levels key bits: 256^levels parts at most, and no more than
+        // those bits take distinct values
+        double parts = std::pow(256.0, (double)levels);
+        if (split && levels <= nsplit) parts = std::min(parts, split[levels - 1]);
+        rest = g / std::max(1.0, std::min(parts, g));
+    }
+    int k = (int)std::ceil(std::log2(std::max(1.0, std::min(rest, (double)local_max))));
+    k = std::max(0, std::min(kLocalSizes - 1, k));
+    per_mrow += local[b][k];
+    return per_mrow * g / 1e6;
+}
+
+double GpuCostTables::SortRoundMs(uint64_t n, double g, uint32_t bank_bytes, uint32_t key_bits, const double *split,
+                                  int nsplit) const
+{
+    if (g < 1.0) g = 1.0;
+    return ((double)n / g) * SortGroupMs(g, bank_bytes, key_bits, split, nsplit);
+}
+
 // ============================================================ StitchComposer
 StitchComposer::StitchComposer(setting_t setting, uint32_t ncolumns, uint64_t nrows, compose_params_t params,
                                Column **column_values)
@@ -238,7 +270,15 @@ double StitchComposer::EstimatePlan(const uint32_t *columnOrder, const std::vect
         ms += tables_.stitch_per_byte * (src_bytes + B) * num_rows_ / 1e6;
         if (r > 0) ms += tables_.gather[bi] * num_rows_ / 1e6;
         const double groups = r == 0 ? 1.0 : estimateGroupNum(prefix, columnOrder);
-        ms += tables_.SortRoundMs(num_rows_, (double)num_rows_ / groups, B, w);
+        // distinct values of the bank's top 8, 16, ... bits inside a group:
+        // how far each radix level can split it (the reference's per-bit
+        // cardinality model, src/stitch_composer.h:16-43)
+        double split_parts[8];
+        const int nsplit = (int)std::min<uint32_t>(8, (w + 7) / 8);
+        for (int l = 0; l < nsplit; ++l)
+            split_parts[l] = estimateGroupNum(prefix + std::min<uint32_t>(w, 8u * (uint32_t)(l + 1)), columnOrder) /
+                             groups;
+        ms += tables_.SortRoundMs(num_rows_, (double)num_rows_ / groups, B, w, split_parts, nsplit);
         ms += tables_.boundary[bi] * num_rows_ / 1e6;
         ms += tables_.round_fixed_ms;
         prefix += w;

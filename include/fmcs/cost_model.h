@@ -53,6 +53,12 @@ struct FMCS_CXX_API GpuCostTables {
     double SortGroupMs(double g, uint32_t bank_bytes, uint32_t key_bits) const;
     /** Estimated ms of one sort round over n rows in groups of average size g. */
     double SortRoundMs(uint64_t n, double g, uint32_t bank_bytes, uint32_t key_bits) const;
+    /** The same with the key's distribution: split[l] = distinct values of
+     *  the top 8 * (l + 1) key bits inside a group (a radix level cannot split
+     *  a group into more parts than that), for l < nsplit. */
+    double SortGroupMs(double g, uint32_t bank_bytes, uint32_t key_bits, const double *split, int nsplit) const;
+    double SortRoundMs(uint64_t n, double g, uint32_t bank_bytes, uint32_t key_bits, const double *split,
+                       int nsplit) const;
 };
 
 }  // namespace multiAttrSort
