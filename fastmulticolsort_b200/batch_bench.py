@@ -232,6 +232,16 @@ def wide(torch, ctx, stream, reps=3, n=WIDE_ROWS):
         # the plain path's last round leaves its group ids in `group` or `g2`
         fin = group if name != "plain" or len(WIDE_BITS) % 2 == 1 else g2
         results[name] = (order.clone(), fin.clone())
+        if name != "plain":
+            # where the time goes: one more run with per-launch CUDA events
+            ctx.profile(True)
+            ctx.profile_report()
+            fn()
+            rep = ctx.profile_report()
+            ctx.profile(False)
+            out[f"{name}_kernels_ms"] = {k: round(v["ms"], 3) for k, v in
+                                         sorted(((k, v) for k, v in rep.items() if not k.startswith("_")),
+                                                key=lambda kv: -kv[1]["ms"])}
     out["speedup_order_by_vs_plain"] = round(out["plain_ms"] / out["order_by_ms"], 2)
     same = bool(torch.equal(results["order_by"][0], results["plain"][0])
                 and torch.equal(results["order_by"][1], results["plain"][1]))
