@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <iostream>
 #include <limits>
 #include <sstream>
@@ -633,6 +634,72 @@ void StitchComposer::TwoRoundsExhaustive_hash()
 }  // namespace multiAttrSort
 
 // ================================================================ C ABI
+namespace {
+
+// A composer over statistics only (bit widths, cardinalities, storage widths):
+// no column data is touched.
+struct StatComposer {
+    std::vector<multiAttrSort::SpecialiedColumn<uint64_t>> cols;
+    std::vector<multiAttrSort::Column *> ptrs;
+    std::vector<uint32_t> widths;
+    multiAttrSort::compose_params_t params;
+    multiAttrSort::setting_t setting;
+    std::unique_ptr<multiAttrSort::StitchComposer> sc;
+
+    bool init(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes, uint32_t ncols, uint64_t n,
+              int ordered)
+    {
+        cols.resize(ncols);
+        ptrs.resize(ncols);
+        widths.assign(bw, bw + ncols);
+        uint32_t sum = 0;
+        for (uint32_t c = 0; c < ncols; ++c) {
+            if (bw[c] == 0 || bw[c] > 64) return false;
+            cols[c].SetWidth(col_bytes[c]);
+            cols[c].SetCardinality(cardinality[c]);
+            ptrs[c] = &cols[c];
+            sum += bw[c];
+        }
+        params.bitwidth = widths.data();
+        params.colwidth_sum = sum;
+        params.ordered = ordered ? 1 : 0;
+        sc.reset(new multiAttrSort::StitchComposer(setting, ncols, n, params, ptrs.data()));
+        return true;
+    }
+};
+
+}  // namespace
+
+extern "C" FMCS_API int fmcs_estimate_plan(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes,
+                                           uint32_t ncols, uint64_t n, const uint32_t *col_order,
+                                           const uint32_t *split, uint32_t nbanks, double *est_ms)
+{
+    if (!bw || !cardinality || !col_bytes || !split || !est_ms || ncols == 0 || ncols > 64 || nbanks == 0)
+        return FMCS_E_INVAL;
+    try {
+        std::vector<uint32_t> order(ncols);
+        std::vector<bool> seen(ncols, false);
+        for (uint32_t c = 0; c < ncols; ++c) {
+            order[c] = col_order ? col_order[c] : c;
+            if (order[c] >= ncols || seen[order[c]]) return FMCS_E_INVAL;
+            seen[order[c]] = true;
+        }
+        uint64_t total = 0, sum = 0;
+        for (uint32_t c = 0; c < ncols; ++c) total += bw[c];
+        for (uint32_t b = 0; b < nbanks; ++b) {
+            if (split[b] == 0 || split[b] > 64) return FMCS_E_INVAL;
+            sum += split[b];
+        }
+        if (sum != total) return FMCS_E_INVAL;
+        StatComposer st;
+        if (!st.init(bw, cardinality, col_bytes, ncols, n, 1)) return FMCS_E_INVAL;
+        *est_ms = st.sc->EstimatePlan(order.data(), std::vector<uint32_t>(split, split + nbanks));
+        return FMCS_OK;
+    } catch (...) {
+        return FMCS_E_INVAL;
+    }
+}
+
 extern "C" FMCS_API int fmcs_optimize_plan(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes,
                                            uint32_t ncols, uint64_t n, int ordered, uint32_t *split_out,
                                            uint32_t max_banks, uint32_t *nbanks_out, uint32_t *col_order_out,
@@ -642,26 +709,11 @@ extern "C" FMCS_API int fmcs_optimize_plan(const uint32_t *bw, const uint64_t *c
     if (!bw || !cardinality || !col_bytes || !split_out || !nbanks_out || ncols == 0 || ncols > 64)
         return FMCS_E_INVAL;
     try {
-        std::vector<SpecialiedColumn<uint64_t>> cols(ncols);   // statistics only: no data is touched
-        std::vector<Column *> ptrs(ncols);
-        std::vector<uint32_t> widths(bw, bw + ncols);
-        uint32_t sum = 0;
-        for (uint32_t c = 0; c < ncols; ++c) {
-            if (bw[c] == 0 || bw[c] > 64) return FMCS_E_INVAL;
-            cols[c].SetWidth(col_bytes[c]);
-            cols[c].SetCardinality(cardinality[c]);
-            ptrs[c] = &cols[c];
-            sum += bw[c];
-        }
-        compose_params_t params;
-        params.bitwidth = widths.data();
-        params.colwidth_sum = sum;
-        params.ordered = ordered ? 1 : 0;
-        setting_t setting;
-        StitchComposer sc(setting, ncols, n, params, ptrs.data());
+        StatComposer st;
+        if (!st.init(bw, cardinality, col_bytes, ncols, n, ordered)) return FMCS_E_INVAL;
         std::vector<uint32_t> order;
         double est = 0.0;
-        std::vector<uint32_t> plan = sc.OptimizePlan(&order, &est);
+        std::vector<uint32_t> plan = st.sc->OptimizePlan(&order, &est);
         if (plan.empty() || plan.size() > max_banks) return FMCS_E_INVAL;
         for (size_t i = 0; i < plan.size(); ++i) split_out[i] = plan[i];
         *nbanks_out = (uint32_t)plan.size();

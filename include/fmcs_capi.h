@@ -291,10 +291,26 @@ FMCS_API int fmcs_run_batch(fmcs_ctx *ctx, const void *const *cols, const uint32
  * width, number of distinct values and storage bytes, returns the estimated
  * cheapest split (split_out, *nbanks_out <= max_banks) and, for GROUP BY
  * (ordered == 0, columns may be permuted), the column order.  Costs come from
- * the GPU tables (tuning/b200.json next to the library, or FMCS_TUNING). */
+ * the GPU tables (tuning/b200.json next to the library, or FMCS_TUNING).
+ * The model assumes the values of a column split the rows into equal groups;
+ * for a skewed column pass its effective cardinality n^2 / sum(count^2) over
+ * its values' row counts (the number of equal groups with the same mean group
+ * size per row) instead of its distinct count: a Zipf(1.0) column of 2^20
+ * codes in 67M rows has about 1M distinct values but an effective cardinality
+ * near 127, and only the latter predicts how far its groups split. */
 FMCS_API int fmcs_optimize_plan(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes,
                                 uint32_t ncols, uint64_t n, int ordered, uint32_t *split_out, uint32_t max_banks,
                                 uint32_t *nbanks_out, uint32_t *col_order_out, double *est_ms);
+
+/* The cost model's estimate (ms on this GPU) of one given plan: split[0..nbanks)
+ * over the columns in col_order (NULL = as given), the same tables and the
+ * same per-round model as fmcs_optimize_plan's search (StitchComposer::
+ * EstimatePlan; the reference estimates plans in StitchComposer::
+ * cost_estimation, src/stitch_composer.cpp:2929-3166).  The split must cover
+ * the columns' bits exactly. */
+FMCS_API int fmcs_estimate_plan(const uint32_t *bw, const uint64_t *cardinality, const uint32_t *col_bytes,
+                                uint32_t ncols, uint64_t n, const uint32_t *col_order, const uint32_t *split,
+                                uint32_t nbanks, double *est_ms);
 
 /* Allocation-free group ids (no counterpart in the reference, which mallocs
  * on every call).  For callers that cannot let a library allocate device

@@ -60,7 +60,7 @@ def data_zipf():
 
 def zipf_plans(cols, bw):
     sizes = np.bincount(cols[0].astype(np.int64), minlength=1 << 20)
-    card = [int((sizes > 0).sum()), 1 << 24, N_ZIPF]
+    card = [capi.effective_cardinality(sizes), 1 << 24, N_ZIPF]
     plan, corder, _ = capi.optimize_plan(bw, card, [4, 4, 8], N_ZIPF)
     assert corder == [0, 1, 2]
     return [list(bw), plan]
