@@ -437,7 +437,7 @@ extern "C" int fmcs_hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_by
     if (ngroups) *ngroups = 0;
     if (!valid_bank(bank_bytes))
         return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: bank_bytes must be 1, 2, 4 or 8");
-    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: n must be < 2^32");
+    if (n >= kHashMaxRows) return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: n must be < 2^31");
     if (n == 0) return FMCS_OK;
     if (!bank || !order || (!last_round && !out_group))
         return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round: bank, order and (unless last) out_group required");
@@ -479,7 +479,8 @@ extern "C" int fmcs_hash_round_unordered(fmcs_ctx *ctx, const void *bank, uint32
     if (ngroups) *ngroups = 0;
     if (!valid_bank(bank_bytes) || (n && (!bank || !out_group)))
         return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round_unordered: invalid arguments");
-    if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round_unordered: n must be < 2^32");
+    if (n >= kHashMaxRows)
+        return set_error(ctx, FMCS_E_INVAL, "fmcs_hash_round_unordered: n must be < 2^31");
     if (n == 0) return FMCS_OK;
     int rc;
     const void *dbank = nullptr, *dig = nullptr;
@@ -510,6 +511,7 @@ int run_plan_impl(fmcs_ctx *ctx, const void *const *cols, const uint32_t *col_by
         nbanks > kMaxPlanBanks)
         return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: invalid arguments");
     if (n >= (1ull << 32)) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: n must be < 2^32");
+    if (hash && n >= kHashMaxRows) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: hash plans take n < 2^31");
     if (n && !order_out) return set_error(ctx, FMCS_E_INVAL, "fmcs_run_plan: order_out is required");
     for (uint32_t c = 0; c < ncols; ++c) {
         if (!valid_bank(col_bytes[c]) || bw[c] == 0 || bw[c] > 8 * col_bytes[c] || (n && !cols[c]))
@@ -799,7 +801,7 @@ static int graph_create(fmcs_ctx *parent, const void *const *cols, const uint32_
     *out = nullptr;
     cudaSetDevice(parent->device);
     if (!cols || !col_bytes || !bw || !split || ncols == 0 || nbanks == 0 || ncols > kMaxPlanCols ||
-        nbanks > kMaxPlanBanks || n == 0 || n >= (1ull << 32) || !order_out)
+        nbanks > kMaxPlanBanks || n == 0 || n >= (hash ? kHashMaxRows : (1ull << 32)) || !order_out)
         return set_error(parent, FMCS_E_INVAL, "fmcs_graph_create: invalid arguments");
     for (uint32_t c = 0; c < ncols; ++c) {
         if (!(col_bytes[c] == 2 || col_bytes[c] == 4 || col_bytes[c] == 8) || bw[c] == 0 || bw[c] > 8 * col_bytes[c])

@@ -248,6 +248,9 @@ int launch_flag_rank(fmcs_ctx *ctx, const uint8_t *flags, uint32_t *rank, uint64
 // ---------------------------------------------------------------- hash grouping
 // fixed_launches: the same launches whatever the data, with no host
 // read-back (graph capture).
+// Rows a hash round takes at most (less one): its table's slot indices are
+// 32-bit words below two sentinels, so it holds at most 2^31 slots.
+constexpr uint64_t kHashMaxRows = 1ull << 31;
 int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint32_t *order_in,
                uint32_t *order_out, const uint32_t *in_group, uint32_t *out_group, uint64_t n,
                bool last_round, uint32_t *d_ngroups, bool group_is_key = false, bool fixed_launches = false);

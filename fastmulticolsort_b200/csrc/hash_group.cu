@@ -54,19 +54,21 @@ __device__ __forceinline__ K key_at(const K *bank, const uint32_t *order, uint64
 // row part can change).  The slot's final row part is the key's first
 // appearance inside its run.
 constexpr unsigned long long kEmptySlot = ~0ull;
+constexpr uint64_t kHashMinSlots = 1024;
+constexpr uint64_t kHashMaxSlots = kHashMaxRows;   // slot indices stay below slot_of's sentinels
 
 // slot_of of a row alone in its parent run: it is its own first appearance
 // and takes no slot.
 constexpr uint32_t kAlone = 0xFFFFFFFFu;
 
 template <typename K>
-__global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ bank, const uint32_t *__restrict__ order,
-                                                          const uint32_t *__restrict__ run, bool runs_contiguous,
-                                                          const uint32_t *__restrict__ seg_start, uint32_t onchip_max,
-                                                          uint64_t n, unsigned long long *slots, uint64_t mask,
-                                                          uint32_t *slot_of, int *status)
+__global__ void __launch_bounds__(256)
+hash_insert_kernel(const K *__restrict__ bank, const uint32_t *__restrict__ order, const uint32_t *__restrict__ run,
+                   bool runs_contiguous, const uint32_t *__restrict__ seg_start, uint32_t onchip_max, uint64_t n,
+                   unsigned long long *slots, const unsigned long long *d_mask, uint32_t *slot_of, int *status)
 {
     kernel_prologue();
+    const uint64_t mask = *d_mask;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t r = run ? run[i] : 0u;
         if (seg_start && seg_start[r + 1] - seg_start[r] <= onchip_max) continue;   // numbered on chip
@@ -93,19 +95,42 @@ __global__ void __launch_bounds__(256) hash_insert_kernel(const K *__restrict__ 
             if ((uint32_t)(cur >> 32) == fp) {
                 const uint32_t rr = (uint32_t)cur;   // a row of this slot's (run, key)
                 if (key_at(bank, order, rr) == k && (run ? run[rr] : 0u) == r) {
-                    atomicMin(&slots[h], mine);
+                    // the slot's row only decreases: a smaller row there already wins
+                    if (rr > (uint32_t)i) atomicMin(&slots[h], mine);
                     slot_of[i] = (uint32_t)h;
                     break;
                 }
             }
             h = (h + 1) & mask;
-            if (++probes > mask) {   // table full: cannot happen with >= 2n slots
+            if (++probes > mask) {   // table full: cannot happen with more slots than rows
                 atomicCAS(status, kDevOk, kDevBadInput);
                 slot_of[i] = 0;
                 break;
             }
         }
     }
+}
+
+// The table's slots set empty: cap_max slots without parent runs, else just
+// enough for the rows of the runs the global table takes (counts[2], set by
+// the classification; none when every run is numbered on chip).  The mask
+// the insert uses is written to *d_mask.
+__global__ void hash_table_clear_kernel(unsigned long long *slots, uint64_t cap_max, const uint32_t *counts,
+                                        unsigned long long *d_mask)
+{
+    kernel_prologue();
+    uint64_t cap = cap_max;
+    if (counts) {
+        const uint64_t rows = counts[2];
+        cap = rows ? kHashMinSlots : 0;
+        while (cap && cap < 2 * rows) cap <<= 1;
+        cap = min(cap, cap_max);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_mask = cap ? cap - 1 : 0;
+    uint4 *w = reinterpret_cast<uint4 *>(slots);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap / 2; i += stride)
+        w[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
 }
 
 // slot_of of a row whose parent run was numbered in shared memory: its fpos
@@ -158,6 +183,9 @@ __global__ void hash_runs_classify_kernel(const uint32_t *__restrict__ seg_start
         const uint32_t slot = base + __popc(peers & lanemask_lt());
         if (which == 0) warp_runs[slot] = s;
         else if (which == 1) cta_runs[slot] = s;
+        // rows of the runs left to the global table (sizes its clear)
+        const uint32_t big = __reduce_add_sync(0xFFFFFFFFu, len > kRunOnChip ? len : 0u);
+        if (lane == 0 && big) atomicAdd(&counts[2], big);
     }
 }
 
@@ -275,16 +303,17 @@ __global__ void assign_ids_kernel(const uint32_t *__restrict__ fpos, const uint3
 
 // The round's numbering: with parent-run starts (seg_start, *d_nseg runs),
 // runs of up to kRunOnChip rows in shared memory, the others in the global
-// table; without, every row in the global table.
+// table; without, every row in the global table.  The table (cap_max slots
+// allocated) is cleared only as far as the rows it takes need.
 template <typename K>
 int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const uint32_t *run, bool runs_contiguous,
                 const uint32_t *seg_start, const uint32_t *d_nseg, uint64_t n, unsigned long long *slots,
-                uint64_t mask, uint32_t *slot_of, uint32_t *fpos, uint8_t *first, uint32_t *warp_runs,
-                uint32_t *cta_runs, uint32_t *counts)
+                uint64_t cap_max, unsigned long long *d_mask, uint32_t *slot_of, uint32_t *fpos, uint8_t *first,
+                uint32_t *warp_runs, uint32_t *cta_runs, uint32_t *counts)
 {
     const unsigned grid = (unsigned)ctx->num_sms * 8;
     if (seg_start) {
-        cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), ctx->stream);
+        cudaMemsetAsync(counts, 0, 3 * sizeof(uint32_t), ctx->stream);
         {
             LaunchScope ls_(ctx, "hash_runs_classify");
             launch_k(hash_runs_classify_kernel, grid, 256, 0, ctx->stream, seg_start, d_nseg, slot_of, fpos, first,
@@ -295,9 +324,13 @@ int hash_insert(fmcs_ctx *ctx, const void *bank, const uint32_t *order, const ui
                  (const uint32_t *)warp_runs, (const uint32_t *)cta_runs, (const uint32_t *)counts, slot_of, fpos,
                  first);
     }
+    { LaunchScope ls_(ctx, "hash_table_clear");
+        launch_k(hash_table_clear_kernel, grid, 256, 0, ctx->stream, slots, cap_max,
+                 (const uint32_t *)(seg_start ? counts : nullptr), d_mask);
+    }
     { LaunchScope ls_(ctx, "hash_insert");
         launch_k(hash_insert_kernel<K>, grid, 256, 0, ctx->stream, (const K *)bank, order, run, runs_contiguous,
-                 seg_start, kRunOnChip, n, slots, mask, slot_of, ctx->d_status);
+                 seg_start, kRunOnChip, n, slots, (const unsigned long long *)d_mask, slot_of, ctx->d_status);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "hash insert launch");
@@ -310,16 +343,16 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
                uint32_t *d_ngroups, bool group_is_key, bool fixed_launches)
 {
     if (n == 0) return FMCS_OK;
+    if (n >= kHashMaxSlots) return set_error(ctx, FMCS_E_INVAL, "hash round: at most 2^31 - 1 rows");
     cudaStream_t st = ctx->stream;
     int rc;
     void *p;
-    uint64_t cap = 1024;
-    while (cap < 2 * n) cap <<= 1;
-    // table: cap 64-bit slots, all empty
+    // table: up to cap 64-bit slots (at least twice the rows, at most 2^31;
+    // always more slots than rows), cleared on the device by hash_insert
+    uint64_t cap = kHashMinSlots;
+    while (cap < 2 * n && cap < kHashMaxSlots) cap <<= 1;
     if ((rc = ws_get(ctx, kSlotHashTable, cap * sizeof(unsigned long long), &p))) return rc;
     unsigned long long *slots = (unsigned long long *)p;
-    cudaMemsetAsync(slots, 0xFF, cap * sizeof(unsigned long long), st);
-    // per-row scratch: slot_of / rank (n), fpos (n), run ids (n), first flags (n bytes)
     // per-row scratch: slot_of / rank, fpos, run ids, first flags; and the
     // queues of parent runs numbered on chip (a warp each: at most n / 2 runs
     // of 2..32 rows; a CTA each: at most n / 33)
@@ -337,7 +370,8 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
     uint32_t *warp_runs = cv.take<uint32_t>(nq_warp);
     uint32_t *cta_runs = cv.take<uint32_t>(nq_cta);
     if ((rc = ws_get(ctx, kSlotCounters, 4096, &p))) return rc;
-    uint32_t *d_cnt = (uint32_t *)p + 32;   // words 32..39 belong to the hash round
+    uint32_t *d_cnt = (uint32_t *)p + 32;   // words 32..39 and 48..49 belong to the hash round
+    unsigned long long *d_mask = reinterpret_cast<unsigned long long *>((uint32_t *)p + 48);
     uint32_t *seg_start = nullptr;
     // The key of a row is (its parent run, its value): the run id from a
     // boundary scan of in_group, or -- when the previous ids are not clustered
@@ -355,14 +389,14 @@ int hash_round(fmcs_ctx *ctx, const void *bank, uint32_t bank_bytes, const uint3
         contiguous = true;
     }
     switch (bank_bytes) {
-    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                      slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
-    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                       slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
-    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                       slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
-    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap - 1,
-                                       slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
+    case 1: rc = hash_insert<uint8_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap,
+                                      d_mask, slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
+    case 2: rc = hash_insert<uint16_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap,
+                                       d_mask, slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
+    case 4: rc = hash_insert<uint32_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap,
+                                       d_mask, slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
+    case 8: rc = hash_insert<uint64_t>(ctx, bank, order_in, keyrun, contiguous, seg_start, d_cnt, n, slots, cap,
+                                       d_mask, slot_of, fpos, first, warp_runs, cta_runs, d_cnt + 4); break;
     default: return set_error(ctx, FMCS_E_INVAL, "hash round: bank_bytes must be 1, 2, 4 or 8");
     }
     if (rc) return rc;

@@ -11,7 +11,8 @@
  *
  * Conventions
  *   - Row ids (oids), order and group vectors are uint32 (surrogate_t,
- *     src/params.h:9-13); n < 2^32.
+ *     src/params.h:9-13); n < 2^32.  Hash rounds (and hash plans) take
+ *     n < 2^31: their table holds up to 2^31 slots with 32-bit indices.
  *   - Banks are 1, 2, 4 or 8 bytes per row (sort rounds: 2, 4 or 8).
  *   - Pointers may be device pointers or host pointers (pageable or pinned);
  *     host data is staged through the context's device buffers, so a host

@@ -48,6 +48,22 @@ def test_row_count_limit_rejected(ctx):
     assert rc == capi.FMCS_E_INVAL
 
 
+def test_hash_row_limit_rejected(ctx):
+    """Hash rounds take n < 2^31 (32-bit slot indices below two sentinels):
+    FMCS_E_INVAL before any staging (tiny stand-in arrays)."""
+    import ctypes
+    L = capi.load()
+    a = np.zeros(4, np.uint64)
+    o = np.zeros(4, np.uint32)
+    g = np.zeros(4, np.uint32)
+    ng = ctypes.c_uint32(0)
+    rc = L.fmcs_hash_round(ctx.handle, a.ctypes.data, 8, o.ctypes.data, None, g.ctypes.data, 1 << 31, 0,
+                           ctypes.byref(ng))
+    assert rc == capi.FMCS_E_INVAL
+    rc = L.fmcs_hash_round_unordered(ctx.handle, a.ctypes.data, 8, None, g.ctypes.data, 1 << 31, ctypes.byref(ng))
+    assert rc == capi.FMCS_E_INVAL
+
+
 @pytest.mark.parametrize("n", [2, 15, 16, 17, 32, 33, 128, 129, 512, 513, 2048, 2049, 2304, 2305, 4096, 4097,
                                8192, 8193])
 def test_tier_edges_round0(ctx, n):
