@@ -175,11 +175,14 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
         // round 0 of a sort plan over more rows than one block sorts: the
         // stitch also counts the first radix level's histogram
         uint32_t *top_hist = nullptr;
+        const uint32_t chunk_rows = msd_chunk_rows(ctx);
         if (!hash && !in_group && n > ctx->local_max) {
-            if ((rc = ws_get(ctx, kSlotTopHist, 256 * sizeof(uint32_t), &p))) return rc;
+            const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
+            if ((rc = ws_get(ctx, kSlotTopHist, nchunks * 256 * sizeof(uint32_t), &p))) return rc;
             top_hist = (uint32_t *)p;
         }
-        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits))) return rc;
+        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits, chunk_rows)))
+            return rc;
         uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
         if (!hash) {
             // (b)+(d): sort, then group ids (+ the next round's segments)

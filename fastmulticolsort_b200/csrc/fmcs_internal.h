@@ -185,11 +185,12 @@ struct StitchSlice {
     uint32_t invert;   // 1: the slice's bits are inverted (its column sorts descending)
 };
 constexpr int kMaxSlices = 32;
-// With top_hist (device, 256 words), the stitch also counts the top digit
-// (bits [key_bits - min(8, key_bits), key_bits)) of every bank value: the
-// first radix level's histogram of a round-0 sort of the bank.
+// With top_hist (device, 256 words per chunk of chunk_rows rows), the stitch
+// also counts the top digit (bits [key_bits - min(8, key_bits), key_bits)) of
+// every bank value, one row per chunk: the first radix level's per-chunk
+// histograms of a round-0 sort of the bank (chunk_rows = msd_chunk_rows).
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0);
+                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0, uint32_t chunk_rows = 0);
 
 // bank[i] <<= lshift (src == NULL) or bank[i] |= (src[i] >> rshift) & mask(width)
 int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,
@@ -212,7 +213,7 @@ struct SortArgs {
     void *keys_out;            // device, n keys, or NULL
     uint64_t n;
     bool fixed_launches = false;  // launch every level (no host read-back), e.g. under graph capture
-    const uint32_t *top_hist = nullptr;  // round 0 only: the first level's digit histogram, already counted
+    const uint32_t *top_hist = nullptr;  // round 0 only: the first level's per-chunk digit histograms, already counted
     // Device-side overrides read by the round's first kernel (no host
     // read-back): the significant key bits (<= key_bits, which then only
     // bounds the number of radix levels), and a flag that, when non-zero,
@@ -221,6 +222,9 @@ struct SortArgs {
     const uint32_t *d_in_order = nullptr;
 };
 int sort_segments(fmcs_ctx *ctx, const SortArgs &a);
+// Rows per look-back chunk of an HBM radix level (kChunkTiles tiles of the
+// context's tile size): the row granularity of the per-chunk histograms.
+uint32_t msd_chunk_rows(const fmcs_ctx *ctx);
 // Stable full-array LSD radix sort of (keys, vals) in place by key bits
 // [0, bits): the plain, unsegmented comparator path.
 int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits);

@@ -78,7 +78,19 @@ constexpr uint32_t kCopySplit = 4096;
 constexpr int kCtrLevel = 15;      // MSD levels started so far (device-side level index)
 constexpr int kCtrLocalC3 = 16;
 constexpr int kCtrLocalC1b = 17;
+constexpr int kCtrChunks0 = 18;    // + level parity: histogram rows (chunks) of the level's large segments
 constexpr int kCtrWords = 32;
+
+// An HBM level cuts each large segment's look-back chain every kChunkTiles
+// tiles.  Each chunk has its own histogram row; msd_plan turns the rows of a
+// segment into per-chunk digit bases (the segment's offset of the digit plus
+// the digit's rows in the segment's earlier chunks), so a chunk's first tile
+// publishes its inclusive prefix at once and no tile walks back past its
+// chunk's start.  One long chain (a round's single segment of thousands of
+// tiles) makes every tile wait on the whole GPU's progress; chains of 16
+// tiles run side by side (one level over 16.8M rows: 0.164 ms as one
+// segment, 0.137 ms as 256 segments of 16 tiles).
+constexpr uint32_t kChunkTiles = 16;
 
 struct LargeSeg {
     uint32_t start, len, shift, src;
@@ -97,7 +109,19 @@ struct LevelRefs {
     uint32_t *ctr;
     int dev_level;
     int hist0_ready;   // level 0's histogram was counted before the sort (by the stitch)
+    // Per large segment, its first histogram row (chunk), prefix-summed by
+    // level_prefix_kernel; NULL: one row and one look-back chain per segment.
+    uint32_t *chunk_prefix;
+    // With hist0_ready: level 0's per-chunk histogram rows as the stitch
+    // counted them (msd_plan reads them and writes the bases to hist[0]).
+    const uint32_t *top_hist;
 };
+
+__host__ __device__ __forceinline__ uint32_t seg_chunks(uint32_t len, uint32_t tile_rows)
+{
+    const uint32_t tiles = (len + tile_rows - 1) / tile_rows;
+    return (tiles + kChunkTiles - 1) / kChunkTiles;
+}
 
 // Index of the level whose launches are running (level_prefix_kernel has
 // already advanced the counter for it).
@@ -214,14 +238,14 @@ __device__ __forceinline__ uint32_t alloc_slot(uint32_t *ctr, int which)
 // A large segment gets its next-level histogram row zeroed here when
 // hist_out is given (the round's initial segments); the children of a radix
 // level get theirs zeroed by that level's scatter grid, coalesced.
-__device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
-                                              uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L,
-                                              uint32_t *hist_out)
+__device__ __forceinline__ int route_segment(uint32_t start, uint32_t len, uint32_t shift, uint32_t src,
+                                             uint32_t *ctr, int large_ctr, LargeSeg *large_out, const Lists &L,
+                                             uint32_t *hist_out)
 {
-    if (len == 0) return;
+    if (len == 0) return -1;
     int which;
     if (len == 1 || shift == 0) {
-        if (src == kSrcBuf0) return;   // already in place
+        if (src == kSrcBuf0) return -1;   // already in place
         which = len > kCopySplit ? kCtrCopyLarge : kCtrCopy;
     } else if (len > L.local_max) {
         which = large_ctr;
@@ -269,6 +293,7 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
         }
     }
     }
+    return which;
 }
 
 // ---------------------------------------------------------------------------
@@ -277,20 +302,19 @@ __device__ __forceinline__ void route_segment(uint32_t start, uint32_t len, uint
 template <typename K>
 __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_start, const uint32_t *d_nseg,
                                 uint64_t n, uint32_t key_bits, uint32_t *ctr, LargeSeg *large0, Lists lists,
-                                uint32_t *hist0, const uint32_t *top_hist, const uint32_t *d_key_bits,
-                                const uint32_t *d_in_order)
+                                const uint32_t *top_hist, const uint32_t *d_key_bits, const uint32_t *d_in_order)
 {
     kernel_prologue();
     if (d_key_bits) key_bits = min(key_bits, *d_key_bits);
     if (d_in_order && *d_in_order) key_bits = 0;   // every segment is in order: copy only
     if (!seg_start && top_hist && n > lists.local_max) {
         // round 0 over the whole array with its first-level histogram already
-        // counted: the one large segment, histogram row 0 = top_hist
-        if (threadIdx.x == 0) {
+        // counted (level 0's msd_plan reads the stitch's rows): the one large
+        // segment
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
             ctr[kCtrLarge0] = 1;
             large0[0] = LargeSeg{0, (uint32_t)n, key_bits, kSrcExt};
         }
-        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist0[d] = top_hist[d];
         return;
     }
     const uint32_t nseg = seg_start ? *d_nseg : 1u;
@@ -307,7 +331,8 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
             b.v0[start] = v;
             continue;
         }
-        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, lists, hist0);
+        // (level 0's histogram rows are zeroed by its level_prefix_kernel)
+        route_segment(start, len, key_bits, kSrcExt, ctr, kCtrLarge0, large0, lists, nullptr);
     }
 }
 
@@ -318,7 +343,7 @@ __global__ void classify_kernel(Bufs<K> b, const uint32_t *__restrict__ seg_star
 // Also resets the level's counters (tile counter, rows moved, next-level
 // count) so that no separate memsets are needed.
 __device__ __forceinline__ void tile_prefix_body(const LargeSeg *segs, uint32_t nseg, uint32_t *tile_prefix,
-                                                 uint32_t tile_rows)
+                                                 uint32_t tile_rows, bool chunks = false)
 {
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry;
@@ -326,7 +351,9 @@ __device__ __forceinline__ void tile_prefix_body(const LargeSeg *segs, uint32_t 
     __syncthreads();
     for (uint32_t base = 0; base < nseg; base += blockDim.x) {
         const uint32_t s = base + threadIdx.x;
-        const uint32_t c = s < nseg ? (segs[s].len + tile_rows - 1) / tile_rows : 0u;
+        const uint32_t c = s >= nseg ? 0u
+                           : chunks  ? seg_chunks(segs[s].len, tile_rows)
+                                     : (segs[s].len + tile_rows - 1) / tile_rows;
         uint32_t incl = c;
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -373,11 +400,24 @@ __global__ void __launch_bounds__(1024) level_prefix_kernel(LevelRefs r, uint32_
     __syncthreads();   // every thread has read the level index before it advances
     if (threadIdx.x == 0) {
         r.ctr[kCtrLarge0 + nxt] = 0;
+        r.ctr[kCtrChunks0 + nxt] = 0;
         r.ctr[kCtrMsdTile] = 0;
         r.ctr[kCtrMoved] = 0;
         if (r.dev_level) r.ctr[kCtrLevel] = lvl + 1;
     }
-    tile_prefix_body((cur ? r.large[1] : r.large[0]), nseg, tile_prefix, tile_rows);
+    const LargeSeg *segs = cur ? r.large[1] : r.large[0];
+    tile_prefix_body(segs, nseg, tile_prefix, tile_rows);
+    if (r.chunk_prefix) {
+        tile_prefix_body(segs, nseg, r.chunk_prefix, tile_rows, true);
+        if (lvl == 0 && !r.hist0_ready) {
+            // level 0's histogram rows start at zero (a level's scatter zeroes
+            // the next level's rows)
+            __syncthreads();
+            const uint64_t words = (uint64_t)r.chunk_prefix[nseg] * (kRadix / 4);
+            uint4 *h = reinterpret_cast<uint4 *>(cur ? r.hist[1] : r.hist[0]);
+            for (uint64_t i = threadIdx.x; i < words; i += blockDim.x) h[i] = make_uint4(0, 0, 0, 0);
+        }
+    }
 }
 
 
@@ -434,6 +474,12 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
     uint32_t s = find_segment_warp(tile_prefix, nseg, t0);
     LargeSeg sg = segs[s];
     uint32_t sfirst = tile_prefix[s], snext = tile_prefix[s + 1];
+    // the histogram row of the tiles counted so far: the segment's, or its
+    // chunk's when the level cuts segments into chunks
+    auto row_of = [&](uint32_t seg, uint32_t k) -> uint32_t {
+        return r.chunk_prefix ? r.chunk_prefix[seg] + k / kChunkTiles : seg;
+    };
+    uint32_t row = row_of(s, t0 - sfirst);
     auto flush = [&]() {
         __syncthreads();
         for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
@@ -443,20 +489,24 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
                 c += sh[w][d];
                 sh[w][d] = 0;
             }
-            if (c) atomicAdd(&hist[(uint64_t)s * kRadix + d], c);
+            if (c) atomicAdd(&hist[(uint64_t)row * kRadix + d], c);
         }
         __syncthreads();
     };
     __syncthreads();
     for (uint32_t t = t0; t < t1; ++t) {
-        if (t >= snext) {
-            flush();
+        if (t >= snext) {   // every large segment has a tile: the next tile starts the next segment
             ++s;
             sg = segs[s];
             sfirst = snext;
             snext = tile_prefix[s + 1];
         }
         const uint32_t k = t - sfirst;
+        const uint32_t trow = row_of(s, k);
+        if (trow != row) {
+            flush();
+            row = trow;
+        }
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
         const uint32_t lo = sg.shift - width;
         const uint64_t beg = (uint64_t)sg.start + (uint64_t)k * tile_rows;
@@ -477,40 +527,90 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
 }
 
 // Per large segment: exclusive digit offsets, skip detection, children.
-__global__ void __launch_bounds__(kRadix) msd_plan_kernel(LevelRefs r, Lists lists, bool emit_children = true)
+// With chunks, a segment's digit counts are the sums of its chunks' rows, and
+// each chunk's row becomes its digit bases: the segment's offset of the digit
+// plus the digit's rows in the segment's earlier chunks.  kPlanThreads threads
+// per segment: kPlanThreads / kRadix of them per digit, each summing (then
+// rewriting) a contiguous share of the chunk rows with kPlanLoads loads in
+// flight, so that a segment of hundreds of chunks costs a few round trips.
+constexpr int kPlanThreads = 1024;
+constexpr int kPlanLoads = 16;
+
+__global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lists lists, bool emit_children = true,
+                                                                uint32_t tile_rows = 0)
 {
     kernel_prologue();
+    constexpr int NQ = kPlanThreads / kRadix;   // threads per digit
     __shared__ uint32_t cnt[kRadix];
-    __shared__ uint32_t tmp[kRadix / 32 + 1];
+    __shared__ uint32_t part[NQ][kRadix];
+    __shared__ uint32_t tmp[kPlanThreads / 32 + 1];
     __shared__ uint32_t s_skip;
-    const uint32_t cur = running_level(r) & 1u, nxt = cur ^ 1u;
+    const uint32_t lvl = running_level(r);
+    const uint32_t cur = lvl & 1u, nxt = cur ^ 1u;
     LargeSeg *segs = (cur ? r.large[1] : r.large[0]);
     uint32_t *hist = (cur ? r.hist[1] : r.hist[0]);
+    // the counts: this level's rows, or at level 0 the stitch's
+    const uint32_t *counts = (lvl == 0 && r.hist0_ready && r.top_hist) ? r.top_hist : hist;
     uint32_t *ctr = r.ctr;
     const int next_large_ctr = kCtrLarge0 + (int)nxt;
     LargeSeg *large_next = (nxt ? r.large[1] : r.large[0]);
     const uint32_t nseg = ctr[kCtrLarge0 + cur];
+    const uint32_t d = threadIdx.x % kRadix;
+    const uint32_t q4 = threadIdx.x / kRadix;
     for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
         const LargeSeg sg = segs[s];
-        const uint32_t d = threadIdx.x;
-        const uint32_t c = hist[(uint64_t)s * kRadix + d];
-        cnt[d] = c;
-        if (d == 0) s_skip = 0;
+        const uint32_t r0 = r.chunk_prefix ? r.chunk_prefix[s] : s;
+        const uint32_t r1 = r.chunk_prefix ? r.chunk_prefix[s + 1] : s + 1;
+        // this thread's share of the rows
+        const uint32_t per = (r1 - r0 + NQ - 1) / NQ;
+        const uint32_t qa = min(r1, r0 + q4 * per), qb = min(r1, qa + per);
+        uint32_t c = 0;
+        for (uint32_t q = qa; q < qb; q += kPlanLoads) {
+            uint32_t v[kPlanLoads];
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + d] : 0u;
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) c += v[j];
+        }
+        part[q4][d] = c;
+        if (threadIdx.x == 0) s_skip = 0;
         __syncthreads();
-        if (c == sg.len) s_skip = 1;   // every row has this digit: the pass is the identity
+        uint32_t tot = 0;
+        if (q4 == 0) {
+#pragma unroll
+            for (int j = 0; j < NQ; ++j) tot += part[j][d];
+            cnt[d] = tot;
+            if (tot == sg.len) s_skip = 1;   // every row has this digit: the pass is the identity
+        }
         uint32_t total;
-        block_exclusive_scan_radix<kRadix>(cnt, tmp, &total);
+        block_exclusive_scan_radix<kPlanThreads>(cnt, tmp, &total);
         const uint32_t off = cnt[d];
-        hist[(uint64_t)s * kRadix + d] = off;
+        // this share's first base: the digit's offset plus the earlier shares' rows
+        uint32_t run = off;
+        for (uint32_t j = 0; j < q4; ++j) run += part[j][d];
+        for (uint32_t q = qa; q < qb; q += kPlanLoads) {
+            uint32_t v[kPlanLoads];
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + d] : 0u;
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) {
+                if (q + j < qb) hist[(uint64_t)(q + j) * kRadix + d] = run;
+                run += v[j];
+            }
+        }
         const bool skip = s_skip != 0;
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
         const uint32_t child_shift = sg.shift - width;
         const uint32_t child_src = skip ? sg.src : (sg.src == kSrcBuf1 ? kSrcBuf0 : kSrcBuf1);
-        if (emit_children && c > 0)
-            route_segment(sg.start + off, c, child_shift, child_src, ctr, next_large_ctr, large_next, lists,
-                          nullptr);   // the next level's histogram rows are zeroed by the scatter grid
-        if (d == 0 && skip) segs[s].src = sg.src | kSkipBit;
-        if (d == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
+        if (q4 == 0 && emit_children && tot > 0) {
+            // (the next level's histogram rows are zeroed by the scatter grid)
+            const int which = route_segment(sg.start + off, tot, child_shift, child_src, ctr, next_large_ctr,
+                                            large_next, lists, nullptr);
+            if (which == next_large_ctr && r.chunk_prefix)
+                atomicAdd(&ctr[kCtrChunks0 + nxt], seg_chunks(tot, tile_rows));
+        }
+        if (threadIdx.x == 0 && skip) segs[s].src = sg.src | kSkipBit;
+        if (threadIdx.x == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
         __syncthreads();
     }
 }
@@ -554,11 +654,12 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
     if (more && blockIdx.x == 0 && threadIdx.x == 0)
         cudaGraphSetConditional(more, (nnext > 0 && lvl + 1 < levels) ? 1u : 0u);
     {
-        // the histogram rows of the next level's large segments start at zero
-        // (this level's plan has placed them; the rows held this level's
-        // predecessor's offsets, which nothing reads any more)
+        // the histogram rows of the next level's large segments (or of their
+        // chunks, counted by this level's plan) start at zero (the rows held
+        // this level's predecessor's offsets, which nothing reads any more)
         uint4 *h = reinterpret_cast<uint4 *>(cur ? r.hist[0] : r.hist[1]);
-        const uint64_t words = (uint64_t)nnext * (kRadix / 4);
+        const uint32_t rows_next = r.chunk_prefix ? r.ctr[kCtrChunks0 + (cur ^ 1u)] : nnext;
+        const uint64_t words = (uint64_t)rows_next * (kRadix / 4);
         for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < words;
              i += (uint64_t)gridDim.x * blockDim.x)
             h[i] = make_uint4(0, 0, 0, 0);
@@ -579,6 +680,9 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
             continue;
         }
         const uint32_t k = t - tile_prefix[s];
+        // the tile's histogram row and its place in its look-back chain
+        const uint32_t row = r.chunk_prefix ? r.chunk_prefix[s] + k / kChunkTiles : s;
+        const uint32_t kc = r.chunk_prefix ? k % kChunkTiles : k;
         const uint32_t width = sg.shift < (uint32_t)kRadixBits ? sg.shift : (uint32_t)kRadixBits;
         const uint32_t lo = sg.shift - width;
         const uint64_t tbeg = (uint64_t)sg.start + (uint64_t)k * kTileM;
@@ -632,15 +736,15 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
             sm.total[d] = run;
             sm.doff[d] = run;
             unsigned long long *mine = &lookback[(uint64_t)t * kRadix + d];
-            st_volatile_u64(mine, lb_word(epoch, k == 0 ? kFlagInclusive : kFlagAggregate, run));
+            st_volatile_u64(mine, lb_word(epoch, kc == 0 ? kFlagInclusive : kFlagAggregate, run));
         }
         __syncthreads();
         uint32_t tot;
         block_exclusive_scan_radix<kNtM>(sm.doff, sm.tmp, &tot);
-        // decoupled look-back along the segment's tiles
+        // decoupled look-back along the chunk's tiles
         for (int d = threadIdx.x; d < kRadix; d += kNtM) {
             uint32_t excl = 0;
-            if (k > 0) {
+            if (kc > 0) {
                 int64_t p = (int64_t)t - 1;
                 for (;;) {
                     const unsigned long long w = lb_wait(&lookback[(uint64_t)p * kRadix + d], epoch, status);
@@ -652,7 +756,7 @@ __global__ void __launch_bounds__(kNtM, msd_ctas_per_sm(IT)) msd_scatter_kernel(
                                 lb_word(epoch, kFlagInclusive, excl + sm.total[d]));
             }
             const uint32_t dof = sm.doff[d];
-            sm.gdst[d] = sg.start + offs[(uint64_t)s * kRadix + d] + excl - dof;   // wraps; + slot is in range
+            sm.gdst[d] = sg.start + offs[(uint64_t)row * kRadix + d] + excl - dof;   // wraps; + slot is in range
             // the warps' exclusive counts become tile positions
 #pragma unroll
             for (int w = 0; w < kNtM / 32; ++w) sm.whist[w][d] += dof;
@@ -1460,16 +1564,25 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         lists.copy_large = cc.take<LargeSeg>(cap_large);
         lists.local_max = local_max;
     }
-    uint32_t *hists[2], *tile_prefix;
-    if ((rc = ws_get(ctx, kSlotSegHist, 2 * carve_round(cap_large * kRadix * sizeof(uint32_t)), &p))) return rc;
+    // histogram rows: one per chunk of kChunkTiles tiles of a large segment
+    // (a segment's chunks <= its tiles / kChunkTiles + 1)
+    const uint64_t max_tiles = n / tile_rows + cap_large + 1;
+    const uint64_t cap_chunks = max_tiles / kChunkTiles + cap_large + 1;
+    uint32_t *hists[2], *tile_prefix, *chunk_prefix;
+    if ((rc = ws_get(ctx, kSlotSegHist, 2 * carve_round(cap_chunks * kRadix * sizeof(uint32_t)), &p))) return rc;
     {
         Carver cv(p);
-        hists[0] = cv.take<uint32_t>(cap_large * kRadix);
-        hists[1] = cv.take<uint32_t>(cap_large * kRadix);
+        hists[0] = cv.take<uint32_t>(cap_chunks * kRadix);
+        hists[1] = cv.take<uint32_t>(cap_chunks * kRadix);
     }
-    if ((rc = ws_get(ctx, kSlotTilePrefix, (cap_large + 1) * sizeof(uint32_t), &p))) return rc;
-    tile_prefix = (uint32_t *)p;
-    const uint64_t max_tiles = n / tile_rows + cap_large + 1;
+    if ((rc = ws_get(ctx, kSlotTilePrefix, carve_total({(cap_large + 1) * sizeof(uint32_t),
+                                                        (cap_large + 1) * sizeof(uint32_t)}), &p)))
+        return rc;
+    {
+        Carver cv(p);
+        tile_prefix = cv.take<uint32_t>(cap_large + 1);
+        chunk_prefix = cv.take<uint32_t>(cap_large + 1);
+    }
     unsigned long long *lookback;
     if ((rc = ws_get(ctx, kSlotLookback, max_tiles * kRadix * sizeof(unsigned long long), &p, true))) return rc;
     lookback = (unsigned long long *)p;
@@ -1488,7 +1601,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         if (seg_start && a.nseg_host == 0) grid = (unsigned)sms * 16;
         { LaunchScope ls_(ctx, "classify");
             launch_k(classify_kernel<K>, grid, 256, 0, st, b, seg_start, d_nseg, n, a.key_bits, ctr, large[0], lists,
-                     hists[0], seg_start ? nullptr : a.top_hist, a.d_key_bits, a.d_in_order);
+                     seg_start ? nullptr : a.top_hist, a.d_key_bits, a.d_in_order);
         }
         FMCS_LAUNCH_CHECK("classify");
     }
@@ -1532,7 +1645,8 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
             tiers_known = true;
         }
         const int hist0_ready = (a.top_hist && !a.seg_start) ? 1 : 0;
-        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready};
+        const LevelRefs lr{{large[0], large[1]}, {hists[0], hists[1]}, ctr, 1, hist0_ready, chunk_prefix,
+                           hist0_ready ? a.top_hist : nullptr};
         const uint32_t epoch_base = ctx->epoch;
         ctx->epoch += (uint32_t)levels;
         const unsigned scatter_grid = sms * msd_ctas_per_sm(IT);
@@ -1549,7 +1663,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                 launch_k(msd_hist_kernel<K>, sms * kHistCtas, kNtM, 0, s, b, lr, tile_prefix, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
-                launch_k(msd_plan_kernel, sms * 8, kRadix, 0, s, lr, lists, true);
+                launch_k(msd_plan_kernel, sms * 2, kPlanThreads, 0, s, lr, lists, true, tile_rows);
             }
             if (read_back) {
                 // read the counters (the next level's count, the rows moved,
@@ -1770,7 +1884,7 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
             launch_k(msd_hist_kernel<K>, sms * kHistCtas, kNtM, 0, st, b, lr, tile_prefix, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_plan");
-            launch_k(msd_plan_kernel, 1, kRadix, 0, st, lr, none, false);
+            launch_k(msd_plan_kernel, 1, kPlanThreads, 0, st, lr, none, false, tile_rows);
         }
         { LaunchScope ls_(ctx, "msd_scatter");
             launch_k(msd_scatter_kernel<K, RANK, IT>, sms * msd_ctas_per_sm(IT), kNtM, msd_smem, st, 
@@ -1787,6 +1901,11 @@ int lsd_sort_full_t(fmcs_ctx *ctx, void *keys, uint32_t *vals, uint64_t n, uint3
 }
 
 }  // namespace
+
+uint32_t msd_chunk_rows(const fmcs_ctx *ctx)
+{
+    return kChunkTiles * (uint32_t)kNtM * (ctx->msd_items >= 16 ? 16u : 8u);
+}
 
 int lsd_sort_full(fmcs_ctx *ctx, void *keys, uint32_t key_bytes, uint32_t *vals, uint64_t n, uint32_t bits)
 {

@@ -91,23 +91,36 @@ __device__ __forceinline__ void store4(B *bank, uint64_t row, bool vec, uint64_t
         if (row + k < n) bank[row + k] = (B)a[k];
 }
 
+// With top_hist the kernel also counts the first radix level's digits, one
+// 256-word row per chunk of 2^chunk_shift rows; each CTA then takes a contiguous
+// range of block_groups groups of 4 rows (at most one chunk long, so that it
+// meets at most two chunks, counted in two shared histograms).  Without, the
+// groups are spread grid-stride.
 template <typename B>
-__global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ StitchParams p, B *bank,
+__global__ void __launch_bounds__(256, 4) stitch_kernel(const __grid_constant__ StitchParams p, B *bank,
                                                      uint64_t n, bool aligned, uint32_t *top_hist,
-                                                     uint32_t hist_lo, uint32_t hist_mask)
+                                                     uint32_t hist_lo, uint32_t hist_mask, uint32_t chunk_shift,
+                                                     uint64_t block_groups)
 {
     kernel_prologue();
-    __shared__ uint32_t sh[256];
+    __shared__ uint32_t sh[2][256];
+    const uint64_t groups = (n + 3) / 4;
+    // this CTA's groups: [g_begin, g_end), `stride` apart per thread step
+    uint64_t g_begin = blockIdx.x * (uint64_t)blockDim.x, g_end = groups;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t chunk0 = 0;   // the chunk of the CTA's first row
     if (top_hist) {
-        for (int d = threadIdx.x; d < 256; d += blockDim.x) sh[d] = 0;
+        for (int d = threadIdx.x; d < 2 * 256; d += blockDim.x) (&sh[0][0])[d] = 0;
         __syncthreads();
+        g_begin = blockIdx.x * block_groups;
+        g_end = min(groups, g_begin + block_groups);
+        stride = blockDim.x;
+        chunk0 = (g_begin * 4) >> chunk_shift;
     }
     // Each thread takes two groups of 4 rows per step (a stride apart), so
     // that the loads of both are in flight together.
-    const uint64_t groups = (n + 3) / 4;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups; g += 2 * stride) {
-        const bool two = g + stride < groups;
+    for (uint64_t g = g_begin + threadIdx.x; g < g_end; g += 2 * stride) {
+        const bool two = g + stride < g_end;
         const uint64_t row0 = g * 4, row1 = (g + stride) * 4;
         const bool vec0 = aligned && row0 + 4 <= n;
         const bool vec1 = aligned && row1 + 4 <= n;
@@ -130,17 +143,24 @@ __global__ void __launch_bounds__(256) stitch_kernel(const __grid_constant__ Sti
         store4<B>(bank, row0, vec0, n, acc0);
         if (two) store4<B>(bank, row1, vec1, n, acc1);
         if (top_hist) {
+            // a group's 4 rows share a chunk (chunks are at least 4 rows)
+            uint32_t *h0 = sh[(row0 >> chunk_shift) - chunk0];
+            uint32_t *h1 = two ? sh[(row1 >> chunk_shift) - chunk0] : h0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                if (row0 + k < n) atomicAdd(&sh[(uint32_t)(acc0[k] >> hist_lo) & hist_mask], 1u);
-                if (two && row1 + k < n) atomicAdd(&sh[(uint32_t)(acc1[k] >> hist_lo) & hist_mask], 1u);
+                if (row0 + k < n) atomicAdd(&h0[(uint32_t)(acc0[k] >> hist_lo) & hist_mask], 1u);
+                if (two && row1 + k < n) atomicAdd(&h1[(uint32_t)(acc1[k] >> hist_lo) & hist_mask], 1u);
             }
         }
     }
     if (top_hist) {
         __syncthreads();
-        for (int d = threadIdx.x; d < 256; d += blockDim.x)
-            if (sh[d]) atomicAdd(&top_hist[d], sh[d]);
+        const uint64_t nchunks = ((n - 1) >> chunk_shift) + 1;
+        for (int i = threadIdx.x; i < 2 * 256; i += blockDim.x) {
+            const uint64_t c = chunk0 + (uint64_t)(i >> 8);
+            const uint32_t v = (&sh[0][0])[i];
+            if (v && c < nchunks) atomicAdd(&top_hist[c * 256 + (i & 255)], v);
+        }
     }
 }
 
@@ -191,7 +211,7 @@ int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t 
 }
 
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist, uint32_t key_bits)
+                  uint64_t n, uint32_t *top_hist, uint32_t key_bits, uint32_t chunk_rows)
 {
     if (ns < 1 || ns > kMaxSlices) return set_error(ctx, FMCS_E_INVAL, "stitch: 1..32 slices");
     if (!(bank_bytes == 1 || bank_bytes == 2 || bank_bytes == 4 || bank_bytes == 8))
@@ -209,11 +229,23 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
     const uint64_t cap = (uint64_t)ctx->num_sms * 8;
     if (blocks > cap) blocks = cap;
     uint32_t hist_lo = 0, hist_mask = 0;
+    uint64_t block_groups = 0;
+    uint32_t chunk_shift = 0;
     if (top_hist) {
+        if (chunk_rows < 4 || (chunk_rows & (chunk_rows - 1)))
+            return set_error(ctx, FMCS_E_INVAL, "stitch: chunk rows must be a power of two >= 4");
+        chunk_shift = (uint32_t)__builtin_ctz(chunk_rows);
         const uint32_t width = key_bits < 8u ? key_bits : 8u;
         hist_lo = key_bits - width;
         hist_mask = (1u << width) - 1u;
-        cudaMemsetAsync(top_hist, 0, 256 * sizeof(uint32_t), ctx->stream);
+        const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
+        cudaMemsetAsync(top_hist, 0, nchunks * 256 * sizeof(uint32_t), ctx->stream);
+        // contiguous ranges of whole 256-group steps, at most one chunk each
+        block_groups = (groups + blocks - 1) / blocks;
+        block_groups = (block_groups + 255) / 256 * 256;
+        const uint64_t chunk_groups = chunk_rows / 4;
+        if (block_groups > chunk_groups) block_groups = chunk_groups;
+        blocks = (groups + block_groups - 1) / block_groups;
     }
     const unsigned grid = (unsigned)blocks;
     cudaStream_t st = ctx->stream;
@@ -221,19 +253,19 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
     switch (bank_bytes) {
     case 1:
         launch_k(stitch_kernel<uint8_t>, grid, 256, 0, st,
-                 p, (uint8_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+                 p, (uint8_t *)bank, n, aligned, top_hist, hist_lo, hist_mask, chunk_shift, block_groups);
         break;
     case 2:
         launch_k(stitch_kernel<uint16_t>, grid, 256, 0, st,
-                 p, (uint16_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+                 p, (uint16_t *)bank, n, aligned, top_hist, hist_lo, hist_mask, chunk_shift, block_groups);
         break;
     case 4:
         launch_k(stitch_kernel<uint32_t>, grid, 256, 0, st,
-                 p, (uint32_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+                 p, (uint32_t *)bank, n, aligned, top_hist, hist_lo, hist_mask, chunk_shift, block_groups);
         break;
     case 8:
         launch_k(stitch_kernel<uint64_t>, grid, 256, 0, st,
-                 p, (uint64_t *)bank, n, aligned, top_hist, hist_lo, hist_mask);
+                 p, (uint64_t *)bank, n, aligned, top_hist, hist_lo, hist_mask, chunk_shift, block_groups);
         break;
     default: return set_error(ctx, FMCS_E_INVAL, "stitch: bank_bytes must be 1, 2, 4 or 8");
     }
