@@ -178,7 +178,7 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
         const uint32_t chunk_rows = msd_chunk_rows(ctx);
         if (!hash && !in_group && n > ctx->local_max) {
             const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
-            if ((rc = ws_get(ctx, kSlotTopHist, nchunks * 256 * sizeof(uint32_t), &p))) return rc;
+            if ((rc = ws_get(ctx, kSlotTopHist, (nchunks + 1) * 256 * sizeof(uint32_t), &p))) return rc;
             top_hist = (uint32_t *)p;
         }
         if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits, chunk_rows)))

@@ -185,10 +185,11 @@ struct StitchSlice {
     uint32_t invert;   // 1: the slice's bits are inverted (its column sorts descending)
 };
 constexpr int kMaxSlices = 32;
-// With top_hist (device, 256 words per chunk of chunk_rows rows), the stitch
-// also counts the top digit (bits [key_bits - min(8, key_bits), key_bits)) of
-// every bank value, one row per chunk: the first radix level's per-chunk
-// histograms of a round-0 sort of the bank (chunk_rows = msd_chunk_rows).
+// With top_hist (device, 256 words per chunk of chunk_rows rows and one more
+// row), the stitch also counts the top digit (bits [key_bits - min(8,
+// key_bits), key_bits)) of every bank value, one row per chunk and the total
+// in the last row: the first radix level's histograms of a round-0 sort of
+// the bank (chunk_rows = msd_chunk_rows).
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
                   uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0, uint32_t chunk_rows = 0);
 

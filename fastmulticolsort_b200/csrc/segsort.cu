@@ -87,10 +87,12 @@ constexpr int kCtrWords = 32;
 // the digit's rows in the segment's earlier chunks), so a chunk's first tile
 // publishes its inclusive prefix at once and no tile walks back past its
 // chunk's start.  One long chain (a round's single segment of thousands of
-// tiles) makes every tile wait on the whole GPU's progress; chains of 16
-// tiles run side by side (one level over 16.8M rows: 0.164 ms as one
-// segment, 0.137 ms as 256 segments of 16 tiles).
-constexpr uint32_t kChunkTiles = 16;
+// tiles) makes every tile wait on the whole GPU's progress; short chains run
+// side by side (one level over 16.8M rows: 0.164 ms as one segment, 0.137 ms
+// as 256 segments of 16 tiles).  Chunks of 32 tiles keep most of that gain
+// (the scatter 3 us slower per step than with 16) and halve the rows the
+// plan walks (8 us faster).
+constexpr uint32_t kChunkTiles = 32;
 
 struct LargeSeg {
     uint32_t start, len, shift, src;
@@ -113,7 +115,8 @@ struct LevelRefs {
     // level_prefix_kernel; NULL: one row and one look-back chain per segment.
     uint32_t *chunk_prefix;
     // With hist0_ready: level 0's per-chunk histogram rows as the stitch
-    // counted them (msd_plan reads them and writes the bases to hist[0]).
+    // counted them, and after them the segment's total row (msd_plan reads
+    // them and writes the bases to hist[0]).
     const uint32_t *top_hist;
 };
 
@@ -532,8 +535,10 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
 // plus the digit's rows in the segment's earlier chunks.  kPlanThreads threads
 // per segment: kPlanThreads / kRadix of them per digit, each summing (then
 // rewriting) a contiguous share of the chunk rows with kPlanLoads loads in
-// flight, so that a segment of hundreds of chunks costs a few round trips.
-constexpr int kPlanThreads = 1024;
+// flight, so that a segment of a hundred chunks costs a few round trips.
+// (1024 threads per segment walk long segments faster, but four times fewer
+// segments are planned at once: slower in all.)
+constexpr int kPlanThreads = 256;
 constexpr int kPlanLoads = 16;
 
 __global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lists lists, bool emit_children = true,
@@ -565,12 +570,17 @@ __global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lis
         const uint32_t per = (r1 - r0 + NQ - 1) / NQ;
         const uint32_t qa = min(r1, r0 + q4 * per), qb = min(r1, qa + per);
         uint32_t c = 0;
-        for (uint32_t q = qa; q < qb; q += kPlanLoads) {
-            uint32_t v[kPlanLoads];
+        if (counts == r.top_hist) {
+            // the stitch's rows end with the (one) segment's total
+            if (q4 == 0) c = counts[(uint64_t)r1 * kRadix + d];
+        } else {
+            for (uint32_t q = qa; q < qb; q += kPlanLoads) {
+                uint32_t v[kPlanLoads];
 #pragma unroll
-            for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + d] : 0u;
+                for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + d] : 0u;
 #pragma unroll
-            for (int j = 0; j < kPlanLoads; ++j) c += v[j];
+                for (int j = 0; j < kPlanLoads; ++j) c += v[j];
+            }
         }
         part[q4][d] = c;
         if (threadIdx.x == 0) s_skip = 0;
@@ -606,8 +616,13 @@ __global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lis
             // (the next level's histogram rows are zeroed by the scatter grid)
             const int which = route_segment(sg.start + off, tot, child_shift, child_src, ctr, next_large_ctr,
                                             large_next, lists, nullptr);
-            if (which == next_large_ctr && r.chunk_prefix)
-                atomicAdd(&ctr[kCtrChunks0 + nxt], seg_chunks(tot, tile_rows));
+            if (r.chunk_prefix) {
+                // the large children's chunks, one atomic per warp
+                const uint32_t mask = __activemask();
+                const uint32_t add = __reduce_add_sync(mask, which == next_large_ctr ? seg_chunks(tot, tile_rows)
+                                                                                     : 0u);
+                if ((int)lane_id() == __ffs(mask) - 1 && add) atomicAdd(&ctr[kCtrChunks0 + nxt], add);
+            }
         }
         if (threadIdx.x == 0 && skip) segs[s].src = sg.src | kSkipBit;
         if (threadIdx.x == 0 && !skip) atomicAdd(&ctr[kCtrMoved], sg.len);
@@ -1663,7 +1678,7 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
                 launch_k(msd_hist_kernel<K>, sms * kHistCtas, kNtM, 0, s, b, lr, tile_prefix, tile_rows);
             }
             { LaunchScope ls_(ctx, "msd_plan");
-                launch_k(msd_plan_kernel, sms * 2, kPlanThreads, 0, s, lr, lists, true, tile_rows);
+                launch_k(msd_plan_kernel, sms * 8, kPlanThreads, 0, s, lr, lists, true, tile_rows);
             }
             if (read_back) {
                 // read the counters (the next level's count, the rows moved,

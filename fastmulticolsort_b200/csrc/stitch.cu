@@ -92,7 +92,8 @@ __device__ __forceinline__ void store4(B *bank, uint64_t row, bool vec, uint64_t
 }
 
 // With top_hist the kernel also counts the first radix level's digits, one
-// 256-word row per chunk of 2^chunk_shift rows; each CTA then takes a contiguous
+// 256-word row per chunk of 2^chunk_shift rows and, after them, one row for
+// the whole bank; each CTA then takes a contiguous
 // range of block_groups groups of 4 rows (at most one chunk long, so that it
 // meets at most two chunks, counted in two shared histograms).  Without, the
 // groups are spread grid-stride.
@@ -160,6 +161,11 @@ __global__ void __launch_bounds__(256, 4) stitch_kernel(const __grid_constant__ 
             const uint64_t c = chunk0 + (uint64_t)(i >> 8);
             const uint32_t v = (&sh[0][0])[i];
             if (v && c < nchunks) atomicAdd(&top_hist[c * 256 + (i & 255)], v);
+        }
+        // and the whole bank's histogram, the row after the chunks' rows
+        for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+            const uint32_t v = sh[0][d] + sh[1][d];
+            if (v) atomicAdd(&top_hist[nchunks * 256 + d], v);
         }
     }
 }
@@ -239,7 +245,7 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
         hist_lo = key_bits - width;
         hist_mask = (1u << width) - 1u;
         const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
-        cudaMemsetAsync(top_hist, 0, nchunks * 256 * sizeof(uint32_t), ctx->stream);
+        cudaMemsetAsync(top_hist, 0, (nchunks + 1) * 256 * sizeof(uint32_t), ctx->stream);
         // contiguous ranges of whole 256-group steps, at most one chunk each
         block_groups = (groups + blocks - 1) / blocks;
         block_groups = (block_groups + 255) / 256 * 256;

@@ -88,11 +88,20 @@ def make_trace(rng, rate, duration, pool_size):
     return trace
 
 
-def warm(torch, srv, pool, rounds=2):
-    """Every slot's workspace grown to what the pool needs before timing: the
-    whole pool submitted at once, so that the slots share out its large
-    requests (a workspace that grows in the middle of a trace would put its
-    cudaMalloc, a device-wide synchronisation, on some request's latency)."""
+def warm(torch, srv, pool, slots, rounds=1):
+    """Every slot's workspace grown to what the pool needs before timing (a
+    workspace that grows in the middle of a trace puts its cudaMalloc, a
+    device-wide synchronisation, on the latency of every request in flight):
+    each request of the pool, largest first, submitted `slots` times at once so
+    that every slot runs it; then the whole pool at once, so that the shared
+    launches of small requests are warm too."""
+    for d in sorted(pool, key=lambda d: -d["n"]):
+        keep = []
+        for _ in range(slots):
+            o = torch.empty(d["n"], dtype=torch.int32, device="cuda")
+            keep.append((srv.submit(d["cols"], d["widths"], o, cardinality=d["card"]), o))
+        for tk, _ in keep:
+            srv.wait(tk)
     for _ in range(rounds):
         keep = []
         for d in pool:
@@ -208,7 +217,7 @@ def burst_benchmark(torch, slots=4, budget=150 << 30, batch_rows_max=1 << 20, se
     results = {}
     for name, brm in (("batched", batch_rows_max), ("unbatched", 0)):
         with capi.Server(0, hbm_budget_bytes=budget, slots=slots, batch_rows_max=brm) as srv:
-            warm(torch, srv, pool)
+            warm(torch, srv, pool, slots)
             torch.cuda.synchronize()
             lat, rows, wall, nb, kept = run_served(torch, srv, pool, trace, slots, keep=keep)
         results[name] = kept
@@ -246,7 +255,7 @@ def benchmark(rate=200.0, duration=5.0, pool_size=32, slots=4, budget=150 << 30,
     pool = [make_request_data(torch, rng) for _ in range(pool_size)]
     trace = make_trace(rng, rate, duration, pool_size)
     with capi.Server(0, hbm_budget_bytes=budget, slots=slots, batch_rows_max=batch_rows_max) as srv:
-        warm(torch, srv, pool)
+        warm(torch, srv, pool, slots)
         torch.cuda.synchronize()
         lat, rows, wall, batched = run_served(torch, srv, pool, trace, slots)
     with capi.Context(0) as ctx:
