@@ -44,10 +44,11 @@ def test_reference_arm_under_torchrun():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", "29518", os.path.join(ROOT, "bench.py"),
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
-    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    env = dict(os.environ, FMCS_REF_JOBS="2")
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
-    assert len(lines) == 1
+    assert len(lines) == 1   # rank 0 alone reports
     d = json.loads(lines[0])
-    assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["cores"] == 1
+    assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["cores"] == 2
     assert d["e2e"]["h2d_bytes_per_step"] == 0
