@@ -1,6 +1,6 @@
 /*
  * fmcs_oracle.c -- CPU restatement of FastMultiColSort's multi-column sort
- * path.  TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.  The shipped
+ * path.  TEST INFRASTRUCTURE ONLY: the parity oracle of the CUDA path.  The shipped
  * library never links or calls it.  Every function cites the reference code
  * it restates (paths are relative to the reference project root).
  *

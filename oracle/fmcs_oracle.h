@@ -1,6 +1,6 @@
 /*
  * fmcs_oracle.h -- CPU restatement of FastMultiColSort's multi-column sort
- * path, used ONLY as the checker for the CUDA path (tests, the smoke check and
+ * path, used ONLY as the parity oracle of the CUDA path (tests, the smoke check and
  * the CPU-baseline leg of the benchmark).  Nothing in the shipped library
  * links or calls this code.
  *

@@ -1,9 +1,9 @@
-"""ctypes front end of the checker: the C restatement (``_build/liboracle.so``)
+"""ctypes front end of the parity oracle: the C restatement (``_build/liboracle.so``)
 and, where it was built, the reference's own composer (``_ref/libfmcs_ref.so``).
 
 TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline / reference legs of ``bench.py`` import this module, and only as
-the checker or the timed CPU baseline.  The product path never does.
+the parity oracle or the timed CPU baseline.  The product path never does.
 
 Every function mirrors one C entry point of ``fmcs_oracle.h`` or
 ``ref_harness.cpp``; those files cite the reference code they follow.
