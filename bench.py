@@ -562,8 +562,13 @@ def run_fmcs(args):
     outs = [(torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32),
              torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)) for _ in range(2)]
     with capi.Server(local, hbm_budget_bytes=150 << 30, slots=2, batch_rows_max=0) as srv:
-        for k in range(2):
-            srv.wait(srv.submit(hcols, bw, outs[k][0], outs[k][1], split=SPLIT))
+        # warm both slots (submitted together, so that each runs one): a slot
+        # whose workspace grew inside the timed steps would put a cudaMalloc,
+        # a device-wide synchronisation, between the other slot's copies
+        for _ in range(2):
+            warm = [srv.submit(hcols, bw, outs[k][0], outs[k][1], split=SPLIT) for k in range(2)]
+            for t in warm:
+                srv.wait(t)
         dist_barrier(world)
         t0 = time.perf_counter()
         tickets = []

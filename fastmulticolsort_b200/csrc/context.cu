@@ -77,6 +77,34 @@ int ws_get(fmcs_ctx *ctx, int slot, size_t bytes, void **out, bool zero_new)
     return FMCS_OK;
 }
 
+int par_stream(fmcs_ctx *ctx, cudaStream_t *par)
+{
+    cudaError_t e = cudaSuccess;
+    if (!ctx->par) e = cudaStreamCreateWithFlags(&ctx->par, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->ev_fork) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "second stream");
+    *par = ctx->par;
+    return FMCS_OK;
+}
+
+int fork_par(fmcs_ctx *ctx, cudaStream_t st)
+{
+    cudaStream_t par = nullptr;
+    int rc = par_stream(ctx, &par);
+    if (rc) return rc;
+    cudaError_t e = cudaEventRecord(ctx->ev_fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(par, ctx->ev_fork, 0);
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "fork");
+}
+
+int join_par(fmcs_ctx *ctx, cudaStream_t st)
+{
+    cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->par);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+    return e == cudaSuccess ? FMCS_OK : cuda_fail(ctx, e, "join");
+}
+
 int capture_while(fmcs_ctx *ctx, cudaStream_t st,
                   const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body)
 {
@@ -287,6 +315,9 @@ extern "C" void fmcs_destroy(fmcs_ctx *ctx)
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
     if (ctx->ev_level) cudaEventDestroy(ctx->ev_level);
     if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->par) cudaStreamDestroy(ctx->par);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -74,6 +74,10 @@ struct fmcs_ctx {
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;     // capture stream of conditional-node bodies (created on first use)
+    // a second stream for independent work of one call (the on-chip tiers
+    // split in two groups) and its fork / join events (created on first use)
+    cudaStream_t par = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     size_t budget = 0;   // 0 = unlimited
     size_t held = 0;     // bytes held by the workspace
     fmcs::Workspace ws;
@@ -152,6 +156,13 @@ class LaunchScope {
 // cudaGraphSetConditional) to end the loop.
 int capture_while(fmcs_ctx *ctx, cudaStream_t st,
                   const std::function<int(cudaStream_t, cudaGraphConditionalHandle)> &body);
+
+// The context's second stream and its fork/join events (created on first
+// use): fork makes `par` wait for the work enqueued on `st` so far, join makes
+// `st` wait for the work enqueued on `par`.
+int par_stream(fmcs_ctx *ctx, cudaStream_t *par);
+int fork_par(fmcs_ctx *ctx, cudaStream_t st);
+int join_par(fmcs_ctx *ctx, cudaStream_t st);
 
 // Launches a library kernel with programmatic stream serialization: it may
 // begin launching while the stream's previous kernel finishes (its prologue

@@ -1806,8 +1806,30 @@ int sort_segments_t(fmcs_ctx *ctx, const SortArgs &a)
         LaunchScope ls_(ctx, "copy_tiles");
         launch_k(copy_tiles_kernel<K>, sms * 8, 256, 0, s, b, lists.copy_large, &ctr[kCtrCopyLarge], tile_prefix);
     }});
-    for (const Tier &t : tiers)
-        if (!tiers_known || hctr[t.word] > 0) t.launch(st);
+    // The tiers' segments are disjoint: the tiers up to the 2048-row one run
+    // on the context's stream, the larger ones and the copies on its second
+    // stream at the same time, so that a tier with few segments (one wave of
+    // one segment per CTA, latency-bound) overlaps a busy one.  While
+    // profiling, every tier stays on the context's stream (one at a time,
+    // each timed alone).
+    auto wanted = [&](const Tier &t) { return !tiers_known || hctr[t.word] > 0; };
+    size_t split = 0;
+    while (split < tiers.size() && tiers[split].word != kCtrLocalC1b) ++split;
+    bool two = !ctx->prof_on;
+    if (two) {
+        bool a = false, bb = false;
+        for (size_t i = 0; i < tiers.size(); ++i) (i < split ? a : bb) |= wanted(tiers[i]);
+        two = a && bb;
+    }
+    if (two) {
+        if ((rc = fork_par(ctx, st))) return rc;
+        for (size_t i = 0; i < tiers.size(); ++i)
+            if (wanted(tiers[i])) tiers[i].launch(i < split ? st : ctx->par);
+        if ((rc = join_par(ctx, st))) return rc;
+    } else {
+        for (const Tier &t : tiers)
+            if (wanted(t)) t.launch(st);
+    }
     FMCS_LAUNCH_CHECK("local tiers");
     return FMCS_OK;
 }
