@@ -159,30 +159,51 @@ int plan_pipeline(fmcs_ctx *ctx, const Plan &plan, const void *const *dcols, con
     const uint32_t *in_group = nullptr;
     const uint32_t *seg_in = nullptr;
     const uint32_t *d_nseg_in = nullptr;
+    // (a) a bank's stitch reads only the columns: the next round's bank is
+    // stitched on the context's second stream while this round sorts (its
+    // buffer held the bank of the round before, finished by then)
+    const uint32_t chunk_rows = msd_chunk_rows(ctx);
+    uint32_t *top_hist = nullptr;
+    auto stitch_bank = [&](uint32_t b, cudaStream_t s, void **bank_out) -> int {
+        const BankPlan &bp = plan.banks[b];
+        int r;
+        if ((r = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, bank_out))) return r;
+        std::vector<StitchSlice> sl(bp.slices.size());
+        for (size_t k = 0; k < bp.slices.size(); ++k) {
+            const SliceRec &sr = bp.slices[k];
+            sl[k] = StitchSlice{dcols[sr.col], col_bytes[sr.col], bw[sr.col] - sr.end, sr.end - sr.start + 1,
+                                descending && descending[sr.col] ? 1u : 0u};
+        }
+        // round 0 of a sort plan over more rows than one block sorts: the
+        // stitch also counts the first radix level's histograms
+        uint32_t *th = nullptr;
+        if (!hash && b == 0 && n > ctx->local_max) {
+            const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
+            void *q;
+            if ((r = ws_get(ctx, kSlotTopHist, (nchunks + 1) * 256 * sizeof(uint32_t), &q))) return r;
+            th = (uint32_t *)q;
+            top_hist = th;
+        }
+        return launch_stitch(ctx, sl.data(), (int)sl.size(), *bank_out, bp.bytes, n, th, bp.bits, chunk_rows, s);
+    };
+    void *next_bank = nullptr;   // the next round's bank, stitched on the second stream
     for (uint32_t b = 0; b < nbanks; ++b) {
         const BankPlan &bp = plan.banks[b];
         const bool last = (b + 1 == nbanks);
         ctx->prof_round = (int)b;
-        // (a) stitch the bank
         void *bank;
-        if ((rc = ws_get(ctx, kSlotBank0 + (b & 1), n * bp.bytes, &bank))) return rc;
-        std::vector<StitchSlice> sl(bp.slices.size());
-        for (size_t k = 0; k < bp.slices.size(); ++k) {
-            const SliceRec &r = bp.slices[k];
-            sl[k] = StitchSlice{dcols[r.col], col_bytes[r.col], bw[r.col] - r.end, r.end - r.start + 1,
-                                descending && descending[r.col] ? 1u : 0u};
-        }
-        // round 0 of a sort plan over more rows than one block sorts: the
-        // stitch also counts the first radix level's histogram
-        uint32_t *top_hist = nullptr;
-        const uint32_t chunk_rows = msd_chunk_rows(ctx);
-        if (!hash && !in_group && n > ctx->local_max) {
-            const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
-            if ((rc = ws_get(ctx, kSlotTopHist, (nchunks + 1) * 256 * sizeof(uint32_t), &p))) return rc;
-            top_hist = (uint32_t *)p;
-        }
-        if ((rc = launch_stitch(ctx, sl.data(), (int)sl.size(), bank, bp.bytes, n, top_hist, bp.bits, chunk_rows)))
+        if (next_bank) {
+            bank = next_bank;
+            next_bank = nullptr;
+            if ((rc = join_par(ctx, ctx->stream))) return rc;
+        } else if ((rc = stitch_bank(b, nullptr, &bank))) {
             return rc;
+        }
+        if (!last && !ctx->prof_on) {
+            if ((rc = fork_par(ctx, ctx->stream))) return rc;
+            if ((rc = stitch_bank(b + 1, ctx->par, &next_bank))) return rc;
+        }
+        if (b > 0) top_hist = nullptr;
         uint32_t *og = last ? (uint32_t *)(dgroup_out ? dgroup_out : g[b & 1]) : g[b & 1];
         if (!hash) {
             // (b)+(d): sort, then group ids (+ the next round's segments)

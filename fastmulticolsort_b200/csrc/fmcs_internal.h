@@ -201,8 +201,10 @@ constexpr int kMaxSlices = 32;
 // key_bits), key_bits)) of every bank value, one row per chunk and the total
 // in the last row: the first radix level's histograms of a round-0 sort of
 // the bank (chunk_rows = msd_chunk_rows).
+// `stream`: NULL for the context's stream.
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0, uint32_t chunk_rows = 0);
+                  uint64_t n, uint32_t *top_hist = nullptr, uint32_t key_bits = 0, uint32_t chunk_rows = 0,
+                  cudaStream_t stream = nullptr);
 
 // bank[i] <<= lshift (src == NULL) or bank[i] |= (src[i] >> rshift) & mask(width)
 int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t n, uint32_t lshift,

@@ -217,8 +217,9 @@ int launch_bank_update(fmcs_ctx *ctx, void *bank, uint32_t bank_bytes, uint64_t 
 }
 
 int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint32_t bank_bytes,
-                  uint64_t n, uint32_t *top_hist, uint32_t key_bits, uint32_t chunk_rows)
+                  uint64_t n, uint32_t *top_hist, uint32_t key_bits, uint32_t chunk_rows, cudaStream_t stream)
 {
+    cudaStream_t st = stream ? stream : ctx->stream;
     if (ns < 1 || ns > kMaxSlices) return set_error(ctx, FMCS_E_INVAL, "stitch: 1..32 slices");
     if (!(bank_bytes == 1 || bank_bytes == 2 || bank_bytes == 4 || bank_bytes == 8))
         return set_error(ctx, FMCS_E_INVAL, "stitch: bank_bytes must be 1, 2, 4 or 8");
@@ -245,7 +246,7 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
         hist_lo = key_bits - width;
         hist_mask = (1u << width) - 1u;
         const uint64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
-        cudaMemsetAsync(top_hist, 0, (nchunks + 1) * 256 * sizeof(uint32_t), ctx->stream);
+        cudaMemsetAsync(top_hist, 0, (nchunks + 1) * 256 * sizeof(uint32_t), st);
         // contiguous ranges of whole 256-group steps, at most one chunk each
         block_groups = (groups + blocks - 1) / blocks;
         block_groups = (block_groups + 255) / 256 * 256;
@@ -254,7 +255,6 @@ int launch_stitch(fmcs_ctx *ctx, const StitchSlice *sl, int ns, void *bank, uint
         blocks = (groups + block_groups - 1) / block_groups;
     }
     const unsigned grid = (unsigned)blocks;
-    cudaStream_t st = ctx->stream;
     LaunchScope ls_(ctx, "stitch");
     switch (bank_bytes) {
     case 1:
