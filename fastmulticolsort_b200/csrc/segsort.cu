@@ -540,6 +540,9 @@ __global__ void __launch_bounds__(kNtM, kHistCtas) msd_hist_kernel(Bufs<K> b, Le
 // segments are planned at once: slower in all.)
 constexpr int kPlanThreads = 256;
 constexpr int kPlanLoads = 16;
+constexpr int kPlanHelpers = 8;   // CTAs writing level 0's chunk bases beside the segment's CTA
+static_assert(kRadix % kPlanHelpers == 0 && kPlanThreads % (kRadix / kPlanHelpers) == 0 &&
+              kPlanThreads / (kRadix / kPlanHelpers) <= 32, "plan helper layout");
 
 __global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lists lists, bool emit_children = true,
                                                                 uint32_t tile_rows = 0)
@@ -562,6 +565,51 @@ __global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lis
     const uint32_t nseg = ctr[kCtrLarge0 + cur];
     const uint32_t d = threadIdx.x % kRadix;
     const uint32_t q4 = threadIdx.x / kRadix;
+    // Level 0 counted by the stitch: one segment with its totals in the last
+    // row.  CTA 0 plans the segment; CTAs 1..kPlanHelpers write the chunk
+    // bases, each for kRadix / kPlanHelpers digits with kPlanThreads /
+    // (kRadix / kPlanHelpers) threads per digit, each over a share of the rows
+    // (a scan across the digit's threads joins the shares).
+    const bool split0 = counts == r.top_hist && r.chunk_prefix != nullptr;
+    if (split0 && blockIdx.x >= 1 && blockIdx.x <= (unsigned)kPlanHelpers && nseg == 1) {
+        constexpr uint32_t DPB = kRadix / kPlanHelpers;        // digits per helper CTA
+        constexpr uint32_t TPD = kPlanThreads / DPB;           // threads per digit (a power of two <= 32)
+        const uint32_t nrows = r.chunk_prefix[1];
+        cnt[d] = q4 == 0 ? counts[(uint64_t)nrows * kRadix + d] : 0u;
+        uint32_t total;
+        block_exclusive_scan_radix<kPlanThreads>(cnt, tmp, &total);
+        const uint32_t dd = (blockIdx.x - 1) * DPB + threadIdx.x / TPD;
+        const uint32_t sub = threadIdx.x % TPD;
+        const uint32_t per = (nrows + TPD - 1) / TPD;
+        const uint32_t qa = min(nrows, sub * per), qb = min(nrows, qa + per);
+        uint32_t c = 0;
+        for (uint32_t q = qa; q < qb; q += kPlanLoads) {
+            uint32_t v[kPlanLoads];
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + dd] : 0u;
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) c += v[j];
+        }
+        // exclusive scan of the shares across the digit's TPD lanes
+        uint32_t incl = c;
+#pragma unroll
+        for (uint32_t o = 1; o < TPD; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o, TPD);
+            if (sub >= o) incl += y;
+        }
+        uint32_t run = cnt[dd] + incl - c;
+        for (uint32_t q = qa; q < qb; q += kPlanLoads) {
+            uint32_t v[kPlanLoads];
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + dd] : 0u;
+#pragma unroll
+            for (int j = 0; j < kPlanLoads; ++j) {
+                if (q + j < qb) hist[(uint64_t)(q + j) * kRadix + dd] = run;
+                run += v[j];
+            }
+        }
+        return;
+    }
     for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
         const LargeSeg sg = segs[s];
         const uint32_t r0 = r.chunk_prefix ? r.chunk_prefix[s] : s;
@@ -598,7 +646,8 @@ __global__ void __launch_bounds__(kPlanThreads) msd_plan_kernel(LevelRefs r, Lis
         // this share's first base: the digit's offset plus the earlier shares' rows
         uint32_t run = off;
         for (uint32_t j = 0; j < q4; ++j) run += part[j][d];
-        for (uint32_t q = qa; q < qb; q += kPlanLoads) {
+        // (with split0 and one segment the helper CTAs write the bases)
+        for (uint32_t q = qa; q < (split0 && nseg == 1 ? qa : qb); q += kPlanLoads) {
             uint32_t v[kPlanLoads];
 #pragma unroll
             for (int j = 0; j < kPlanLoads; ++j) v[j] = q + j < qb ? counts[(uint64_t)(q + j) * kRadix + d] : 0u;
