@@ -285,6 +285,11 @@ extern "C" int fmcs_create(fmcs_ctx **out, int device, size_t hbm_budget_bytes)
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_status, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_small, 64 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_level, cudaEventDisableTiming);
+    // the second stream and its events exist from the start, so that a call
+    // made while the caller captures the context's stream creates nothing
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->par, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
         fmcs_destroy(ctx);
