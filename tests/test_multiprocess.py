@@ -52,3 +52,16 @@ def test_reference_arm_under_torchrun():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["cores"] == 2
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_host_budget_reports_usable_cores_and_memory():
+    """The reference arm sizes its job count from these: the CPUs of the
+    affinity mask (capped by any cgroup quota) and the memory available."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    cores, mem = bench.host_budget()
+    assert 1 <= cores <= len(os.sched_getaffinity(0))
+    assert mem > 0
+    assert max(1, min(cores, bench.REF_MAX_JOBS, mem // bench.REF_JOB_BYTES)) >= 1
